@@ -1,0 +1,204 @@
+/*
+ * mgbvh.h — C ABI of the B200-native SAH BVH builder.
+ *
+ * This is the drop-in boundary for marigold's `bvh` crate. Each entry point
+ * replaces one piece of the crate's public interface (paths are relative to
+ * the marigold repository):
+ *
+ *   BoundingVolumeHierarchy::<MIN,MAX>::new(list, source, settings)
+ *       bvh/src/lib.rs:698-878
+ *       -> mgbvh_build_indexed   (T = MeshTriangle, S = MeshVertex;
+ *                                 mesh_interface/src/lib.rs:19-30)
+ *       -> mgbvh_build_aabbs     (any T: AsBoundingVolume, e.g. the TLAS over
+ *                                 UploadedMesh, mesh_interface/src/lib.rs:87-91)
+ *   BoundingVolumeHierarchy::nodes / into_nodes   bvh/src/lib.rs:880-886
+ *       -> the out_nodes / out_lens arrays
+ *   the in-place permutation of `list`            bvh/src/lib.rs:597-612
+ *       -> out_perm (out_perm[i] = original index of the object now at i)
+ *   AsGpuBytes for BvhNode                        bvh/src/lib.rs:157-212
+ *       -> mgbvh_node (exact bytes when MAX_LEAF_OBJECTS == 1)
+ *       -> mgbvh_encode_gpu_bytes (the packed form for MAX_LEAF_OBJECTS > 1)
+ *   BvhProfilingInfo                              bvh/src/lib.rs:676-689, 767-875
+ *       -> mgbvh_stats
+ *
+ * The builder runs on one CUDA device. There is no CPU fallback: without a
+ * usable device every build returns MGBVH_ERR_NO_DEVICE.
+ *
+ * Threading: one mgbvh_ctx per calling thread. Calls on distinct contexts may
+ * run concurrently (the crate is called from rayon workers, one mesh each,
+ * marigold/src/app/data/scene/model.rs:77-95). A context is not thread-safe.
+ *
+ * Errors: no exceptions cross this ABI. Negative status = error, nothing
+ * valid written; positive status = warning, outputs valid.
+ */
+#ifndef MGBVH_H
+#define MGBVH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGBVH_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define MGBVH_API __attribute__((visibility("default")))
+#else
+#define MGBVH_API
+#endif
+
+typedef enum mgbvh_status {
+    MGBVH_OK = 0,
+    /* Empty object list: zero nodes written. The crate logs a warning and
+       returns an empty hierarchy (bvh/src/lib.rs:703-708). */
+    MGBVH_WARN_EMPTY = 1,
+    /* MIN/MAX leaf bounds cannot all be met for this object count; the tree is
+       built and follows the max rule first (bvh/src/lib.rs:710-726). */
+    MGBVH_WARN_INFEASIBLE = 2,
+    MGBVH_ERR_INVALID_ARG = -1,
+    MGBVH_ERR_CAPACITY = -2,   /* node_capacity too small for the result */
+    MGBVH_ERR_CUDA = -3,       /* a CUDA runtime call failed */
+    MGBVH_ERR_TIMEOUT = -4,    /* a bounded device-side wait gave up */
+    /* One of the crate's release-mode assertions would have panicked
+       (bvh/src/lib.rs:588, 618-646): child counts or centroid containment. */
+    MGBVH_ERR_ASSERT = -5,
+    MGBVH_ERR_UNSUPPORTED = -6, /* a knob or size outside this build's limits */
+    MGBVH_ERR_NO_DEVICE = -7
+} mgbvh_status;
+
+/* One node, 32 bytes. For MAX_LEAF_OBJECTS == 1 these are exactly the bytes
+   AsGpuBytes writes (bvh/src/lib.rs:163-169) and scene.slang's BvhNode reads.
+   child_node == 0 marks a leaf (the root, index 0, is nobody's child); the
+   children of an inner node are child_node (gt side) and child_node + 1
+   (lt side), bvh/src/lib.rs:650-653. */
+typedef struct mgbvh_node {
+    float min[3];
+    uint32_t start_index;
+    float max[3];
+    uint32_t child_node;
+} mgbvh_node;
+
+/* BvhSettings (bvh/src/lib.rs:668-674) plus the const generics and the split
+   knobs. Fill with mgbvh_default_settings(), which sets the reference profile:
+   32 bins above 32 objects, adaptive sweep at or below 32 objects with
+   len.clamp(8,32) steps, exact centroid thresholds below 8 objects. */
+typedef struct mgbvh_settings {
+    uint32_t min_leaf_objects; /* MIN_LEAF_OBJECTS (>= 1) */
+    uint32_t max_leaf_objects; /* MAX_LEAF_OBJECTS (>= 1) */
+    uint32_t max_depth;        /* BvhSettings::max_depth */
+    uint32_t has_bounds;       /* BvhSettings::bounds is Some(..) */
+    float bounds[6];           /* min xyz, max xyz when has_bounds */
+    /* Split knobs. The reference has none of these (its values are
+       hard-wired at bvh/src/lib.rs:343, 399, 430, 518); defaults reproduce it. */
+    uint32_t bins;           /* 0: len.clamp(16,32); else a fixed count 2..32 */
+    uint32_t adaptive_max_n; /* nodes with len <= this use the adaptive sweep
+                                (reference 32, max 32); 0 turns it off */
+    uint32_t adaptive_steps; /* 0: len.clamp(8,32) thresholds for len >= 8;
+                                else a fixed count 1..32 */
+    uint32_t profiling_info; /* fill mgbvh_stats leaf statistics */
+} mgbvh_settings;
+
+/* BvhProfilingInfo field set (bvh/src/lib.rs:676-689), plus counters that
+   the reference does not keep. construction_time is device time in seconds
+   from the first build kernel to the last. */
+typedef struct mgbvh_stats {
+    double construction_time;
+    uint32_t node_count;
+    uint32_t leaf_node_count;
+    uint32_t min_leaf_object_count;
+    uint32_t max_leaf_object_count;
+    double avg_leaf_object_count;
+    double stddev_leaf_object_count;
+    uint32_t total_object_count;
+    uint32_t height;
+    uint32_t max_depth;
+    uint32_t median_splits;       /* forced median splits taken */
+    uint32_t depth_capped_leaves; /* leaves made by depth == max_depth with len > 1 */
+    uint32_t feasible;            /* the crate's feasibility flag */
+} mgbvh_stats;
+
+typedef struct mgbvh_ctx mgbvh_ctx;
+
+/* Fills *s with the reference profile and max_depth 32
+   (marigold/src/app/data/scene/mod.rs:28-29), MIN = MAX = 1, no bounds. */
+MGBVH_API void mgbvh_default_settings(mgbvh_settings* s);
+
+/* Device context: owns scratch buffers (grown on demand), a stream and events. */
+MGBVH_API int mgbvh_create(int device, mgbvh_ctx** out_ctx);
+MGBVH_API void mgbvh_destroy(mgbvh_ctx* ctx);
+/* Run subsequent builds on a caller stream (cudaStream_t); NULL = own stream. */
+MGBVH_API int mgbvh_set_stream(mgbvh_ctx* ctx, void* cuda_stream);
+/* Text of the last error recorded on this context. */
+MGBVH_API const char* mgbvh_last_error(const mgbvh_ctx* ctx);
+MGBVH_API const char* mgbvh_status_string(int status);
+
+/*
+ * BLAS build over MeshTriangle / MeshVertex. Replaces
+ * BoundingVolumeHierarchy::<MIN,MAX>::new(&mut triangles, &vertices, settings)
+ * (bvh/src/lib.rs:698), as called at marigold/src/app/data/scene/model.rs:93.
+ *
+ * vertices: vertex_count records of vertex_stride_bytes bytes whose first 12
+ *   bytes are the f32 position (MeshVertex is 32 bytes,
+ *   mesh_interface/src/lib.rs:6-12).
+ * triangles: triangle_count * 3 vertex indices (MeshTriangle).
+ * out_nodes: node_capacity >= 2 * triangle_count - 1 is always enough.
+ * out_lens: per-node object count (BvhNode::len), may be NULL.
+ * out_perm: triangle_count entries; apply it to the triangle list to obtain
+ *   the crate's in-place permutation.
+ * out_stats: may be NULL.
+ * All pointers are host pointers. Returns mgbvh_status.
+ */
+MGBVH_API int mgbvh_build_indexed(mgbvh_ctx* ctx, const float* vertices, uint32_t vertex_stride_bytes,
+                        uint32_t vertex_count, const uint32_t* triangles, uint32_t triangle_count,
+                        const mgbvh_settings* settings, mgbvh_node* out_nodes,
+                        uint32_t node_capacity, uint32_t* out_node_count, uint32_t* out_lens,
+                        uint32_t* out_perm, mgbvh_stats* out_stats);
+
+/*
+ * Build over precomputed object AABBs (min xyz, max xyz per object, 24 bytes):
+ * the AsBoundingVolume path, e.g. the TLAS over UploadedMesh built by
+ * marigold/src/app/data/scene/geometry/mod.rs:175-199. Same outputs.
+ */
+MGBVH_API int mgbvh_build_aabbs(mgbvh_ctx* ctx, const float* aabbs, uint32_t count,
+                      const mgbvh_settings* settings, mgbvh_node* out_nodes,
+                      uint32_t node_capacity, uint32_t* out_node_count, uint32_t* out_lens,
+                      uint32_t* out_perm, mgbvh_stats* out_stats);
+
+/* Device-pointer forms of the two builds: every array argument is device
+   memory; out_node_count and out_stats stay host pointers. The call returns
+   after the build has finished on the context's stream. */
+MGBVH_API int mgbvh_build_indexed_dev(mgbvh_ctx* ctx, const float* d_vertices, uint32_t vertex_stride_bytes,
+                            uint32_t vertex_count, const uint32_t* d_triangles,
+                            uint32_t triangle_count, const mgbvh_settings* settings,
+                            mgbvh_node* d_out_nodes, uint32_t node_capacity,
+                            uint32_t* out_node_count, uint32_t* d_out_lens, uint32_t* d_out_perm,
+                            mgbvh_stats* out_stats);
+MGBVH_API int mgbvh_build_aabbs_dev(mgbvh_ctx* ctx, const float* d_aabbs, uint32_t count,
+                          const mgbvh_settings* settings, mgbvh_node* d_out_nodes,
+                          uint32_t node_capacity, uint32_t* out_node_count, uint32_t* d_out_lens,
+                          uint32_t* d_out_perm, mgbvh_stats* out_stats);
+
+/*
+ * AsGpuBytes for BvhNode (bvh/src/lib.rs:157-212), host side: 8 u32 words per
+ * node. For MAX_LEAF_OBJECTS == 1 this copies the node. For larger MAX the
+ * last word packs len into the top ilog2(MAX.next_power_of_two()) bits and
+ * keeps child_node & !len_mask in the rest, exactly as the crate writes it.
+ * Returns MGBVH_ERR_ASSERT where the crate's assert (leaf len < 2^len_bits)
+ * would panic.
+ */
+MGBVH_API int mgbvh_encode_gpu_bytes(const mgbvh_node* nodes, const uint32_t* lens, uint32_t count,
+                           uint32_t max_leaf_objects, uint32_t* out_words);
+
+/* Total SAH cost of a built tree, normalised by the root's surface area, with
+   the crate's DEPTH_COST = 1 and OBJECT_COST = 8 (bvh/src/lib.rs:217-218):
+   sum over inner nodes of SA(n)/SA(root) + sum over leaves of
+   8 * len * SA(n)/SA(root). Host computation in f64. */
+MGBVH_API double mgbvh_sah_cost(const mgbvh_node* nodes, const uint32_t* lens, uint32_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MGBVH_H */

@@ -1,0 +1,166 @@
+"""ctypes binding of ``libmgbvh.so`` (the C ABI in include/mgbvh.h).
+
+The library is the only compute path: there is no CPU fallback. Loading
+fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmgbvh.so")
+
+OK = 0
+WARN_EMPTY = 1
+WARN_INFEASIBLE = 2
+ERR_INVALID_ARG = -1
+ERR_CAPACITY = -2
+ERR_CUDA = -3
+ERR_TIMEOUT = -4
+ERR_ASSERT = -5
+ERR_UNSUPPORTED = -6
+ERR_NO_DEVICE = -7
+
+# every entry point declared in include/mgbvh.h
+EXPORTED = (
+    "mgbvh_default_settings", "mgbvh_create", "mgbvh_destroy", "mgbvh_set_stream",
+    "mgbvh_last_error", "mgbvh_status_string", "mgbvh_build_indexed", "mgbvh_build_aabbs",
+    "mgbvh_build_indexed_dev", "mgbvh_build_aabbs_dev", "mgbvh_encode_gpu_bytes",
+    "mgbvh_sah_cost",
+)
+
+
+class Node(ctypes.Structure):
+    """mgbvh_node: 32 bytes, AsGpuBytes layout for MAX_LEAF_OBJECTS == 1."""
+
+    _fields_ = [("min", ctypes.c_float * 3), ("start_index", ctypes.c_uint32),
+                ("max", ctypes.c_float * 3), ("child_node", ctypes.c_uint32)]
+
+
+class Settings(ctypes.Structure):
+    _fields_ = [
+        ("min_leaf_objects", ctypes.c_uint32),
+        ("max_leaf_objects", ctypes.c_uint32),
+        ("max_depth", ctypes.c_uint32),
+        ("has_bounds", ctypes.c_uint32),
+        ("bounds", ctypes.c_float * 6),
+        ("bins", ctypes.c_uint32),
+        ("adaptive_max_n", ctypes.c_uint32),
+        ("adaptive_steps", ctypes.c_uint32),
+        ("profiling_info", ctypes.c_uint32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("construction_time", ctypes.c_double),
+        ("node_count", ctypes.c_uint32),
+        ("leaf_node_count", ctypes.c_uint32),
+        ("min_leaf_object_count", ctypes.c_uint32),
+        ("max_leaf_object_count", ctypes.c_uint32),
+        ("avg_leaf_object_count", ctypes.c_double),
+        ("stddev_leaf_object_count", ctypes.c_double),
+        ("total_object_count", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("max_depth", ctypes.c_uint32),
+        ("median_splits", ctypes.c_uint32),
+        ("depth_capped_leaves", ctypes.c_uint32),
+        ("feasible", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class MgbvhError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"mgbvh status {status}: {message}")
+        self.status = status
+
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load():
+    """Load libmgbvh.so and declare its prototypes."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m marigold_b200.build` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        u32 = ctypes.c_uint32
+        pu32 = ctypes.POINTER(u32)
+        L.mgbvh_default_settings.argtypes = [ctypes.POINTER(Settings)]
+        L.mgbvh_default_settings.restype = None
+        L.mgbvh_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+        L.mgbvh_create.restype = ctypes.c_int
+        L.mgbvh_destroy.argtypes = [P]
+        L.mgbvh_destroy.restype = None
+        L.mgbvh_set_stream.argtypes = [P, P]
+        L.mgbvh_set_stream.restype = ctypes.c_int
+        L.mgbvh_last_error.argtypes = [P]
+        L.mgbvh_last_error.restype = ctypes.c_char_p
+        L.mgbvh_status_string.argtypes = [ctypes.c_int]
+        L.mgbvh_status_string.restype = ctypes.c_char_p
+        build_args = [P, P, u32, u32, P, u32, ctypes.POINTER(Settings), P, u32, pu32, P, P,
+                      ctypes.POINTER(Stats)]
+        L.mgbvh_build_indexed.argtypes = build_args
+        L.mgbvh_build_indexed.restype = ctypes.c_int
+        L.mgbvh_build_indexed_dev.argtypes = build_args
+        L.mgbvh_build_indexed_dev.restype = ctypes.c_int
+        aabb_args = [P, P, u32, ctypes.POINTER(Settings), P, u32, pu32, P, P, ctypes.POINTER(Stats)]
+        L.mgbvh_build_aabbs.argtypes = aabb_args
+        L.mgbvh_build_aabbs.restype = ctypes.c_int
+        L.mgbvh_build_aabbs_dev.argtypes = aabb_args
+        L.mgbvh_build_aabbs_dev.restype = ctypes.c_int
+        L.mgbvh_encode_gpu_bytes.argtypes = [P, P, u32, u32, P]
+        L.mgbvh_encode_gpu_bytes.restype = ctypes.c_int
+        L.mgbvh_sah_cost.argtypes = [P, P, u32]
+        L.mgbvh_sah_cost.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def status_string(status: int) -> str:
+    return load().mgbvh_status_string(status).decode()
+
+
+class Context:
+    """An mgbvh_ctx: one CUDA device, its stream and scratch buffers."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.ptr = ctypes.c_void_p()
+        rc = self.L.mgbvh_create(device, ctypes.byref(self.ptr))
+        if rc != OK:
+            raise MgbvhError(rc, status_string(rc))
+
+    def last_error(self) -> str:
+        return self.L.mgbvh_last_error(self.ptr).decode()
+
+    def check(self, rc: int) -> int:
+        if rc < 0:
+            raise MgbvhError(rc, f"{status_string(rc)}: {self.last_error()}")
+        return rc
+
+    def set_stream(self, stream_handle: int | None):
+        self.check(self.L.mgbvh_set_stream(self.ptr, ctypes.c_void_p(stream_handle or 0)))
+
+    def close(self):
+        if self.ptr:
+            self.L.mgbvh_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,1659 @@
+// mgbvh_build.cu — B200 SAH BVH builder: kernels, orchestration and C ABI.
+//
+// The tree is the one bvh/src/lib.rs:698-878 builds, bit for bit: same split
+// decisions, node bounds, child links, start indices and (for single-object
+// leaves) object order. Work is split by node size:
+//
+//   large  (len > kMediumMax)   level-synchronous over all large nodes:
+//                               lvl_bin   per-tile 3x32-bin histograms of
+//                                         counts and AABBs in shared memory,
+//                                         merged across tiles with atomics
+//                               lvl_eval  one warp per node: prefix/suffix
+//                                         sweeps, SAH costs, argmin, children
+//                               lvl_part  stable scan partition of the
+//                                         node's 32-byte object records
+//   medium (33..kMediumMax)     one CTA per node builds the whole subtree
+//                               with records in shared memory, warps per
+//                               sub-node, 16-bit index partitions
+//   small  (<= 32)              one warp per subtree, objects in registers
+//                               (mgbvh_device.cuh)
+//
+// Node slots come from the closed-form pre-order numbering (see Out in
+// mgbvh_device.cuh); a compaction pass removes holes left by multi-object
+// leaves.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/device/device_scan.cuh>
+
+#include "mgbvh_device.cuh"
+
+namespace mgbvh {
+
+constexpr uint32_t kMediumMax = 1024;
+constexpr uint32_t kTile = 2048;
+constexpr int kTileThreads = 256;
+constexpr int kMediumWarps = 8;
+constexpr int kMediumThreads = kMediumWarps * 32;
+constexpr uint32_t kBinWords = 3 * 32 * 7;  // [axis][bin]{count, lo key xyz, hi key xyz}
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kMediumListCap = kMediumMax / (kSmallMax + 1) + 1;
+
+struct Rec {
+    float4 lo;  // min xyz, object id (bits)
+    float4 hi;  // max xyz, 0
+};
+
+// A node waiting to be split (large, medium or small list entry). 64 bytes.
+struct Task {
+    float lo[3];
+    uint32_t start;
+    float hi[3];
+    uint32_t len;
+    uint32_t slot, pair, depth, buf;
+    uint32_t tile0, ntiles, pad0, pad1;
+};
+
+// Split decision of one large node, read by its partition tiles.
+struct Decision {
+    uint32_t kind;  // 0 split, 1 leaf
+    uint32_t axis, split_bin, bins;
+    float cmin, ext;
+    uint32_t n_lt;
+    uint32_t child_task[2];  // [0] gt, [1] lt: next-level large task, or kNone
+    uint32_t child_leaf[2];
+    uint32_t pad;
+    float ltb[6], gtb[6];
+};
+
+// ---------------------------------------------------------------- helpers
+
+__device__ __forceinline__ void block_reduce_keys_to_global(uint32_t* keys /*12*/, uint32_t* smem12,
+                                                            uint32_t* global12) {
+    // keys[0..5]: min keys; keys[6..11] : max keys ; layout per call site
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+        const bool is_min = (k % 6) < 3;
+        const uint32_t v = is_min ? __reduce_min_sync(kFull, keys[k]) : __reduce_max_sync(kFull, keys[k]);
+        if (lane == 0) {
+            if (is_min)
+                atomicMin(&smem12[k], v);
+            else
+                atomicMax(&smem12[k], v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        const bool is_min = (threadIdx.x % 6) < 3;
+        if (is_min)
+            atomicMin(&global12[threadIdx.x], smem12[threadIdx.x]);
+        else
+            atomicMax(&global12[threadIdx.x], smem12[threadIdx.x]);
+    }
+}
+
+__device__ __forceinline__ void init_key12(uint32_t* k) {
+#pragma unroll
+    for (int i = 0; i < 12; ++i) k[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+}
+
+__device__ __forceinline__ void accum_keys(uint32_t* k, float lx, float ly, float lz, float hx,
+                                           float hy, float hz) {
+    // bounds: k[0..2] min lo, k[3..5] max hi; centroids: k[6..8] min, k[9..11] max
+    k[0] = min(k[0], fkey(lx));
+    k[1] = min(k[1], fkey(ly));
+    k[2] = min(k[2], fkey(lz));
+    k[3] = max(k[3], fkey(hx));
+    k[4] = max(k[4], fkey(hy));
+    k[5] = max(k[5], fkey(hz));
+    const uint32_t c0 = fkey(center_of(lx, hx)), c1 = fkey(center_of(ly, hy)),
+                   c2 = fkey(center_of(lz, hz));
+    k[6] = min(k[6], c0);
+    k[7] = min(k[7], c1);
+    k[8] = min(k[8], c2);
+    k[9] = max(k[9], c0);
+    k[10] = max(k[10], c1);
+    k[11] = max(k[11], c2);
+}
+
+// ---------------------------------------------------------------- prep
+
+// Object records from MeshTriangle/MeshVertex (mesh_interface/src/lib.rs:19-30)
+// plus the root's bounds and centroid bounds.
+__global__ void __launch_bounds__(256) prep_indexed_kernel(const float* __restrict__ verts,
+                                                           uint32_t stride_floats, uint32_t nverts,
+                                                           const uint32_t* __restrict__ tris,
+                                                           uint32_t n, Rec* __restrict__ out,
+                                                           Counters* ctr) {
+    __shared__ uint32_t sk[12];
+    if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    __syncthreads();
+    uint32_t k[12];
+    init_key12(k);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t t0 = tris[3 * (size_t)i], t1 = tris[3 * (size_t)i + 1], t2 = tris[3 * (size_t)i + 2];
+        if (t0 >= nverts || t1 >= nverts || t2 >= nverts) {
+            set_error(ctr, MGBVH_ERR_INVALID_ARG, kSiteIndex);
+            t0 = t1 = t2 = 0;
+        }
+        const float* p0 = verts + (size_t)t0 * stride_floats;
+        const float* p1 = verts + (size_t)t1 * stride_floats;
+        const float* p2 = verts + (size_t)t2 * stride_floats;
+        float lo[3], hi[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float x0 = __fadd_rn(__ldg(p0 + a), 0.0f), x1 = __fadd_rn(__ldg(p1 + a), 0.0f),
+                        x2 = __fadd_rn(__ldg(p2 + a), 0.0f);
+            lo[a] = fminf(fminf(x0, x1), x2);
+            hi[a] = fmaxf(fmaxf(x0, x1), x2);
+        }
+        Rec r;
+        r.lo = make_float4(lo[0], lo[1], lo[2], __uint_as_float(i));
+        r.hi = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        out[i] = r;
+        accum_keys(k, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
+    }
+    block_reduce_keys_to_global(k, sk, ctr->root_keys);
+}
+
+// Object records from AABBs (min xyz, max xyz): the AsBoundingVolume path.
+__global__ void __launch_bounds__(256) prep_aabbs_kernel(const float* __restrict__ aabbs, uint32_t n,
+                                                         Rec* __restrict__ out, Counters* ctr) {
+    __shared__ uint32_t sk[12];
+    if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    __syncthreads();
+    uint32_t k[12];
+    init_key12(k);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float* p = aabbs + 6 * (size_t)i;
+        float v[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) v[j] = __fadd_rn(__ldg(p + j), 0.0f);
+        Rec r;
+        r.lo = make_float4(v[0], v[1], v[2], __uint_as_float(i));
+        r.hi = make_float4(v[3], v[4], v[5], 0.0f);
+        out[i] = r;
+        accum_keys(k, v[0], v[1], v[2], v[3], v[4], v[5]);
+    }
+    block_reduce_keys_to_global(k, sk, ctr->root_keys);
+}
+
+__device__ __forceinline__ void init_task_bins(uint32_t* b, uint32_t lane, uint32_t nthreads) {
+    for (uint32_t w = lane; w < kBinWords; w += nthreads) {
+        const uint32_t f = w % 7u;
+        b[w] = f == 0 ? 0u : (f <= 3 ? kKeyPosInf : kKeyNegInf);
+    }
+}
+
+// Root node: classify and enqueue (or finish, when the root is a leaf).
+// cls: 0 leaf, 1 small, 2 medium, 3 large.
+__global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, float b0, float b1,
+                                 float b2, float b3, float b4, float b5, Task* large, uint32_t* bins,
+                                 uint32_t* cbkeys, uint32_t* tile_task, uint32_t* tile_begin,
+                                 Task* medium, Task* small, Out O, uint32_t ntiles,
+                                 uint32_t max_depth) {
+    float b[6];
+    if (has_bounds) {
+        b[0] = b0; b[1] = b1; b[2] = b2; b[3] = b3; b[4] = b4; b[5] = b5;
+    } else {
+        for (int i = 0; i < 6; ++i) b[i] = funkey(O.ctr->root_keys[i]);
+    }
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t gsz = gridDim.x * blockDim.x;
+    Task t;
+    for (int a = 0; a < 3; ++a) {
+        t.lo[a] = b[a];
+        t.hi[a] = b[3 + a];
+    }
+    t.start = 0;
+    t.len = n;
+    t.slot = 0;
+    t.pair = 1;
+    t.depth = 0;
+    t.buf = 0;
+    t.tile0 = 0;
+    t.ntiles = ntiles;
+    t.pad0 = t.pad1 = 0;
+    if (cls == 0) {
+        if (gtid == 0) {
+            mgbvh_node nd;
+            for (int a = 0; a < 3; ++a) {
+                nd.min[a] = b[a];
+                nd.max[a] = b[3 + a];
+            }
+            nd.start_index = 0;
+            nd.child_node = 0;
+            O.nodes[0] = nd;
+            O.lens[0] = n;
+            O.used[0] = 1;
+            if (n > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (max_depth == 0) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+        }
+        for (uint32_t i = gtid; i < n; i += gsz) O.perm[i] = i;
+        return;
+    }
+    if (cls == 1) {
+        if (gtid == 0) {
+            small[0] = t;
+            O.ctr->n_small = 1;
+        }
+        return;
+    }
+    if (cls == 2) {
+        if (gtid == 0) {
+            medium[0] = t;
+            O.ctr->n_medium = 1;
+        }
+        return;
+    }
+    if (gtid == 0) large[0] = t;
+    if (blockIdx.x == 0) init_task_bins(bins, threadIdx.x, blockDim.x);
+    if (gtid < 6) cbkeys[gtid] = O.ctr->root_keys[6 + gtid];
+    for (uint32_t i = gtid; i < ntiles; i += gsz) {
+        tile_task[i] = 0;
+        tile_begin[i] = i * kTile;
+    }
+}
+
+// ---------------------------------------------------------------- large level
+
+__global__ void __launch_bounds__(kTileThreads) lvl_bin_kernel(
+    const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* __restrict__ bins,
+    const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
+    uint32_t* __restrict__ tile_hist, const Rec* __restrict__ rec0, const Rec* __restrict__ rec1,
+    Params P) {
+    __shared__ uint32_t sb[kBinWords];
+    const uint32_t tile = blockIdx.x;
+    const uint32_t ti = tile_task[tile];
+    const Task& t = tasks[ti];
+    const uint32_t begin = tile_begin[tile];
+    const uint32_t cnt = min(kTile, t.len - begin);
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+    init_task_bins(sb, threadIdx.x, blockDim.x);
+    float cmn[3], ext[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        cmn[a] = funkey(cbkeys[6 * ti + a]);
+        ext[a] = __fsub_rn(funkey(cbkeys[6 * ti + 3 + a]), cmn[a]);
+    }
+    const uint32_t B = P.bins ? P.bins : 32u;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+        const float4 lo = src[i].lo, hi = src[i].hi;
+        const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (ext[a] == 0.0f) continue;
+            const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
+            uint32_t* w = sb + (a * 32 + b) * 7;
+            atomicAdd(w, 1u);
+            atomicMin(w + 1, fkey(l[0]));
+            atomicMin(w + 2, fkey(l[1]));
+            atomicMin(w + 3, fkey(l[2]));
+            atomicMax(w + 4, fkey(h[0]));
+            atomicMax(w + 5, fkey(h[1]));
+            atomicMax(w + 6, fkey(h[2]));
+        }
+    }
+    __syncthreads();
+    for (uint32_t w = threadIdx.x; w < 96; w += blockDim.x) tile_hist[tile * 96 + w] = sb[w * 7];
+    uint32_t* gb = bins + (size_t)ti * kBinWords;
+    for (uint32_t k = threadIdx.x; k < kBinWords; k += blockDim.x) {
+        const uint32_t bin = k / 7u, f = k % 7u;
+        const uint32_t v = sb[k];
+        if (sb[bin * 7] == 0) continue;
+        if (f == 0)
+            atomicAdd(gb + k, v);
+        else if (f <= 3)
+            atomicMin(gb + k, v);
+        else
+            atomicMax(gb + k, v);
+    }
+}
+
+struct EvalArgs {
+    const Task* tasks;
+    uint32_t n_tasks;
+    const uint32_t* bins;
+    const uint32_t* cbkeys;
+    const uint32_t* tile_hist;
+    uint32_t* tile_lt;
+    Decision* dec;
+    Task* next_tasks;
+    uint32_t* next_bins;
+    uint32_t* next_cbkeys;
+    uint32_t* next_tile_task;
+    uint32_t* next_tile_begin;
+    Task* medium;
+    Task* small;
+    uint32_t cap_tasks, cap_tiles, cap_medium, cap_small;
+};
+
+__global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= A.n_tasks) return;
+    const Task t = A.tasks[w];
+    const uint32_t* tb = A.bins + (size_t)w * kBinWords;
+    float cmn[3], ext[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        cmn[a] = funkey(A.cbkeys[6 * w + a]);
+        ext[a] = __fsub_rn(funkey(A.cbkeys[6 * w + 3 + a]), cmn[a]);
+    }
+    const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    const uint32_t B = P.bins ? P.bins : 32u;
+    bool leaf = t.depth == P.max_depth || (t.len <= P.max_leaf && t.len < 2u * P.min_leaf);
+    Decision d;
+    d.kind = 1;
+    d.axis = d.split_bin = 0;
+    d.bins = B;
+    d.cmin = d.ext = 0.0f;
+    d.n_lt = 0;
+    d.child_task[0] = d.child_task[1] = kNone;
+    d.child_leaf[0] = d.child_leaf[1] = 0;
+    d.pad = 0;
+    Cand win;
+    if (!leaf) {
+        uint32_t cnt[3];
+        float box[3][6];
+        bool axis_ok[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t* bw = tb + (a * 32 + lane) * 7;
+            cnt[a] = bw[0];
+            for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
+            axis_ok[a] = !(ext[a] == 0.0f);
+        }
+        Cand best;
+        binned_candidates(cnt, box, axis_ok, B, t.len, surface_area6(nb), P, lane, best);
+        const uint64_t wk = warp_min_key(best.key);
+        const uint32_t wlo = static_cast<uint32_t>(wk);
+        if (wlo == kNoKey) {
+            if (t.len > P.max_leaf) {
+                if (lane == 0) set_error(O.ctr, MGBVH_ERR_UNSUPPORTED, kSiteLargeMedian);
+                return;
+            }
+            leaf = true;
+        } else {
+            d.axis = (wlo >> 8) & 3u;
+            d.split_bin = wlo & 0xFFu;
+            win = best;
+            shfl_cand(win, d.split_bin);
+            const float cost = funkey(static_cast<uint32_t>(wk >> 32));
+            if (t.len <= P.max_leaf && cost >= leaf_cost(t.len)) leaf = true;
+        }
+    }
+    if (leaf) {
+        warp_store_node(O, t.slot, nb, t.start, t.len, 0u, lane);
+        if (lane == 0) {
+            A.dec[w] = d;
+            if (t.len > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (t.depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+        }
+        return;
+    }
+    d.kind = 0;
+    d.cmin = cmn[d.axis];
+    d.ext = ext[d.axis];
+    d.n_lt = win.n_lt;
+    for (int i = 0; i < 6; ++i) {
+        d.ltb[i] = win.lt[i];
+        d.gtb[i] = win.gt[i];
+    }
+    // lt count of every tile of the node, exclusive-scanned across tiles
+    uint32_t carry = 0;
+    for (uint32_t b0 = 0; b0 < t.ntiles; b0 += 32) {
+        const uint32_t ti = b0 + lane;
+        uint32_t v = 0;
+        if (ti < t.ntiles) {
+            const uint32_t* h = A.tile_hist + (size_t)(t.tile0 + ti) * 96 + d.axis * 32;
+            for (uint32_t b = 0; b < d.split_bin; ++b) v += h[b];
+        }
+        uint32_t inc = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t u = __shfl_up_sync(kFull, inc, off);
+            if (lane >= static_cast<uint32_t>(off)) inc += u;
+        }
+        if (ti < t.ntiles) A.tile_lt[t.tile0 + ti] = carry + inc - v;
+        carry += __shfl_sync(kFull, inc, 31);
+    }
+    if (carry != d.n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
+    warp_store_node(O, t.slot, nb, t.start, t.len, t.pair, lane);
+    if (lane == 0) atomicMax(&O.ctr->height, t.depth);
+    const uint32_t n_gt = t.len - d.n_lt;
+    for (int c = 0; c < 2; ++c) {
+        const uint32_t len = c == 0 ? n_gt : d.n_lt;
+        const uint32_t start = c == 0 ? t.start + d.n_lt : t.start;
+        const uint32_t slot = c == 0 ? t.pair : t.pair + 1u;
+        const uint32_t pair = c == 0 ? t.pair + 2u : t.pair + 2u * n_gt;
+        const uint32_t depth = t.depth + 1u;
+        const float* cb = c == 0 ? win.gt : win.lt;
+        const bool cleaf = len <= 1u || depth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
+        Task ct;
+        for (int a = 0; a < 3; ++a) {
+            ct.lo[a] = cb[a];
+            ct.hi[a] = cb[3 + a];
+        }
+        ct.start = start;
+        ct.len = len;
+        ct.slot = slot;
+        ct.pair = pair;
+        ct.depth = depth;
+        ct.buf = t.buf ^ 1u;
+        ct.tile0 = ct.ntiles = 0;
+        ct.pad0 = ct.pad1 = 0;
+        if (cleaf) {
+            warp_store_node(O, slot, cb, start, len, 0u, lane);
+            d.child_leaf[c] = 1;
+            if (lane == 0 && len > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+        } else if (len > kMediumMax) {
+            const uint32_t nt = (len + kTile - 1) / kTile;
+            uint32_t ti = 0, t0 = 0;
+            if (lane == 0) {
+                ti = atomicAdd(&O.ctr->n_next_large, 1u);
+                t0 = atomicAdd(&O.ctr->n_next_tiles, nt);
+            }
+            ti = __shfl_sync(kFull, ti, 0);
+            t0 = __shfl_sync(kFull, t0, 0);
+            if (ti >= A.cap_tasks || t0 + nt > A.cap_tiles) {
+                if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                continue;
+            }
+            ct.tile0 = t0;
+            ct.ntiles = nt;
+            if (lane == 0) A.next_tasks[ti] = ct;
+            init_task_bins(A.next_bins + (size_t)ti * kBinWords, lane, 32);
+            if (lane < 6) A.next_cbkeys[6 * ti + lane] = lane < 3 ? kKeyPosInf : kKeyNegInf;
+            for (uint32_t i = lane; i < nt; i += 32) {
+                A.next_tile_task[t0 + i] = ti;
+                A.next_tile_begin[t0 + i] = i * kTile;
+            }
+            d.child_task[c] = ti;
+        } else if (len > kSmallMax) {
+            uint32_t mi = 0;
+            if (lane == 0) mi = atomicAdd(&O.ctr->n_medium, 1u);
+            mi = __shfl_sync(kFull, mi, 0);
+            if (mi >= A.cap_medium) {
+                if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                continue;
+            }
+            if (lane == 0) A.medium[mi] = ct;
+        } else {
+            uint32_t si = 0;
+            if (lane == 0) si = atomicAdd(&O.ctr->n_small, 1u);
+            si = __shfl_sync(kFull, si, 0);
+            if (si >= A.cap_small) {
+                if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                continue;
+            }
+            if (lane == 0) A.small[si] = ct;
+        }
+    }
+    if (lane == 0) A.dec[w] = d;
+}
+
+__global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
+    const Task* __restrict__ tasks, const Decision* __restrict__ dec,
+    const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
+    const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, uint32_t* next_cbkeys, Out O) {
+    __shared__ uint32_t wcnt[kTileThreads / 32];
+    __shared__ uint32_t sk[12];
+    const uint32_t tile = blockIdx.x;
+    const uint32_t ti = tile_task[tile];
+    const Task t = tasks[ti];
+    const Decision d = dec[ti];
+    const uint32_t begin = tile_begin[tile];
+    const uint32_t cnt = min(kTile, t.len - begin);
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+    Rec* dst = t.buf ? rec0 : rec1;
+    if (d.kind == 1) {
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+            O.perm[t.start + begin + i] = __float_as_uint(src[i].lo.w);
+        return;
+    }
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t below = (1u << lane) - 1u;
+    const uint32_t lt_off = tile_lt[tile];
+    const uint32_t lt_base = t.start + lt_off;
+    const uint32_t gt_base = t.start + d.n_lt + (begin - lt_off);
+    // child centroid bounds: k[0..5] lt (min xyz, max xyz), k[6..11] gt
+    uint32_t k[12];
+    init_key12(k);
+    if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    bool bad = false;
+    uint32_t run_lt = 0;
+    for (uint32_t r = 0; r < cnt; r += blockDim.x) {
+        const uint32_t i = r + threadIdx.x;
+        const bool valid = i < cnt;
+        Rec rec;
+        rec.lo = rec.hi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (valid) rec = src[i];
+        const float c[3] = {center_of(rec.lo.x, rec.hi.x), center_of(rec.lo.y, rec.hi.y),
+                            center_of(rec.lo.z, rec.hi.z)};
+        const float ca = d.axis == 0 ? c[0] : (d.axis == 1 ? c[1] : c[2]);
+        const bool pred = valid && bin_of(ca, d.cmin, d.ext, d.bins) < d.split_bin;
+        const uint32_t m = __ballot_sync(kFull, pred);
+        if (lane == 0) wcnt[warp] = __popc(m);
+        __syncthreads();
+        uint32_t wpre = 0, tot = 0;
+        for (uint32_t q = 0; q < blockDim.x / 32; ++q) {
+            const uint32_t v = wcnt[q];
+            if (q < warp) wpre += v;
+            tot += v;
+        }
+        __syncthreads();
+        if (valid) {
+            const uint32_t ltr = run_lt + wpre + __popc(m & below);
+            const uint32_t side = pred ? 1u : 0u;  // child index: 0 gt, 1 lt
+            const uint32_t dest = pred ? lt_base + ltr : gt_base + (i - ltr);
+            if (dest - t.start < t.len) {
+                dst[dest] = rec;
+                if (d.child_leaf[side]) O.perm[dest] = __float_as_uint(rec.lo.w);
+            } else {
+                bad = true;  // inconsistent counts; never write outside the node
+            }
+            bad |= !box_contains(pred ? d.ltb : d.gtb, c[0], c[1], c[2]);
+            uint32_t* kk = pred ? k : k + 6;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                kk[a] = min(kk[a], fkey(c[a]));
+                kk[3 + a] = max(kk[3 + a], fkey(c[a]));
+            }
+        }
+        run_lt += tot;
+    }
+    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+    // centroid bounds of the large children
+    const bool need_lt = d.child_task[1] != kNone, need_gt = d.child_task[0] != kNone;
+    if (need_lt || need_gt) {
+#pragma unroll
+        for (int q = 0; q < 12; ++q) {
+            const bool is_min = (q % 6) < 3;
+            const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+            if (lane == 0) {
+                if (is_min)
+                    atomicMin(&sk[q], v);
+                else
+                    atomicMax(&sk[q], v);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < 12) {
+            const uint32_t q = threadIdx.x;
+            const uint32_t child = q < 6 ? d.child_task[1] : d.child_task[0];
+            if (child != kNone) {
+                uint32_t* g = next_cbkeys + 6 * child + (q % 6);
+                if ((q % 6) < 3)
+                    atomicMin(g, sk[q]);
+                else
+                    atomicMax(g, sk[q]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- medium
+
+struct MNode {  // 64 bytes
+    float b[6];
+    float cb[6];
+    uint32_t s, n, slot, pair;
+};
+struct MNodeExtra {
+    uint32_t depth, ib;
+};
+
+struct MediumSmem {
+    float4 rlo[kMediumMax];
+    float4 rhi[kMediumMax];
+    uint16_t idx[2][kMediumMax];
+    MNode list[2][kMediumListCap];
+    MNodeExtra list_x[2][kMediumListCap];
+    uint32_t bins[kMediumWarps][kBinWords];
+    XRec xchg[kMediumWarps][32];
+    uint32_t list_n[2];
+    uint32_t rootk[12];
+};
+
+__device__ __forceinline__ void medium_load_warp_records(const MediumSmem& S, uint32_t ib, uint32_t s,
+                                                         uint32_t n, uint32_t lane, float* lo,
+                                                         float* hi, uint32_t& id) {
+    if (lane < n) {
+        const uint32_t r = S.idx[ib][s + lane];
+        const float4 a = S.rlo[r], b = S.rhi[r];
+        lo[0] = a.x;
+        lo[1] = a.y;
+        lo[2] = a.z;
+        id = __float_as_uint(a.w);
+        hi[0] = b.x;
+        hi[1] = b.y;
+        hi[2] = b.z;
+    } else {
+        lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0.0f;
+        id = 0;
+    }
+}
+
+// Warp: finish a leaf of the medium subtree (record + permutation).
+__device__ __forceinline__ void medium_leaf(const MediumSmem& S, uint32_t ib, uint32_t base,
+                                            uint32_t s, uint32_t n, uint32_t slot, uint32_t depth,
+                                            const float* b, const Params& P, const Out& O,
+                                            uint32_t lane) {
+    warp_store_node(O, slot, b, base + s, n, 0u, lane);
+    for (uint32_t p = lane; p < n; p += 32)
+        O.perm[base + s + p] = __float_as_uint(S.rlo[S.idx[ib][s + p]].w);
+    if (lane == 0 && n > 1) {
+        atomicAdd(&O.ctr->holes, 1u);
+        if (depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+    }
+}
+
+// Warp: stable partition of [s, s+n) from idx[ib] into idx[ib^1] by pred(p);
+// returns the lt count; accumulates child centroid keys.
+template <class Pred>
+__device__ __forceinline__ uint32_t medium_partition(MediumSmem& S, uint32_t ib, uint32_t s,
+                                                     uint32_t n, uint32_t n_lt_expect, uint32_t lane,
+                                                     Pred pred, uint32_t* k /*12*/) {
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t lt_run = 0, gt_run = 0;
+    for (uint32_t b0 = s; b0 < s + n; b0 += 32) {
+        const uint32_t p = b0 + lane;
+        const bool valid = p < s + n;
+        uint32_t r = 0;
+        float c[3] = {0.f, 0.f, 0.f};
+        bool pr = false;
+        if (valid) {
+            r = S.idx[ib][p];
+            const float4 a = S.rlo[r], b = S.rhi[r];
+            c[0] = center_of(a.x, b.x);
+            c[1] = center_of(a.y, b.y);
+            c[2] = center_of(a.z, b.z);
+            pr = pred(p, c);
+        }
+        const uint32_t m = __ballot_sync(kFull, pr);
+        const uint32_t vm = __ballot_sync(kFull, valid);
+        if (valid) {
+            const uint32_t dst = pr ? s + lt_run + __popc(m & below)
+                                    : s + n_lt_expect + gt_run + __popc(vm & ~m & below);
+            if (dst < s + n) S.idx[ib ^ 1u][dst] = static_cast<uint16_t>(r);
+            uint32_t* kk = pr ? k : k + 6;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                kk[a] = min(kk[a], fkey(c[a]));
+                kk[3 + a] = max(kk[3 + a], fkey(c[a]));
+            }
+        }
+        lt_run += __popc(m);
+        gt_run += __popc(vm & ~m);
+    }
+    __syncwarp();
+    return lt_run;
+}
+
+__device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
+#pragma unroll
+    for (int q = 0; q < 12; ++q)
+        k[q] = ((q % 6) < 3) ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+}
+
+__global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
+                                                                const Rec* __restrict__ rec0,
+                                                                const Rec* __restrict__ rec1,
+                                                                Params P, Out O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const Task t = tasks[blockIdx.x];
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+    const uint32_t base = t.start;
+    uint32_t k[12];
+    init_key12(k);
+    if (threadIdx.x < 12) S.rootk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    if (threadIdx.x < 2) S.list_n[threadIdx.x] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) {
+        const Rec r = src[i];
+        S.rlo[i] = r.lo;
+        S.rhi[i] = r.hi;
+        S.idx[0][i] = static_cast<uint16_t>(i);
+        accum_keys(k, r.lo.x, r.lo.y, r.lo.z, r.hi.x, r.hi.y, r.hi.z);
+    }
+    // root centroid bounds (keys 6..11)
+#pragma unroll
+    for (int q = 6; q < 12; ++q) {
+        const bool is_min = q < 9;
+        const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+        if (lane == 0) {
+            if (is_min)
+                atomicMin(&S.rootk[q], v);
+            else
+                atomicMax(&S.rootk[q], v);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        MNode& r = S.list[0][0];
+        for (int a = 0; a < 3; ++a) {
+            r.b[a] = t.lo[a];
+            r.b[3 + a] = t.hi[a];
+            r.cb[a] = funkey(S.rootk[6 + a]);
+            r.cb[3 + a] = funkey(S.rootk[9 + a]);
+        }
+        r.s = 0;
+        r.n = t.len;
+        r.slot = t.slot;
+        r.pair = t.pair;
+        S.list_x[0][0].depth = t.depth;
+        S.list_x[0][0].ib = 0;
+        S.list_n[0] = 1;
+    }
+    uint32_t cur = 0;
+    uint32_t hmax = 0;
+    bool any_split = false;
+    uint32_t n_median = 0;
+    for (;;) {
+        __syncthreads();
+        const uint32_t ncur = S.list_n[cur];
+        if (ncur == 0) break;
+        if (threadIdx.x == 0) S.list_n[cur ^ 1u] = 0;
+        __syncthreads();
+        for (uint32_t li = warp; li < ncur; li += kMediumWarps) {
+            const MNode nd = S.list[cur][li];
+            const MNodeExtra nx = S.list_x[cur][li];
+            const uint32_t s = nd.s, n = nd.n, depth = nx.depth, ib = nx.ib;
+            bool leaf = depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf);
+            Cand win;
+            uint32_t axis = 0, sbin = 0, n_lt = 0;
+            bool median = false;
+            const uint32_t B = P.bins ? P.bins : 32u;
+            float ext[3];
+            bool axis_ok[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                ext[a] = __fsub_rn(nd.cb[3 + a], nd.cb[a]);
+                axis_ok[a] = !(ext[a] == 0.0f);
+            }
+            if (!leaf) {
+                uint32_t* wb = S.bins[warp];
+                init_task_bins(wb, lane, 32);
+                __syncwarp();
+                for (uint32_t p = s + lane; p < s + n; p += 32) {
+                    const uint32_t r = S.idx[ib][p];
+                    const float4 lo = S.rlo[r], hi = S.rhi[r];
+                    const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        if (!axis_ok[a]) continue;
+                        const uint32_t b = bin_of(center_of(l[a], h[a]), nd.cb[a], ext[a], B);
+                        uint32_t* bw = wb + (a * 32 + b) * 7;
+                        atomicAdd(bw, 1u);
+                        atomicMin(bw + 1, fkey(l[0]));
+                        atomicMin(bw + 2, fkey(l[1]));
+                        atomicMin(bw + 3, fkey(l[2]));
+                        atomicMax(bw + 4, fkey(h[0]));
+                        atomicMax(bw + 5, fkey(h[1]));
+                        atomicMax(bw + 6, fkey(h[2]));
+                    }
+                }
+                __syncwarp();
+                uint32_t cnt[3];
+                float box[3][6];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const uint32_t* bw = wb + (a * 32 + lane) * 7;
+                    cnt[a] = bw[0];
+                    for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
+                }
+                Cand best;
+                binned_candidates(cnt, box, axis_ok, B, n, surface_area6(nd.b), P, lane, best);
+                const uint64_t wk = warp_min_key(best.key);
+                const uint32_t wlo = static_cast<uint32_t>(wk);
+                if (wlo == kNoKey) {
+                    if (n > P.max_leaf)
+                        median = true;
+                    else
+                        leaf = true;
+                } else {
+                    axis = (wlo >> 8) & 3u;
+                    sbin = wlo & 0xFFu;
+                    win = best;
+                    shfl_cand(win, sbin);
+                    const float cost = funkey(static_cast<uint32_t>(wk >> 32));
+                    if (n <= P.max_leaf && cost >= leaf_cost(n)) leaf = true;
+                    n_lt = win.n_lt;
+                }
+            }
+            if (leaf) {
+                medium_leaf(S, ib, base, s, n, nd.slot, depth, nd.b, P, O, lane);
+                continue;
+            }
+            uint32_t ck[12];
+            init_key12(ck);
+            uint32_t ob = ib ^ 1u;
+            if (!median) {
+                const float cmin = nd.cb[axis], ex = ext[axis];
+                const uint32_t got = medium_partition(
+                    S, ib, s, n, n_lt, lane,
+                    [&](uint32_t, const float* c) {
+                        return bin_of(c[axis], cmin, ex, B) < sbin;
+                    },
+                    ck);
+                if (got != n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
+            } else {
+                // median_split on axes 0, 1, 2 over the same list (bvh/src/lib.rs:444-491,
+                // 528-530): stable selection of the n/2 smallest centroid keys.
+                const uint32_t m = n / 2u;
+                uint32_t cb = ib;
+                uint32_t best_ck = 0;
+                for (uint32_t a = 0; a < 3; ++a) {
+                    uint32_t dummy[12];
+                    init_key12(dummy);
+                    medium_partition(
+                        S, cb, s, n, m, lane,
+                        [&](uint32_t p, const float* c) {
+                            const uint32_t key = fkey(c[a]);
+                            uint32_t rank = 0;
+                            for (uint32_t q = s; q < s + n; ++q) {
+                                const uint32_t r = S.idx[cb][q];
+                                const uint32_t kq = fkey(center_of(
+                                    a == 0 ? S.rlo[r].x : (a == 1 ? S.rlo[r].y : S.rlo[r].z),
+                                    a == 0 ? S.rhi[r].x : (a == 1 ? S.rhi[r].y : S.rhi[r].z)));
+                                rank += (kq < key || (kq == key && q < p)) ? 1u : 0u;
+                            }
+                            return rank < m;
+                        },
+                        dummy);
+                    cb ^= 1u;
+                    float blt[6], bgt[6];
+                    box_empty(blt);
+                    box_empty(bgt);
+                    for (uint32_t p = s + lane; p < s + n; p += 32) {
+                        const uint32_t r = S.idx[cb][p];
+                        const float4 lo = S.rlo[r], hi = S.rhi[r];
+                        box_grow(p < s + m ? blt : bgt, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z);
+                    }
+                    for (int i = 0; i < 3; ++i) {
+                        blt[i] = funkey(__reduce_min_sync(kFull, fkey(blt[i])));
+                        bgt[i] = funkey(__reduce_min_sync(kFull, fkey(bgt[i])));
+                        blt[3 + i] = funkey(__reduce_max_sync(kFull, fkey(blt[3 + i])));
+                        bgt[3 + i] = funkey(__reduce_max_sync(kFull, fkey(bgt[3 + i])));
+                    }
+                    const float cost = split_cost(surface_area6(blt), surface_area6(bgt),
+                                                  surface_area6(nd.b), m, n - m);
+                    const uint32_t key = fkey(cost);
+                    if (a == 0 || key < best_ck) {
+                        best_ck = key;
+                        for (int i = 0; i < 6; ++i) {
+                            win.lt[i] = blt[i];
+                            win.gt[i] = bgt[i];
+                        }
+                    }
+                }
+                ob = cb;
+                n_lt = m;
+                n_median++;
+                for (uint32_t p = s + lane; p < s + n; p += 32) {
+                    const uint32_t r = S.idx[ob][p];
+                    const float4 lo = S.rlo[r], hi = S.rhi[r];
+                    const float c[3] = {center_of(lo.x, hi.x), center_of(lo.y, hi.y), center_of(lo.z, hi.z)};
+                    uint32_t* kk = p < s + m ? ck : ck + 6;
+                    for (int a = 0; a < 3; ++a) {
+                        kk[a] = min(kk[a], fkey(c[a]));
+                        kk[3 + a] = max(kk[3 + a], fkey(c[a]));
+                    }
+                }
+            }
+            // containment of centroids in child bounds (bvh/src/lib.rs:637-646)
+            bool bad = false;
+            for (uint32_t p = s + lane; p < s + n; p += 32) {
+                const uint32_t r = S.idx[ob][p];
+                const float4 lo = S.rlo[r], hi = S.rhi[r];
+                bad |= !box_contains(p < s + n_lt ? win.lt : win.gt, center_of(lo.x, hi.x),
+                                     center_of(lo.y, hi.y), center_of(lo.z, hi.z));
+            }
+            if (__any_sync(kFull, bad) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+            warp_reduce_keys12(ck);
+            warp_store_node(O, nd.slot, nd.b, base + s, n, nd.pair, lane);
+            any_split = true;
+            hmax = max(hmax, depth);
+            const uint32_t n_gt = n - n_lt;
+            for (int c = 0; c < 2; ++c) {
+                const uint32_t len = c == 0 ? n_gt : n_lt;
+                const uint32_t cs = c == 0 ? s + n_lt : s;
+                const uint32_t slot = c == 0 ? nd.pair : nd.pair + 1u;
+                const uint32_t pair = c == 0 ? nd.pair + 2u : nd.pair + 2u * n_gt;
+                const uint32_t cdepth = depth + 1u;
+                const float* cbx = c == 0 ? win.gt : win.lt;
+                const uint32_t* cck = c == 0 ? ck + 6 : ck;
+                const bool cleaf =
+                    len <= 1u || cdepth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
+                if (cleaf) {
+                    medium_leaf(S, ob, base, cs, len, slot, cdepth, cbx, P, O, lane);
+                } else if (len > kSmallMax) {
+                    uint32_t li2 = 0;
+                    if (lane == 0) li2 = atomicAdd(&S.list_n[cur ^ 1u], 1u);
+                    li2 = __shfl_sync(kFull, li2, 0);
+                    if (lane == 0) {
+                        MNode& q = S.list[cur ^ 1u][li2];
+                        for (int i = 0; i < 6; ++i) {
+                            q.b[i] = cbx[i];
+                            q.cb[i] = funkey(cck[i]);
+                        }
+                        q.s = cs;
+                        q.n = len;
+                        q.slot = slot;
+                        q.pair = pair;
+                        S.list_x[cur ^ 1u][li2].depth = cdepth;
+                        S.list_x[cur ^ 1u][li2].ib = ob;
+                    }
+                } else {
+                    float lo[3], hi[3];
+                    uint32_t id;
+                    medium_load_warp_records(S, ob, cs, len, lane, lo, hi, id);
+                    warp_build_subtree(lo, hi, id, len, base + cs, slot, pair, cdepth, cbx, P, O,
+                                       S.xchg[warp]);
+                }
+            }
+        }
+        cur ^= 1u;
+    }
+    if (lane == 0) {
+        if (any_split) atomicMax(&O.ctr->height, hmax);
+        if (n_median) atomicAdd(&O.ctr->median_splits, n_median);
+    }
+}
+
+// ---------------------------------------------------------------- small
+
+__global__ void __launch_bounds__(256) small_kernel(const Task* __restrict__ tasks, uint32_t n_tasks,
+                                                   const Rec* __restrict__ rec0,
+                                                   const Rec* __restrict__ rec1, Params P, Out O) {
+    __shared__ XRec xchg[8][32];
+    const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+    const uint32_t w = blockIdx.x * 8 + wib;
+    if (w >= n_tasks) return;
+    const Task t = tasks[w];
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+    float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+    uint32_t id = 0;
+    if (lane < t.len) {
+        const Rec r = src[lane];
+        lo[0] = r.lo.x;
+        lo[1] = r.lo.y;
+        lo[2] = r.lo.z;
+        id = __float_as_uint(r.lo.w);
+        hi[0] = r.hi.x;
+        hi[1] = r.hi.y;
+        hi[2] = r.hi.z;
+    }
+    const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O, xchg[wib]);
+}
+
+// ---------------------------------------------------------------- compaction
+
+__global__ void widen_used_kernel(const uint8_t* __restrict__ used, uint32_t n, uint32_t* __restrict__ out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = used[i];
+}
+
+__global__ void compact_kernel(const mgbvh_node* __restrict__ src, const uint32_t* __restrict__ lens,
+                               const uint8_t* __restrict__ used, const uint32_t* __restrict__ newidx,
+                               uint32_t cap, mgbvh_node* __restrict__ dst, uint32_t* dst_lens) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < cap; s += gridDim.x * blockDim.x) {
+        if (!used[s]) continue;
+        mgbvh_node nd = src[s];
+        if (nd.child_node) nd.child_node = newidx[nd.child_node];
+        const uint32_t d = newidx[s];
+        dst[d] = nd;
+        if (dst_lens) dst_lens[d] = lens[s];
+    }
+}
+
+}  // namespace mgbvh
+
+// =================================================================== host
+
+using namespace mgbvh;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct mgbvh_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    DevBuf rec[2], tasks[2], bins[2], cbkeys[2], tile_task[2], tile_begin[2];
+    DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
+    DevBuf in_a, in_b, out_nodes, out_lens;
+    Counters* h_ctr = nullptr;
+};
+
+namespace {
+
+int fail(mgbvh_ctx* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return status;
+}
+
+#define MG_CUDA(call)                                                                      \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail(ctx, MGBVH_ERR_CUDA,                                               \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));               \
+    } while (0)
+
+int ensure(mgbvh_ctx* ctx, DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (b.bytes >= bytes) return MGBVH_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    const size_t want = bytes + bytes / 8;
+    MG_CUDA(cudaMalloc(&b.p, want));
+    b.bytes = want;
+    return MGBVH_OK;
+}
+
+template <class T>
+T* P_(DevBuf& b) {
+    return reinterpret_cast<T*>(b.p);
+}
+
+struct Caps {
+    uint32_t tasks, tiles, medium, small, nodes;
+};
+
+Caps caps_for(uint32_t n) {
+    Caps c;
+    c.tasks = n / (kMediumMax + 1) + 2;
+    c.tiles = n / kTile + c.tasks + 2;
+    c.medium = 4 * (n / kMediumMax) + 8;
+    c.small = c.medium;
+    c.nodes = 2 * n - 1;
+    return c;
+}
+
+int validate_settings(mgbvh_ctx* ctx, const mgbvh_settings* s) {
+    if (!s) return fail(ctx, MGBVH_ERR_INVALID_ARG, "settings is NULL");
+    if (s->min_leaf_objects < 1 || s->max_leaf_objects < 1)
+        return fail(ctx, MGBVH_ERR_INVALID_ARG, "min/max leaf objects must be >= 1");
+    if (s->min_leaf_objects > (1u << 30))
+        return fail(ctx, MGBVH_ERR_INVALID_ARG, "min leaf objects too large");
+    if (s->bins == 1 || s->bins > kMaxBins)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "bins must be 0 (reference) or 2..32");
+    if (s->adaptive_max_n > kSmallMax)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "adaptive_max_n must be <= 32");
+    if (s->adaptive_steps > 32)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "adaptive_steps must be 0 (reference) or 1..32");
+    return MGBVH_OK;
+}
+
+enum InputKind { kIndexed, kAabbs };
+
+struct Input {
+    InputKind kind;
+    const float* verts;
+    uint32_t stride_bytes;
+    uint32_t nverts;
+    const uint32_t* tris;
+    const float* aabbs;
+    uint32_t n;
+};
+
+const char* site_text(uint32_t site) {
+    switch (site) {
+        case kSiteIndex: return "a triangle index is past the vertex count";
+        case kSiteCount: return "partition count differs from the split's count (bvh/src/lib.rs:621-634)";
+        case kSiteContain: return "a centroid lies outside its child's bounds (bvh/src/lib.rs:637-646)";
+        case kSiteLargeMedian:
+            return "forced median split on a node above 1024 objects is not built (no binned split "
+                   "passed the MIN_LEAF_OBJECTS filter)";
+        case kSiteCapacity: return "internal task list overflow";
+        default: return "device error";
+    }
+}
+
+// Runs a build whose inputs are device-resident. Outputs go to device memory:
+// d_nodes (capacity cap), d_lens (nullable), d_perm. Returns status.
+int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_node* d_nodes,
+              uint32_t cap, uint32_t* d_lens, uint32_t* d_perm, uint32_t* out_count,
+              mgbvh_stats* stats) {
+    const uint32_t n = in.n;
+    const cudaStream_t sm = ctx->stream;
+    if (n > 0x7FFFFFFFu) return fail(ctx, MGBVH_ERR_UNSUPPORTED, "more than 2^31-1 objects");
+    const Caps C = caps_for(n);
+    int rc;
+#define ENS(buf, bytes) \
+    if ((rc = ensure(ctx, buf, (bytes))) != MGBVH_OK) return rc
+    ENS(ctx->rec[0], sizeof(Rec) * (size_t)n);
+    ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
+    for (int i = 0; i < 2; ++i) {
+        ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
+        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
+        ENS(ctx->cbkeys[i], 24ull * C.tasks);
+        ENS(ctx->tile_task[i], 4ull * C.tiles);
+        ENS(ctx->tile_begin[i], 4ull * C.tiles);
+    }
+    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);
+    ENS(ctx->tile_lt, 4ull * C.tiles);
+    ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
+    ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
+    ENS(ctx->small, sizeof(Task) * (size_t)C.small);
+    ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
+    ENS(ctx->lens, 4ull * C.nodes);
+    ENS(ctx->used, (size_t)C.nodes);
+    ENS(ctx->ctr, sizeof(Counters));
+#undef ENS
+    Params P;
+    P.min_leaf = st->min_leaf_objects;
+    P.max_leaf = st->max_leaf_objects;
+    P.max_depth = st->max_depth;
+    P.bins = st->bins;
+    P.adaptive_max_n = st->adaptive_max_n;
+    P.adaptive_steps = st->adaptive_steps;
+
+    Counters init;
+    std::memset(&init, 0, sizeof(init));
+    for (int i = 0; i < 12; ++i) init.root_keys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    Counters* d_ctr = P_<Counters>(ctx->ctr);
+    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
+
+    Out O;
+    O.nodes = P_<mgbvh_node>(ctx->nodes);
+    O.lens = P_<uint32_t>(ctx->lens);
+    O.used = P_<uint8_t>(ctx->used);
+    O.perm = d_perm;
+    O.ctr = d_ctr;
+    O.node_cap = C.nodes;
+    Rec* rec0 = P_<Rec>(ctx->rec[0]);
+    Rec* rec1 = P_<Rec>(ctx->rec[1]);
+
+    MG_CUDA(cudaEventRecord(ctx->ev0, sm));
+    const int prep_blocks = (int)std::min<uint32_t>((n + 255) / 256, 148u * 8u);
+    if (in.kind == kIndexed)
+        prep_indexed_kernel<<<prep_blocks, 256, 0, sm>>>(in.verts, in.stride_bytes / 4, in.nverts,
+                                                          in.tris, n, rec0, d_ctr);
+    else
+        prep_aabbs_kernel<<<prep_blocks, 256, 0, sm>>>(in.aabbs, n, rec0, d_ctr);
+
+    const bool root_leaf = n <= 1 || st->max_depth == 0 ||
+                           (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
+    const uint32_t cls = root_leaf ? 0u : (n <= kSmallMax ? 1u : (n <= kMediumMax ? 2u : 3u));
+    const uint32_t ntiles0 = (n + kTile - 1) / kTile;
+    const float* bb = st->bounds;
+    {
+        const int blocks = (int)std::min<uint32_t>((std::max(n, ntiles0) + 255) / 256 + 1, 1024u);
+        init_root_kernel<<<blocks, 256, 0, sm>>>(
+            n, cls, st->has_bounds, bb[0], bb[1], bb[2], bb[3], bb[4], bb[5], P_<Task>(ctx->tasks[0]),
+            P_<uint32_t>(ctx->bins[0]), P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]),
+            P_<uint32_t>(ctx->tile_begin[0]), P_<Task>(ctx->medium), P_<Task>(ctx->small), O, ntiles0,
+            st->max_depth);
+    }
+    MG_CUDA(cudaGetLastError());
+
+    uint32_t n_tasks = cls == 3 ? 1u : 0u, n_tiles = ntiles0;
+    uint32_t cur = 0;
+    while (n_tasks > 0) {
+        const uint32_t nx = cur ^ 1u;
+        lvl_bin_kernel<<<n_tiles, kTileThreads, 0, sm>>>(
+            P_<Task>(ctx->tasks[cur]), P_<uint32_t>(ctx->cbkeys[cur]), P_<uint32_t>(ctx->bins[cur]),
+            P_<uint32_t>(ctx->tile_task[cur]), P_<uint32_t>(ctx->tile_begin[cur]),
+            P_<uint32_t>(ctx->tile_hist), rec0, rec1, P);
+        MG_CUDA(cudaMemsetAsync(&d_ctr->n_next_large, 0, 8, sm));
+        EvalArgs A;
+        A.tasks = P_<Task>(ctx->tasks[cur]);
+        A.n_tasks = n_tasks;
+        A.bins = P_<uint32_t>(ctx->bins[cur]);
+        A.cbkeys = P_<uint32_t>(ctx->cbkeys[cur]);
+        A.tile_hist = P_<uint32_t>(ctx->tile_hist);
+        A.tile_lt = P_<uint32_t>(ctx->tile_lt);
+        A.dec = P_<Decision>(ctx->dec);
+        A.next_tasks = P_<Task>(ctx->tasks[nx]);
+        A.next_bins = P_<uint32_t>(ctx->bins[nx]);
+        A.next_cbkeys = P_<uint32_t>(ctx->cbkeys[nx]);
+        A.next_tile_task = P_<uint32_t>(ctx->tile_task[nx]);
+        A.next_tile_begin = P_<uint32_t>(ctx->tile_begin[nx]);
+        A.medium = P_<Task>(ctx->medium);
+        A.small = P_<Task>(ctx->small);
+        A.cap_tasks = C.tasks;
+        A.cap_tiles = C.tiles;
+        A.cap_medium = C.medium;
+        A.cap_small = C.small;
+        lvl_eval_kernel<<<(n_tasks + 3) / 4, 128, 0, sm>>>(A, P, O);
+        lvl_part_kernel<<<n_tiles, kTileThreads, 0, sm>>>(
+            P_<Task>(ctx->tasks[cur]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[cur]),
+            P_<uint32_t>(ctx->tile_begin[cur]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
+            P_<uint32_t>(ctx->cbkeys[nx]), O);
+        MG_CUDA(cudaGetLastError());
+        MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        if (ctx->h_ctr->error) break;
+        n_tasks = ctx->h_ctr->n_next_large;
+        n_tiles = ctx->h_ctr->n_next_tiles;
+        cur = nx;
+    }
+    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaStreamSynchronize(sm));
+    if (!ctx->h_ctr->error) {
+        const uint32_t n_medium = ctx->h_ctr->n_medium, n_small = ctx->h_ctr->n_small;
+        if (n_medium > 0)
+            medium_kernel<<<n_medium, kMediumThreads, sizeof(MediumSmem), sm>>>(P_<Task>(ctx->medium),
+                                                                                 rec0, rec1, P, O);
+        if (n_small > 0)
+            small_kernel<<<(n_small + 7) / 8, 256, 0, sm>>>(P_<Task>(ctx->small), n_small, rec0, rec1,
+                                                             P, O);
+        MG_CUDA(cudaGetLastError());
+    }
+    MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaStreamSynchronize(sm));
+    const Counters hc = *ctx->h_ctr;
+    if (hc.error) {
+        return fail(ctx, (int)hc.error, site_text(hc.error_site));
+    }
+    float ms = 0.0f;
+    MG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+
+    // node count and compaction
+    uint32_t count = C.nodes;
+    if (hc.holes > 0) {
+        if ((rc = ensure(ctx, ctx->newidx, 4ull * C.nodes)) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->widened, 4ull * C.nodes)) != MGBVH_OK) return rc;
+        widen_used_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
+            P_<uint8_t>(ctx->used), C.nodes, P_<uint32_t>(ctx->widened));
+        size_t tmp = 0;
+        MG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, P_<uint32_t>(ctx->widened),
+                                              P_<uint32_t>(ctx->newidx), C.nodes, sm));
+        if ((rc = ensure(ctx, ctx->cub_tmp, tmp)) != MGBVH_OK) return rc;
+        MG_CUDA(cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp, P_<uint32_t>(ctx->widened),
+                                              P_<uint32_t>(ctx->newidx), C.nodes, sm));
+        uint32_t last_idx = 0;
+        uint8_t last_used = 0;
+        MG_CUDA(cudaMemcpyAsync(&last_idx, P_<uint32_t>(ctx->newidx) + (C.nodes - 1), 4,
+                                cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaMemcpyAsync(&last_used, P_<uint8_t>(ctx->used) + (C.nodes - 1), 1,
+                                cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        count = last_idx + last_used;
+        if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
+        compact_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
+            P_<mgbvh_node>(ctx->nodes), P_<uint32_t>(ctx->lens), P_<uint8_t>(ctx->used),
+            P_<uint32_t>(ctx->newidx), C.nodes, d_nodes, d_lens);
+        MG_CUDA(cudaGetLastError());
+    } else {
+        if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
+        MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
+                                cudaMemcpyDeviceToDevice, sm));
+        if (d_lens)
+            MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * count, cudaMemcpyDeviceToDevice, sm));
+    }
+    MG_CUDA(cudaStreamSynchronize(sm));
+    *out_count = count;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->construction_time = ms * 1e-3;
+        stats->node_count = count;
+        stats->total_object_count = n;
+        stats->height = hc.height;
+        stats->max_depth = st->max_depth;
+        stats->median_splits = hc.median_splits;
+        stats->depth_capped_leaves = hc.depth_capped;
+        const uint32_t MINs = st->min_leaf_objects, MAXs = st->max_leaf_objects;
+        stats->feasible = (MINs == MAXs) ? (n % MINs == 0) : (MAXs >= 2 * MINs - 1);
+        if (st->profiling_info) {
+            // leaf statistics as bvh/src/lib.rs:769-788 computes them
+            std::vector<mgbvh_node> hn(count);
+            std::vector<uint32_t> hl(count);
+            MG_CUDA(cudaMemcpy(hn.data(), d_nodes, sizeof(mgbvh_node) * (size_t)count,
+                               cudaMemcpyDeviceToHost));
+            const uint32_t* lens_src = d_lens ? d_lens : nullptr;
+            if (lens_src) {
+                MG_CUDA(cudaMemcpy(hl.data(), lens_src, 4ull * count, cudaMemcpyDeviceToHost));
+            } else if (hc.holes == 0) {
+                MG_CUDA(cudaMemcpy(hl.data(), ctx->lens.p, 4ull * count, cudaMemcpyDeviceToHost));
+            } else {
+                // compacted lens were not requested: compact again into scratch
+                if ((rc = ensure(ctx, ctx->out_lens, 4ull * count)) != MGBVH_OK) return rc;
+                if ((rc = ensure(ctx, ctx->out_nodes, sizeof(mgbvh_node) * (size_t)count)) != MGBVH_OK)
+                    return rc;
+                compact_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
+                    P_<mgbvh_node>(ctx->nodes), P_<uint32_t>(ctx->lens), P_<uint8_t>(ctx->used),
+                    P_<uint32_t>(ctx->newidx), C.nodes, P_<mgbvh_node>(ctx->out_nodes),
+                    P_<uint32_t>(ctx->out_lens));
+                MG_CUDA(cudaStreamSynchronize(sm));
+                MG_CUDA(cudaMemcpy(hl.data(), ctx->out_lens.p, 4ull * count, cudaMemcpyDeviceToHost));
+            }
+            std::vector<uint32_t> leaf;
+            for (uint32_t i = 1; i < count; ++i)
+                if (hn[i].child_node == 0) leaf.push_back(hl[i]);
+            stats->leaf_node_count = (uint32_t)leaf.size();
+            stats->min_leaf_object_count = leaf.empty() ? n : *std::min_element(leaf.begin(), leaf.end());
+            stats->max_leaf_object_count = leaf.empty() ? n : *std::max_element(leaf.begin(), leaf.end());
+            uint32_t sum = 0;
+            for (uint32_t l : leaf) sum += l;
+            const double avg = (double)sum / (double)leaf.size();
+            double var = 0.0;
+            for (uint32_t l : leaf) var += ((double)l - avg) * ((double)l - avg);
+            stats->avg_leaf_object_count = avg;
+            stats->stddev_leaf_object_count = std::sqrt(var / (double)leaf.size());
+        }
+    }
+    const uint32_t MIN = st->min_leaf_objects, MAX = st->max_leaf_objects;
+    const bool feasible = (MIN == MAX) ? (n % MIN == 0) : (MAX >= 2 * MIN - 1);  // :710-714
+    return feasible ? MGBVH_OK : MGBVH_WARN_INFEASIBLE;
+}
+
+int check_ctx(mgbvh_ctx* ctx) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return fail(ctx, MGBVH_ERR_CUDA, cudaGetErrorString(e));
+    return MGBVH_OK;
+}
+
+int build_common(mgbvh_ctx* ctx, const Input& in_dev, const mgbvh_settings* s, mgbvh_node* d_nodes,
+                 uint32_t cap, uint32_t* out_count, uint32_t* d_lens, uint32_t* d_perm,
+                 mgbvh_stats* stats) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if ((rc = validate_settings(ctx, s)) != MGBVH_OK) return rc;
+    if (!out_count) return fail(ctx, MGBVH_ERR_INVALID_ARG, "out_node_count is NULL");
+    *out_count = 0;
+    if (in_dev.n == 0) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return MGBVH_WARN_EMPTY;
+    }
+    if (!d_nodes || !d_perm) return fail(ctx, MGBVH_ERR_INVALID_ARG, "output pointer is NULL");
+    return run_build(ctx, in_dev, s, d_nodes, cap, d_lens, d_perm, out_count, stats);
+}
+
+// Host-pointer builds: copy inputs in, build into scratch, copy results out.
+int build_host(mgbvh_ctx* ctx, Input in, const mgbvh_settings* s, mgbvh_node* out_nodes, uint32_t cap,
+               uint32_t* out_count, uint32_t* out_lens, uint32_t* out_perm, mgbvh_stats* stats) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if ((rc = validate_settings(ctx, s)) != MGBVH_OK) return rc;
+    if (!out_count) return fail(ctx, MGBVH_ERR_INVALID_ARG, "out_node_count is NULL");
+    *out_count = 0;
+    if (in.n == 0) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return MGBVH_WARN_EMPTY;
+    }
+    if (!out_nodes || !out_perm) return fail(ctx, MGBVH_ERR_INVALID_ARG, "output pointer is NULL");
+    const cudaStream_t sm = ctx->stream;
+    Input d = in;
+    if (in.kind == kIndexed) {
+        if ((rc = ensure(ctx, ctx->in_a, (size_t)in.nverts * in.stride_bytes))) return rc;
+        if ((rc = ensure(ctx, ctx->in_b, 12ull * in.n))) return rc;
+        MG_CUDA(cudaMemcpyAsync(ctx->in_a.p, in.verts, (size_t)in.nverts * in.stride_bytes,
+                                cudaMemcpyHostToDevice, sm));
+        MG_CUDA(cudaMemcpyAsync(ctx->in_b.p, in.tris, 12ull * in.n, cudaMemcpyHostToDevice, sm));
+        d.verts = P_<float>(ctx->in_a);
+        d.tris = P_<uint32_t>(ctx->in_b);
+    } else {
+        if ((rc = ensure(ctx, ctx->in_a, 24ull * in.n))) return rc;
+        MG_CUDA(cudaMemcpyAsync(ctx->in_a.p, in.aabbs, 24ull * in.n, cudaMemcpyHostToDevice, sm));
+        d.aabbs = P_<float>(ctx->in_a);
+    }
+    const uint32_t full = 2 * in.n - 1;
+    if ((rc = ensure(ctx, ctx->out_nodes, sizeof(mgbvh_node) * (size_t)full))) return rc;
+    if ((rc = ensure(ctx, ctx->out_lens, 4ull * full))) return rc;
+    if ((rc = ensure(ctx, ctx->perm, 4ull * in.n))) return rc;
+    uint32_t count = 0;
+    rc = run_build(ctx, d, s, P_<mgbvh_node>(ctx->out_nodes), full, P_<uint32_t>(ctx->out_lens),
+                   P_<uint32_t>(ctx->perm), &count, stats);
+    if (rc < 0) return rc;
+    if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
+    MG_CUDA(cudaMemcpyAsync(out_nodes, ctx->out_nodes.p, sizeof(mgbvh_node) * (size_t)count,
+                            cudaMemcpyDeviceToHost, sm));
+    if (out_lens)
+        MG_CUDA(cudaMemcpyAsync(out_lens, ctx->out_lens.p, 4ull * count, cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaMemcpyAsync(out_perm, ctx->perm.p, 4ull * in.n, cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaStreamSynchronize(sm));
+    *out_count = count;
+    return rc;
+}
+
+Input make_indexed(const float* v, uint32_t stride, uint32_t nv, const uint32_t* t, uint32_t n) {
+    Input in;
+    in.kind = kIndexed;
+    in.verts = v;
+    in.stride_bytes = stride;
+    in.nverts = nv;
+    in.tris = t;
+    in.aabbs = nullptr;
+    in.n = n;
+    return in;
+}
+
+Input make_aabbs(const float* a, uint32_t n) {
+    Input in;
+    in.kind = kAabbs;
+    in.verts = nullptr;
+    in.stride_bytes = 0;
+    in.nverts = 0;
+    in.tris = nullptr;
+    in.aabbs = a;
+    in.n = n;
+    return in;
+}
+
+int check_indexed_args(mgbvh_ctx* ctx, const float* v, uint32_t stride, const uint32_t* t, uint32_t n) {
+    if (n == 0) return MGBVH_OK;
+    if (!v || !t) return fail(ctx, MGBVH_ERR_INVALID_ARG, "vertices/triangles pointer is NULL");
+    if (stride < 12 || stride % 4) return fail(ctx, MGBVH_ERR_INVALID_ARG, "vertex stride must be >= 12 and a multiple of 4");
+    return MGBVH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void mgbvh_default_settings(mgbvh_settings* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    s->min_leaf_objects = 1;
+    s->max_leaf_objects = 1;
+    s->max_depth = 32;
+    s->has_bounds = 0;
+    s->bins = 0;
+    s->adaptive_max_n = 32;
+    s->adaptive_steps = 0;
+    s->profiling_info = 0;
+}
+
+int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
+    if (!out_ctx) return MGBVH_ERR_INVALID_ARG;
+    *out_ctx = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return MGBVH_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return MGBVH_ERR_INVALID_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    mgbvh_ctx* ctx = new mgbvh_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
+        cudaFuncSetAttribute(medium_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmem)) != cudaSuccess) {
+        mgbvh_destroy(ctx);
+        return MGBVH_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+    *out_ctx = ctx;
+    return MGBVH_OK;
+}
+
+void mgbvh_destroy(mgbvh_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    DevBuf* all[] = {&ctx->rec[0], &ctx->rec[1], &ctx->tasks[0], &ctx->tasks[1], &ctx->bins[0],
+                     &ctx->bins[1], &ctx->cbkeys[0], &ctx->cbkeys[1], &ctx->tile_task[0],
+                     &ctx->tile_task[1], &ctx->tile_begin[0], &ctx->tile_begin[1], &ctx->tile_hist,
+                     &ctx->tile_lt, &ctx->dec, &ctx->medium, &ctx->small, &ctx->nodes, &ctx->lens,
+                     &ctx->used, &ctx->newidx, &ctx->widened, &ctx->perm, &ctx->ctr, &ctx->cub_tmp, &ctx->in_a,
+                     &ctx->in_b, &ctx->out_nodes, &ctx->out_lens};
+    for (DevBuf* b : all)
+        if (b->p) cudaFree(b->p);
+    if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int mgbvh_set_stream(mgbvh_ctx* ctx, void* stream) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (stream) {
+        ctx->stream = reinterpret_cast<cudaStream_t>(stream);
+        ctx->own_stream = false;
+    } else {
+        cudaSetDevice(ctx->device);
+        if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return MGBVH_ERR_CUDA;
+        ctx->own_stream = true;
+    }
+    return MGBVH_OK;
+}
+
+const char* mgbvh_last_error(const mgbvh_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+const char* mgbvh_status_string(int status) {
+    switch (status) {
+        case MGBVH_OK: return "ok";
+        case MGBVH_WARN_EMPTY: return "empty object list: empty hierarchy";
+        case MGBVH_WARN_INFEASIBLE: return "leaf-size bounds infeasible for this object count";
+        case MGBVH_ERR_INVALID_ARG: return "invalid argument";
+        case MGBVH_ERR_CAPACITY: return "output capacity too small";
+        case MGBVH_ERR_CUDA: return "CUDA error";
+        case MGBVH_ERR_TIMEOUT: return "device wait timed out";
+        case MGBVH_ERR_ASSERT: return "reference assertion would fail";
+        case MGBVH_ERR_UNSUPPORTED: return "unsupported";
+        case MGBVH_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int mgbvh_build_indexed(mgbvh_ctx* ctx, const float* vertices, uint32_t vertex_stride_bytes,
+                        uint32_t vertex_count, const uint32_t* triangles, uint32_t triangle_count,
+                        const mgbvh_settings* settings, mgbvh_node* out_nodes, uint32_t node_capacity,
+                        uint32_t* out_node_count, uint32_t* out_lens, uint32_t* out_perm,
+                        mgbvh_stats* out_stats) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    int rc = check_indexed_args(ctx, vertices, vertex_stride_bytes, triangles, triangle_count);
+    if (rc) return rc;
+    return build_host(ctx, make_indexed(vertices, vertex_stride_bytes, vertex_count, triangles, triangle_count),
+                      settings, out_nodes, node_capacity, out_node_count, out_lens, out_perm, out_stats);
+}
+
+int mgbvh_build_aabbs(mgbvh_ctx* ctx, const float* aabbs, uint32_t count, const mgbvh_settings* settings,
+                      mgbvh_node* out_nodes, uint32_t node_capacity, uint32_t* out_node_count,
+                      uint32_t* out_lens, uint32_t* out_perm, mgbvh_stats* out_stats) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (count && !aabbs) return fail(ctx, MGBVH_ERR_INVALID_ARG, "aabbs pointer is NULL");
+    return build_host(ctx, make_aabbs(aabbs, count), settings, out_nodes, node_capacity, out_node_count,
+                      out_lens, out_perm, out_stats);
+}
+
+int mgbvh_build_indexed_dev(mgbvh_ctx* ctx, const float* d_vertices, uint32_t vertex_stride_bytes,
+                            uint32_t vertex_count, const uint32_t* d_triangles, uint32_t triangle_count,
+                            const mgbvh_settings* settings, mgbvh_node* d_out_nodes,
+                            uint32_t node_capacity, uint32_t* out_node_count, uint32_t* d_out_lens,
+                            uint32_t* d_out_perm, mgbvh_stats* out_stats) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    int rc = check_indexed_args(ctx, d_vertices, vertex_stride_bytes, d_triangles, triangle_count);
+    if (rc) return rc;
+    return build_common(ctx, make_indexed(d_vertices, vertex_stride_bytes, vertex_count, d_triangles, triangle_count),
+                        settings, d_out_nodes, node_capacity, out_node_count, d_out_lens, d_out_perm,
+                        out_stats);
+}
+
+int mgbvh_build_aabbs_dev(mgbvh_ctx* ctx, const float* d_aabbs, uint32_t count,
+                          const mgbvh_settings* settings, mgbvh_node* d_out_nodes, uint32_t node_capacity,
+                          uint32_t* out_node_count, uint32_t* d_out_lens, uint32_t* d_out_perm,
+                          mgbvh_stats* out_stats) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (count && !d_aabbs) return fail(ctx, MGBVH_ERR_INVALID_ARG, "aabbs pointer is NULL");
+    return build_common(ctx, make_aabbs(d_aabbs, count), settings, d_out_nodes, node_capacity,
+                        out_node_count, d_out_lens, d_out_perm, out_stats);
+}
+
+int mgbvh_encode_gpu_bytes(const mgbvh_node* nodes, const uint32_t* lens, uint32_t count,
+                           uint32_t max_leaf_objects, uint32_t* out_words) {
+    if ((count && (!nodes || !out_words)) || max_leaf_objects < 1) return MGBVH_ERR_INVALID_ARG;
+    if (max_leaf_objects == 1) {
+        std::memcpy(out_words, nodes, sizeof(mgbvh_node) * (size_t)count);
+        return MGBVH_OK;
+    }
+    if (!lens) return MGBVH_ERR_INVALID_ARG;
+    // bvh/src/lib.rs:170-195
+    uint64_t overflow = 1;
+    while (overflow < max_leaf_objects) overflow <<= 1;  // next_power_of_two
+    uint32_t len_bits = 0;
+    while ((1ull << (len_bits + 1)) <= overflow) ++len_bits;  // ilog2
+    if (len_bits >= 32) return MGBVH_ERR_ASSERT;
+    const uint32_t child_bits = 32 - len_bits;
+    const uint32_t len_mask = (1u << len_bits) - 1u;
+    const uint32_t child_mask = ~len_mask;
+    for (uint32_t i = 0; i < count; ++i) {
+        const mgbvh_node& nd = nodes[i];
+        if (nd.child_node == 0 && lens[i] >= overflow) return MGBVH_ERR_ASSERT;
+        uint32_t* w = out_words + 8ull * i;
+        std::memcpy(w, &nd, 28);
+        const uint32_t packed = (child_bits >= 32 ? 0u : ((lens[i] & len_mask) << child_bits)) |
+                                (nd.child_node & child_mask);
+        w[7] = packed;
+    }
+    return MGBVH_OK;
+}
+
+double mgbvh_sah_cost(const mgbvh_node* nodes, const uint32_t* lens, uint32_t count) {
+    if (!nodes || !lens || count == 0) return 0.0;
+    auto sa = [](const mgbvh_node& n) {
+        const double w = (double)n.max[0] - n.min[0], h = (double)n.max[1] - n.min[1],
+                     d = (double)n.max[2] - n.min[2];
+        if (w < 0 || h < 0 || d < 0) return 0.0;
+        return 2.0 * (w * h + w * d + h * d);
+    };
+    const double root = sa(nodes[0]);
+    if (!(root > 0.0)) return 0.0;
+    double c = 0.0;
+    for (uint32_t i = 0; i < count; ++i) {
+        const double r = sa(nodes[i]) / root;
+        c += nodes[i].child_node ? (double)kDepthCost * r : (double)kObjectCost * lens[i] * r;
+    }
+    return c;
+}
+
+}  // extern "C"

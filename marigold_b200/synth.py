@@ -1,0 +1,198 @@
+"""Seeded synthetic inputs for the builder: meshes, scenes and rays.
+
+Every generator is counter based (one hash per element, no sequential RNG
+state), so any slice of a workload can be regenerated on its own and the
+same seed gives the same f32 data on every host. Only IEEE-exact float64
+operations are used (add, multiply, divide, sqrt, floor); sine and cosine are
+evaluated by a fixed Taylor polynomial, so no platform libm enters the data.
+Negative zeros are canonicalised to +0.0, as the builder's min/max semantics
+leave the sign of a zero unspecified.
+
+Vertices use marigold's 32-byte MeshVertex layout (position xyz, uv_x,
+normal xyz, uv_y; mesh_interface/src/lib.rs:6-12) with zero normals and uvs.
+Triangles are MeshTriangle index triples (mesh_interface/src/lib.rs:14-17).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_M32 = np.uint64(0xFFFFFFFF)
+
+
+def pcg_hash(v):
+    """PCG-RXS-M-XS 32-bit hash (O'Neill's PCG output permutation applied to
+    one LCG step, as popularised by Jarzynski & Olano 2020). uint32 in/out."""
+    v = np.asarray(v, dtype=np.uint32)
+    with np.errstate(over="ignore"):
+        state = v * np.uint32(747796405) + np.uint32(2891336453)
+        word = ((state >> ((state >> np.uint32(28)) + np.uint32(4))) ^ state) * np.uint32(277803737)
+    return (word >> np.uint32(22)) ^ word
+
+
+def stream_key(seed: int, stream: int) -> np.uint32:
+    s = pcg_hash(np.uint32(seed & 0xFFFFFFFF))
+    with np.errstate(over="ignore"):
+        return pcg_hash(s ^ pcg_hash(np.uint32(stream & 0xFFFFFFFF) + np.uint32(0x9E3779B9)))
+
+
+def uniform(seed: int, stream: int, idx) -> np.ndarray:
+    """float64 uniform in [0, 1) with 24 random bits, element idx of a stream."""
+    k = stream_key(seed, stream)
+    with np.errstate(over="ignore"):
+        h = pcg_hash(np.asarray(idx, dtype=np.uint32) + k)
+    return (h >> np.uint32(8)).astype(np.float64) * (1.0 / 16777216.0)
+
+
+def _sincos(x):
+    """sin and cos of x in [-pi, pi] by a fixed Taylor polynomial (|err| < 1e-15)."""
+    x = np.asarray(x, dtype=np.float64)
+    x2 = x * x
+    term_s = x.copy()
+    term_c = np.ones_like(x)
+    s = term_s.copy()
+    c = term_c.copy()
+    for k in range(1, 16):
+        term_s = term_s * x2 / ((2 * k) * (2 * k + 1)) * -1.0
+        term_c = term_c * x2 / ((2 * k - 1) * (2 * k)) * -1.0
+        s = s + term_s
+        c = c + term_c
+    return s, c
+
+
+def unit_vectors(seed: int, stream: int, idx) -> np.ndarray:
+    """Directions uniform on the sphere: z = 2u - 1, phi = 2 pi v."""
+    z = 2.0 * uniform(seed, stream, idx) - 1.0
+    phi = (2.0 * uniform(seed, stream + 1, idx) - 1.0) * np.pi
+    r = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    s, c = _sincos(phi)
+    return np.stack([r * c, r * s, z], axis=-1)
+
+
+def _f32(a) -> np.ndarray:
+    out = np.asarray(a, dtype=np.float32)
+    return out + np.float32(0.0)  # -0.0 -> +0.0
+
+
+def pack_vertices(pos: np.ndarray) -> np.ndarray:
+    """float32 [V, 8] MeshVertex records with the given positions."""
+    v = np.zeros((pos.shape[0], 8), dtype=np.float32)
+    v[:, 0:3] = _f32(pos)
+    return v
+
+
+def mesh_bounds(vertices: np.ndarray) -> np.ndarray:
+    """Accessor-style bounds (min xyz, max xyz) over the vertex positions."""
+    p = vertices[:, 0:3]
+    return np.concatenate([p.min(axis=0), p.max(axis=0)]).astype(np.float32)
+
+
+def triangle_aabbs(vertices: np.ndarray, triangles: np.ndarray) -> np.ndarray:
+    """float32 [N, 6] AABBs (MeshTriangle::bounding_volume)."""
+    p = vertices[:, 0:3][triangles]  # [N, 3, 3]
+    return np.concatenate([p.min(axis=1), p.max(axis=1)], axis=1).astype(np.float32)
+
+
+def random_triangles(n: int, seed: int = 1):
+    """Small random triangles: vertex 0 uniform in [0,1]^3, vertices 1 and 2
+    offset from it by lengths U(0.001, 0.02) in uniform directions. Vertices
+    are not shared: triangle i uses vertices 3i, 3i+1, 3i+2."""
+    i = np.arange(n, dtype=np.uint32)
+    v0 = np.stack([uniform(seed, s, i) for s in (0, 1, 2)], axis=-1)
+    pts = [v0]
+    for k in (1, 2):
+        length = 0.001 + 0.019 * uniform(seed, 10 * k, i)
+        d = unit_vectors(seed, 10 * k + 1, i)
+        pts.append(v0 + length[:, None] * d)
+    pos = np.stack(pts, axis=1).reshape(3 * n, 3)
+    vertices = pack_vertices(pos)
+    triangles = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    return vertices, triangles
+
+
+_PHI = (1.0 + np.sqrt(5.0)) / 2.0
+_ICO_V = np.array([
+    [-1, _PHI, 0], [1, _PHI, 0], [-1, -_PHI, 0], [1, -_PHI, 0],
+    [0, -1, _PHI], [0, 1, _PHI], [0, -1, -_PHI], [0, 1, -_PHI],
+    [_PHI, 0, -1], [_PHI, 0, 1], [-_PHI, 0, -1], [-_PHI, 0, 1]], dtype=np.float64)
+_ICO_F = np.array([
+    [0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11],
+    [1, 5, 9], [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8],
+    [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9],
+    [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], dtype=np.int64)
+
+
+def _normalize(p):
+    return p / np.sqrt((p * p).sum(axis=1, keepdims=True))
+
+
+def icosphere(level: int):
+    """Unit icosphere subdivided `level` times: 20*4^L faces, 10*4^L+2 vertices."""
+    v = _normalize(_ICO_V.copy())
+    f = _ICO_F.copy()
+    for _ in range(level):
+        nv = v.shape[0]
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]], axis=0)
+        key = np.minimum(e[:, 0], e[:, 1]) * nv + np.maximum(e[:, 0], e[:, 1])
+        uniq, inv = np.unique(key, return_inverse=True)
+        a = uniq // nv
+        b = uniq % nv
+        mid = _normalize((v[a] + v[b]) * 0.5)
+        m = inv.reshape(3, -1) + nv  # midpoint ids of edges (01, 12, 20)
+        m01, m12, m20 = m[0], m[1], m[2]
+        f = np.concatenate([
+            np.stack([f[:, 0], m01, m20], axis=1),
+            np.stack([f[:, 1], m12, m01], axis=1),
+            np.stack([f[:, 2], m20, m12], axis=1),
+            np.stack([m01, m12, m20], axis=1)], axis=0)
+        v = np.concatenate([v, mid], axis=0)
+    return v, f
+
+
+def _lattice(seed: int, octave: int, ix, iy, iz):
+    k = stream_key(seed, 1000 + octave)
+    with np.errstate(over="ignore"):
+        h = pcg_hash((ix.astype(np.int64) & 0xFFFFFFFF).astype(np.uint32) ^ k)
+        h = pcg_hash(h ^ (iy.astype(np.int64) & 0xFFFFFFFF).astype(np.uint32))
+        h = pcg_hash(h ^ (iz.astype(np.int64) & 0xFFFFFFFF).astype(np.uint32))
+    return (h >> np.uint32(8)).astype(np.float64) * (2.0 / 16777216.0) - 1.0
+
+
+def value_noise(p: np.ndarray, seed: int, octaves=(1.0, 2.0, 4.0), amps=(1.0, 0.5, 0.25)):
+    """3-octave value noise on a hashed integer lattice, smoothstep-weighted
+    trilinear interpolation, normalised by the amplitude sum (range [-1, 1])."""
+    total = np.zeros(p.shape[0], dtype=np.float64)
+    for o, (freq, amp) in enumerate(zip(octaves, amps)):
+        q = p * freq
+        q0 = np.floor(q)
+        t = q - q0
+        w = t * t * (3.0 - 2.0 * t)
+        i0 = q0.astype(np.int64)
+        acc = np.zeros(p.shape[0], dtype=np.float64)
+        for dx in (0, 1):
+            wx = w[:, 0] if dx else 1.0 - w[:, 0]
+            for dy in (0, 1):
+                wy = w[:, 1] if dy else 1.0 - w[:, 1]
+                for dz in (0, 1):
+                    wz = w[:, 2] if dz else 1.0 - w[:, 2]
+                    val = _lattice(seed, o, i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz)
+                    acc = acc + val * (wx * wy * wz)
+        total = total + amp * acc
+    return total / float(sum(amps))
+
+
+def noisy_icosphere(level: int = 8, seed: int = 2, amplitude: float = 0.05):
+    """Icosphere with vertices displaced radially by 1 + amplitude * noise(p)."""
+    v, f = icosphere(level)
+    r = 1.0 + amplitude * value_noise(v, seed)
+    vertices = pack_vertices(v * r[:, None])
+    return vertices, f.astype(np.uint32)
+
+
+def config1_mesh(seed: int = 1):
+    """65,536 random small triangles (the binned-SAH BLAS workload)."""
+    return random_triangles(65536, seed)
+
+
+def config2_mesh(seed: int = 2):
+    """Noisy icosphere, level 8: 1,310,720 triangles, 655,362 shared vertices."""
+    return noisy_icosphere(8, seed)

@@ -1,0 +1,128 @@
+"""ctypes front end of the CPU oracle (``bvh_oracle.cpp``).
+
+TEST INFRASTRUCTURE ONLY: tests, ``__graft_entry__.smoke`` and the CPU
+baseline leg of ``bench.py`` use it as the checker. The product path never
+imports this module.
+
+PARITY UNPINNED: the reference crate cannot be built here and ships no
+golden vectors; the oracle restates ``bvh/src/lib.rs`` and is pinned by
+hand-worked known-answer trees and by the reference's own invariants.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libmgbvh_oracle.so")
+_lock = threading.Lock()
+_lib = None
+
+
+class Stats(ctypes.Structure):
+    """Mirror of ``mgbvh_stats`` (include/mgbvh.h)."""
+
+    _fields_ = [
+        ("construction_time", ctypes.c_double),
+        ("node_count", ctypes.c_uint32),
+        ("leaf_node_count", ctypes.c_uint32),
+        ("min_leaf_object_count", ctypes.c_uint32),
+        ("max_leaf_object_count", ctypes.c_uint32),
+        ("avg_leaf_object_count", ctypes.c_double),
+        ("stddev_leaf_object_count", ctypes.c_double),
+        ("total_object_count", ctypes.c_uint32),
+        ("height", ctypes.c_uint32),
+        ("max_depth", ctypes.c_uint32),
+        ("median_splits", ctypes.c_uint32),
+        ("depth_capped_leaves", ctypes.c_uint32),
+        ("feasible", ctypes.c_uint32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class _Knobs(ctypes.Structure):
+    _fields_ = [
+        ("bins", ctypes.c_uint32),
+        ("adaptive_max_n", ctypes.c_uint32),
+        ("adaptive_steps", ctypes.c_uint32),
+        ("faithful", ctypes.c_uint32),
+    ]
+
+
+def build_library(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc only; no GPU needed)."""
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+        os.path.join(_HERE, "bvh_oracle.cpp")
+    ):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(_LIB_PATH):
+                build_library()
+            L = ctypes.CDLL(_LIB_PATH)
+            P = ctypes.c_void_p
+            u32 = ctypes.c_uint32
+            L.oracle_build.argtypes = [P, u32, P, P, u32, P, u32, u32, u32,
+                                       ctypes.POINTER(_Knobs), P, u32, P, P,
+                                       ctypes.POINTER(u32), ctypes.POINTER(Stats)]
+            L.oracle_build.restype = ctypes.c_int
+            L.oracle_last_tie_events.restype = u32
+            _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def build(vertices=None, triangles=None, aabbs=None, *, vertex_stride_bytes=32,
+          root_bounds=None, min_leaf=1, max_leaf=1, max_depth=32, bins=0,
+          adaptive_max_n=32, adaptive_steps=0, faithful=False):
+    """Build one BVH with the oracle.
+
+    Either ``vertices`` (float32 [V, stride/4]) + ``triangles`` (uint32 [N, 3])
+    or ``aabbs`` (float32 [N, 6]). Returns a dict with ``status``, ``nodes``
+    (uint32 [count, 8], the mgbvh_node layout), ``lens``, ``perm``, ``stats``
+    and ``tie_events``.
+    """
+    L = lib()
+    if aabbs is not None:
+        aabbs = np.ascontiguousarray(aabbs, dtype=np.float32)
+        n = aabbs.shape[0]
+        vp = tp = None
+    else:
+        vertices = np.ascontiguousarray(vertices, dtype=np.float32)
+        triangles = np.ascontiguousarray(triangles, dtype=np.uint32)
+        n = triangles.shape[0]
+        vp, tp = vertices, triangles
+    cap = max(2 * n - 1, 1)
+    nodes = np.zeros((cap, 8), dtype=np.uint32)
+    lens = np.zeros(cap, dtype=np.uint32)
+    perm = np.zeros(max(n, 1), dtype=np.uint32)
+    rb = None if root_bounds is None else np.ascontiguousarray(root_bounds, dtype=np.float32)
+    count = ctypes.c_uint32(0)
+    st = Stats()
+    kn = _Knobs(bins, adaptive_max_n, adaptive_steps, 1 if faithful else 0)
+    status = L.oracle_build(_ptr(vp), vertex_stride_bytes, _ptr(tp), _ptr(aabbs), n, _ptr(rb),
+                            min_leaf, max_leaf, max_depth, ctypes.byref(kn), _ptr(nodes), cap,
+                            _ptr(lens), _ptr(perm), ctypes.byref(count), ctypes.byref(st))
+    c = count.value
+    return {
+        "status": status,
+        "nodes": nodes[:c].copy(),
+        "lens": lens[:c].copy(),
+        "perm": perm[:n].copy(),
+        "stats": st.as_dict(),
+        "tie_events": L.oracle_last_tie_events(),
+    }

@@ -1,0 +1,171 @@
+"""CUDA builder vs the CPU oracle, bit for bit (needs a B200).
+
+Every case builds the same seeded input with the oracle (stable parity mode)
+and with libmgbvh.so through the C ABI, and compares node words, per-node
+object counts and the permutation exactly. Structural invariants of the
+reference (treecheck.check_tree) are checked on the GPU result as well.
+"""
+import numpy as np
+import pytest
+
+from marigold_b200 import synth
+from tests.gpuhelp import gpu_build
+from tests.treecheck import check_tree, compare_exact
+
+pytestmark = pytest.mark.gpu
+
+
+def unit_box(x, y=0.0, z=0.0):
+    return [x, y, z, x + 1.0, y + 1.0, z + 1.0]
+
+
+def both(oracle, ctx, **kw):
+    o = oracle.build(**kw)
+    g = gpu_build(ctx, **kw)
+    assert g["status"] == o["status"], (g["status"], g["error"], o["status"])
+    msg = compare_exact(g["nodes"], g["lens"], g["perm"], o["nodes"], o["lens"], o["perm"])
+    assert msg is None, msg
+    return o, g
+
+
+KNOWN = [
+    [unit_box(0)],
+    [unit_box(0), unit_box(2)],
+    [unit_box(2), unit_box(0)],
+    [unit_box(0), unit_box(2), unit_box(4), unit_box(6)],
+    [unit_box(0)] * 4,
+    [unit_box(0)] * 40,      # forced medians through the medium-node path
+    [unit_box(0)] * 1030,    # coincident centroids in a node above the CTA size
+]
+
+
+@pytest.mark.parametrize("case", range(len(KNOWN)))
+def test_known_answer_cases(oracle, gpu_ctx, case):
+    boxes = np.array(KNOWN[case], np.float32)
+    if case == 6:
+        g = gpu_build(gpu_ctx, aabbs=boxes)
+        # a forced median above 1024 objects is reported, not silently built
+        assert g["status"] == -6, g
+        return
+    both(oracle, gpu_ctx, aabbs=boxes)
+
+
+def test_depth_cap_known_answer(oracle, gpu_ctx):
+    boxes = np.array([unit_box(0), unit_box(2), unit_box(4), unit_box(6)], np.float32)
+    o, g = both(oracle, gpu_ctx, aabbs=boxes, max_depth=1)
+    assert g["stats"]["depth_capped_leaves"] == 2 and g["nodes"].shape[0] == 3
+
+
+@pytest.mark.parametrize("n", [2, 3, 5, 7, 8, 9, 16, 31, 32, 33, 34, 63, 64, 100, 500, 1000, 1023,
+                               1024, 1025, 1026, 2047, 2048, 2049, 4096, 5000, 20000])
+def test_random_sizes(oracle, gpu_ctx, n):
+    v, t = synth.random_triangles(n, 100 + n)
+    b = synth.mesh_bounds(v)
+    o, g = both(oracle, gpu_ctx, vertices=v, triangles=t, root_bounds=b)
+    check_tree(g["nodes"], g["lens"], g["perm"], synth.triangle_aabbs(v, t), root_bounds=b)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(max_depth=0), dict(max_depth=1), dict(max_depth=3), dict(max_depth=8), dict(max_depth=12),
+    dict(min_leaf=2, max_leaf=4), dict(min_leaf=1, max_leaf=8), dict(min_leaf=4, max_leaf=4),
+    dict(min_leaf=3, max_leaf=16), dict(min_leaf=1, max_leaf=2000),
+    dict(bins=16, adaptive_max_n=0), dict(bins=16), dict(bins=8), dict(bins=2), dict(bins=31),
+    dict(adaptive_steps=16), dict(adaptive_steps=1), dict(adaptive_max_n=8), dict(adaptive_max_n=1),
+    dict(adaptive_max_n=0), dict(bins=12, adaptive_steps=5, adaptive_max_n=20),
+])
+def test_knobs_and_leaf_bounds(oracle, gpu_ctx, kw):
+    v, t = synth.random_triangles(6000, 7)
+    both(oracle, gpu_ctx, vertices=v, triangles=t, **kw)
+
+
+def test_aabb_path_tlas_like(oracle, gpu_ctx):
+    # the TLAS path: AsBoundingVolume objects, root bounds = union (bounds: None)
+    rng = np.random.default_rng(3)
+    lo = rng.uniform(-100, 100, size=(4096, 3)).astype(np.float32)
+    ext = rng.uniform(0.5, 20, size=(4096, 3)).astype(np.float32)
+    boxes = np.concatenate([lo, lo + ext], axis=1)
+    o, g = both(oracle, gpu_ctx, aabbs=boxes)
+    check_tree(g["nodes"], g["lens"], g["perm"], boxes)
+
+
+def test_duplicates_and_clusters(oracle, gpu_ctx):
+    # many exactly duplicated triangles: coincident centroids below the CTA size
+    v, t = synth.random_triangles(300, 9)
+    t = np.concatenate([t] * 3 + [t[:7]] * 5, axis=0)
+    both(oracle, gpu_ctx, vertices=v, triangles=t)
+
+
+def test_config1_reference_profile(oracle, gpu_ctx):
+    v, t = synth.config1_mesh()
+    b = synth.mesh_bounds(v)
+    o, g = both(oracle, gpu_ctx, vertices=v, triangles=t, root_bounds=b)
+    assert g["nodes"].shape[0] == 2 * 65536 - 1
+    for k in ("node_count", "leaf_node_count", "height", "min_leaf_object_count",
+              "max_leaf_object_count"):
+        assert g["stats"][k] == o["stats"][k], k
+
+
+def test_config1_sixteen_bins_adaptive_off(oracle, gpu_ctx):
+    v, t = synth.config1_mesh()
+    both(oracle, gpu_ctx, vertices=v, triangles=t, root_bounds=synth.mesh_bounds(v), bins=16,
+         adaptive_max_n=0)
+
+
+def test_config2_reference_profile(oracle, gpu_ctx):
+    v, t = synth.config2_mesh()
+    b = synth.mesh_bounds(v)
+    o, g = both(oracle, gpu_ctx, vertices=v, triangles=t, root_bounds=b)
+    check_tree(g["nodes"], g["lens"], g["perm"], synth.triangle_aabbs(v, t), root_bounds=b)
+
+
+def test_config2_thirtytwo_bins_sixteen_thresholds(oracle, gpu_ctx):
+    v, t = synth.config2_mesh()
+    both(oracle, gpu_ctx, vertices=v, triangles=t, root_bounds=synth.mesh_bounds(v), bins=32,
+         adaptive_steps=16)
+
+
+def test_bad_index_is_an_error(gpu_ctx):
+    v, t = synth.random_triangles(100, 1)
+    t = t.copy()
+    t[50, 1] = v.shape[0] + 5
+    g = gpu_build(gpu_ctx, vertices=v, triangles=t)
+    assert g["status"] == -1 and "index" in g["error"]
+
+
+def test_capacity_too_small_is_an_error(gpu_ctx):
+    v, t = synth.random_triangles(100, 1)
+    g = gpu_build(gpu_ctx, vertices=v, triangles=t, capacity=150)
+    assert g["status"] == -2
+
+
+def test_empty_input_warns(gpu_ctx):
+    g = gpu_build(gpu_ctx, aabbs=np.zeros((0, 6), np.float32))
+    assert g["status"] == 1 and g["nodes"].shape[0] == 0
+
+
+def test_repeated_builds_on_one_context(oracle, gpu_ctx):
+    # scratch reuse across sizes must not leak state between builds
+    for n in (5000, 100, 70000, 33, 5000):
+        v, t = synth.random_triangles(n, 500 + n)
+        both(oracle, gpu_ctx, vertices=v, triangles=t)
+
+
+def test_device_entry_point_matches_host_entry_point(oracle, gpu_ctx):
+    import torch
+    from marigold_b200 import BvhSettings, build_device
+    v, t = synth.random_triangles(40000, 77)
+    o = oracle.build(v, t)
+    dv = torch.from_numpy(v).cuda()
+    dt = torch.from_numpy(t.astype(np.int32)).cuda()
+    n = t.shape[0]
+    nodes = torch.zeros((2 * n - 1) * 8, dtype=torch.int32, device="cuda")
+    lens = torch.zeros(2 * n - 1, dtype=torch.int32, device="cuda")
+    perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    count, rc, st = build_device(gpu_ctx, BvhSettings(), nodes, perm, vertices=dv, triangles=dt,
+                                 out_lens=lens)
+    torch.cuda.synchronize()
+    assert rc == 0 and count == 2 * n - 1
+    gw = nodes.cpu().numpy().view(np.uint32).reshape(-1, 8)
+    msg = compare_exact(gw, lens.cpu().numpy().view(np.uint32), perm.cpu().numpy().view(np.uint32),
+                        o["nodes"], o["lens"], o["perm"])
+    assert msg is None, msg
