@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""bench.py — SAH BVH build throughput (Mtri/s) on B200.
+
+Workload: the noisy level-8 icosphere (1,310,720 f32 triangles, 655,362
+shared vertices, 3-octave value noise of amplitude 0.05, seeded), leaf size
+MIN = MAX = 1, max_depth 32, the reference's split profile (32 bins above
+32 objects, adaptive sweep at or below). One step = one full BVH build.
+
+  value  builds timed with CUDA events on the build stream, inputs already
+         in HBM; L2 flushed (256 MiB write) before every step, outside the
+         timed interval; max over ranks; Mtri/s = triangles / time.
+  e2e    the same build through the C ABI's host-pointer entry point
+         (mgbvh_build_indexed): pinned host inputs copied in, nodes, lens and
+         permutation copied out, every step.
+  cpu_baseline / --impl reference: the oracle port (faithful mode: the
+         reference's algorithmic form, bvh/src/lib.rs) on host cores, one
+         single-threaded build per process like the reference's sample
+         collector (bvh_sample_collector/src/main.rs:41-44), on a bounded
+         sample: the first 131,072 triangles of the same mesh.
+
+With torchrun (N > 1) every rank builds its own replica (the path does not
+shard within a mesh); value = all ranks' triangles / the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BVH build Mtri/s"
+UNIT = "Mtri/s"
+SAMPLE_TRIS = 131072
+WORKLOAD = ("noisy icosphere L8 (1,310,720 tris, 655,362 verts), leaf 1, max_depth 32, "
+            "reference split profile")
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--profile-steps", type=int, default=None, help=argparse.SUPPRESS)
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload():
+    from marigold_b200 import synth
+    v, t = synth.config2_mesh()
+    return v, t, synth.mesh_bounds(v)
+
+
+# ---------------------------------------------------------------- CPU leg
+
+_cpu_mesh = None
+
+
+def _cpu_init():
+    global _cpu_mesh
+    from marigold_b200 import synth
+    v, t, _ = workload()
+    t = np.ascontiguousarray(t[:SAMPLE_TRIS])
+    aabb = synth.triangle_aabbs(v, t)
+    bounds = np.concatenate([aabb[:, 0:3].min(0), aabb[:, 3:6].max(0)]).astype(np.float32)
+    _cpu_mesh = (v, t, bounds)
+
+
+def _cpu_build(_):
+    from oracle import oracle
+    v, t, b = _cpu_mesh
+    t0 = time.perf_counter()
+    r = oracle.build(v, t, root_bounds=b, faithful=True)
+    dt = time.perf_counter() - t0
+    assert r["status"] == 0
+    return dt
+
+
+def cpu_measure(steps: int, warmup: int):
+    """Faithful oracle builds of the sample, one per process on every host core."""
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_cpu_init) as pool:
+        for _ in range(warmup):
+            pool.map(_cpu_build, range(cores))
+        walls = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_build, range(cores))
+            walls.append(time.perf_counter() - t0)
+    wall = sum(walls) / len(walls)
+    value = cores * SAMPLE_TRIS / wall / 1e6
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {SAMPLE_TRIS} triangles of the workload mesh, one single-threaded "
+                      f"faithful-oracle build per core, {cores} concurrent, mean of {steps} steps",
+            "ms_per_step": wall * 1e3}
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+               0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting"}
+
+    def __init__(self, index: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and bit != 0x1:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.01)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv:
+            self.t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- GPU leg
+
+def algorithmic_bytes(n, n_verts, internal_len_sum, node_count):
+    """Bytes a build must move at minimum (per object per level of the
+    partition: read + write of a 24-byte AABB and a 4-byte index)."""
+    return (n * (12 + 3 * 32) + n * 24 + internal_len_sum * 56 + node_count * 32)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from marigold_b200 import BvhSettings, _lib, build_device
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    v, t, bounds = workload()
+    n = t.shape[0]
+    settings = BvhSettings(name="bench", bounds=bounds, max_depth=32)
+    ctx = _lib.Context(local)
+    dv = torch.from_numpy(v).cuda()
+    dt = torch.from_numpy(t.view(np.int32)).cuda()
+    cap = 2 * n - 1
+    d_nodes = torch.empty(cap * 8, dtype=torch.int32, device="cuda")
+    d_lens = torch.empty(cap, dtype=torch.int32, device="cuda")
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def one():
+        return build_device(ctx, settings, d_nodes, d_perm, vertices=dv, triangles=dt,
+                            out_lens=d_lens, stream=stream)
+
+    for _ in range(max(args.warmup, 3)):
+        flush.fill_(1)
+        one()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    launches = 0
+    phase = np.zeros(4)
+    with ClockSampler(local) as clocks:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            ev[k][0].record(stream)
+            count, rc, st = one()
+            ev[k][1].record(stream)
+            launches += st["kernel_launches"]
+            phase += np.asarray(st["phase_seconds"])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    ms_per_step = float(np.mean(ms))
+    if world > 1:
+        tt = torch.tensor([ms_per_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_per_step = float(tt.item())
+    value = world * n / (ms_per_step * 1e-3) / 1e6
+
+    # tree statistics for the algorithmic byte count (S = sum of inner lens)
+    nodes_h = d_nodes.cpu().numpy().view(np.uint32).reshape(-1, 8)
+    lens_h = d_lens.cpu().numpy().view(np.uint32)[:count].astype(np.int64)
+    inner = nodes_h[:count, 7] != 0
+    S = int(lens_h[inner].sum())
+    alg = algorithmic_bytes(n, v.shape[0], S, count)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs")
+    peak_src = "measured" if hbm else "fallback"
+    hbm = hbm or 6650.0
+    achieved = alg / (ms_per_step * 1e-3) / 1e9
+
+    # e2e through the host-pointer C ABI entry point, pinned host buffers
+    import ctypes
+    L = ctx.L
+    pin_v = torch.from_numpy(v).pin_memory()
+    pin_t = torch.from_numpy(t.view(np.int32)).pin_memory()
+    pin_nodes = torch.empty(cap * 8, dtype=torch.int32).pin_memory()
+    pin_lens = torch.empty(cap, dtype=torch.int32).pin_memory()
+    pin_perm = torch.empty(n, dtype=torch.int32).pin_memory()
+    cs = settings.to_c(1, 1)
+    cnt = ctypes.c_uint32(0)
+    ctx.set_stream(None)
+
+    def e2e_one():
+        rc = L.mgbvh_build_indexed(ctx.ptr, ctypes.c_void_p(pin_v.data_ptr()), 32, v.shape[0],
+                                   ctypes.c_void_p(pin_t.data_ptr()), n, ctypes.byref(cs),
+                                   ctypes.c_void_p(pin_nodes.data_ptr()), cap, ctypes.byref(cnt),
+                                   ctypes.c_void_p(pin_lens.data_ptr()),
+                                   ctypes.c_void_p(pin_perm.data_ptr()), None)
+        ctx.check(rc)
+
+    for _ in range(3):
+        e2e_one()
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_one()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = float(np.mean(e2e_ms))
+    if world > 1:
+        tt = torch.tensor([e2e_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_step = float(tt.item())
+    h2d = v.nbytes + t.nbytes
+    d2h = cnt.value * 32 + cnt.value * 4 + n * 4
+
+    out = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded noisy icosphere; no public dataset is named)",
+        "config": {"workload": WORKLOAD, "triangles": n, "vertices": int(v.shape[0]),
+                   "min_leaf": 1, "max_leaf": 1, "max_depth": 32, "bins": 32,
+                   "adaptive_max_n": 32, "parallelism": f"replicas x{world}",
+                   "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
+        "e2e": {"value": round(world * n / (e2e_step * 1e-3) / 1e6, 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": round(e2e_step, 4)},
+        "roofline": {"bound": "hbm", "kernel": "whole build (all phases)",
+                     "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "peak_source": peak_src,
+                     "traffic": None, "algorithmic_bytes_per_build": int(alg),
+                     "inner_len_sum": S},
+        "phase_ms": [round(x * 1e3 / args.steps, 4) for x in phase],
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "nodes": int(count),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_measure(steps=2, warmup=1)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    cb = cpu_measure(steps=args.steps, warmup=args.warmup)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(cb["value"], 4), "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(cb["ms_per_step"], 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded noisy icosphere)",
+        "config": {"workload": WORKLOAD, "triangles": 1310720, "sample_triangles": SAMPLE_TRIS,
+                   "min_leaf": 1, "max_leaf": 1, "max_depth": 32, "parallelism": "host cores"},
+        "cpu_baseline": cb,
+        "e2e": {"value": round(cb["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

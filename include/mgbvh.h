@@ -117,6 +117,11 @@ typedef struct mgbvh_stats {
     uint32_t median_splits;       /* forced median splits taken */
     uint32_t depth_capped_leaves; /* leaves made by depth == max_depth with len > 1 */
     uint32_t feasible;            /* the crate's feasibility flag */
+    uint32_t kernel_launches;     /* builder kernels launched by this build */
+    uint32_t levels;              /* level-synchronous passes over nodes above 1024 objects */
+    /* device seconds per phase: [0] object records + root, [1] level passes,
+       [2] subtrees of 33..1024 objects, [3] subtrees of <= 32 objects */
+    double phase_seconds[4];
 } mgbvh_stats;
 
 typedef struct mgbvh_ctx mgbvh_ctx;

@@ -1046,7 +1046,7 @@ struct mgbvh_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp[3] = {nullptr, nullptr, nullptr};
     std::string err;
     DevBuf rec[2], tasks[2], bins[2], cbkeys[2], tile_task[2], tile_begin[2];
     DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
@@ -1218,10 +1218,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
             st->max_depth);
     }
     MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+    uint32_t launches = 2, levels = 0;
 
     uint32_t n_tasks = cls == 3 ? 1u : 0u, n_tiles = ntiles0;
     uint32_t cur = 0;
     while (n_tasks > 0) {
+        launches += 3;
+        levels++;
         const uint32_t nx = cur ^ 1u;
         lvl_bin_kernel<<<n_tiles, kTileThreads, 0, sm>>>(
             P_<Task>(ctx->tasks[cur]), P_<uint32_t>(ctx->cbkeys[cur]), P_<uint32_t>(ctx->bins[cur]),
@@ -1262,15 +1266,23 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     }
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
     MG_CUDA(cudaStreamSynchronize(sm));
+    MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
     if (!ctx->h_ctr->error) {
         const uint32_t n_medium = ctx->h_ctr->n_medium, n_small = ctx->h_ctr->n_small;
-        if (n_medium > 0)
+        if (n_medium > 0) {
             medium_kernel<<<n_medium, kMediumThreads, sizeof(MediumSmem), sm>>>(P_<Task>(ctx->medium),
                                                                                  rec0, rec1, P, O);
-        if (n_small > 0)
+            launches++;
+        }
+        MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
+        if (n_small > 0) {
             small_kernel<<<(n_small + 7) / 8, 256, 0, sm>>>(P_<Task>(ctx->small), n_small, rec0, rec1,
                                                              P, O);
+            launches++;
+        }
         MG_CUDA(cudaGetLastError());
+    } else {
+        MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
     }
     MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
@@ -1308,6 +1320,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
             P_<mgbvh_node>(ctx->nodes), P_<uint32_t>(ctx->lens), P_<uint8_t>(ctx->used),
             P_<uint32_t>(ctx->newidx), C.nodes, d_nodes, d_lens);
         MG_CUDA(cudaGetLastError());
+        launches += 2;
     } else {
         if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
         MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
@@ -1326,6 +1339,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
         stats->max_depth = st->max_depth;
         stats->median_splits = hc.median_splits;
         stats->depth_capped_leaves = hc.depth_capped;
+        stats->kernel_launches = launches;
+        stats->levels = levels;
+        float pm[4] = {0.f, 0.f, 0.f, 0.f};
+        cudaEventElapsedTime(&pm[0], ctx->ev0, ctx->evp[0]);
+        cudaEventElapsedTime(&pm[1], ctx->evp[0], ctx->evp[1]);
+        cudaEventElapsedTime(&pm[2], ctx->evp[1], ctx->evp[2]);
+        cudaEventElapsedTime(&pm[3], ctx->evp[2], ctx->ev1);
+        for (int i = 0; i < 4; ++i) stats->phase_seconds[i] = pm[i] * 1e-3;
         const uint32_t MINs = st->min_leaf_objects, MAXs = st->max_leaf_objects;
         stats->feasible = (MINs == MAXs) ? (n % MINs == 0) : (MAXs >= 2 * MINs - 1);
         if (st->profiling_info) {
@@ -1503,6 +1524,8 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
     ctx->device = device;
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreate(&ctx->evp[0]) != cudaSuccess || cudaEventCreate(&ctx->evp[1]) != cudaSuccess ||
+        cudaEventCreate(&ctx->evp[2]) != cudaSuccess ||
         cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(MediumSmem)) != cudaSuccess) {
@@ -1528,6 +1551,8 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (cudaEvent_t e : ctx->evp)
+        if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

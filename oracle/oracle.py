@@ -40,10 +40,15 @@ class Stats(ctypes.Structure):
         ("median_splits", ctypes.c_uint32),
         ("depth_capped_leaves", ctypes.c_uint32),
         ("feasible", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32),
+        ("levels", ctypes.c_uint32),
+        ("phase_seconds", ctypes.c_double * 4),
     ]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        d = {name: getattr(self, name) for name, _ in self._fields_}
+        d["phase_seconds"] = list(self.phase_seconds)
+        return d
 
 
 class _Knobs(ctypes.Structure):
