@@ -51,6 +51,7 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-e2e", action="store_true", help="skip the host-pointer (e2e) leg")
     p.add_argument("--profile-steps", type=int, default=None, help=argparse.SUPPRESS)
     return p.parse_args()
 
@@ -240,6 +241,16 @@ def run_ours(args):
     peak_src = "measured" if hbm else "fallback"
     hbm = hbm or 6650.0
     achieved = alg / (ms_per_step * 1e-3) / 1e9
+
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": UNIT,
+                              "ms_per_step": round(ms_per_step, 4), "n_gpus": world,
+                              "phase_ms": [round(x * 1e3 / args.steps, 4) for x in phase],
+                              "gpu_launches": int(launches), "clocks": clocks.summary()}))
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # e2e through the host-pointer C ABI entry point, pinned host buffers
     import ctypes

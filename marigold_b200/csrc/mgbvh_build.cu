@@ -714,14 +714,13 @@ __device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
 }
 
 __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
-                                                                const Rec* __restrict__ rec0,
-                                                                const Rec* __restrict__ rec1,
-                                                                Params P, Out O) {
+                                                                Rec* rec0, Rec* rec1, Task* small,
+                                                                uint32_t cap_small, Params P, Out O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const Task t = tasks[blockIdx.x];
-    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+    Rec* src = (t.buf ? rec1 : rec0) + t.start;
     const uint32_t base = t.start;
     uint32_t k[12];
     init_key12(k);
@@ -964,11 +963,35 @@ __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __re
                         S.list_x[cur ^ 1u][li2].ib = ob;
                     }
                 } else {
-                    float lo[3], hi[3];
-                    uint32_t id;
-                    medium_load_warp_records(S, ob, cs, len, lane, lo, hi, id);
-                    warp_build_subtree(lo, hi, id, len, base + cs, slot, pair, cdepth, cbx, P, O,
-                                       S.xchg[warp]);
+                    // subtree of <= 32 objects: write its records back to this task's
+                    // range of the record buffer and queue it for small_kernel
+                    if (lane < len) {
+                        const uint32_t r = S.idx[ob][cs + lane];
+                        Rec rr;
+                        rr.lo = S.rlo[r];
+                        rr.hi = S.rhi[r];
+                        src[cs + lane] = rr;
+                    }
+                    uint32_t si = 0;
+                    if (lane == 0) si = atomicAdd(&O.ctr->n_small, 1u);
+                    si = __shfl_sync(kFull, si, 0);
+                    if (si >= cap_small) {
+                        if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                    } else if (lane == 0) {
+                        Task st;
+                        for (int a = 0; a < 3; ++a) {
+                            st.lo[a] = cbx[a];
+                            st.hi[a] = cbx[3 + a];
+                        }
+                        st.start = base + cs;
+                        st.len = len;
+                        st.slot = slot;
+                        st.pair = pair;
+                        st.depth = cdepth;
+                        st.buf = t.buf;
+                        st.tile0 = st.ntiles = st.pad0 = st.pad1 = 0;
+                        small[si] = st;
+                    }
                 }
             }
         }
@@ -982,29 +1005,30 @@ __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __re
 
 // ---------------------------------------------------------------- small
 
-__global__ void __launch_bounds__(256) small_kernel(const Task* __restrict__ tasks, uint32_t n_tasks,
+__global__ void __launch_bounds__(256, 2) small_kernel(const Task* __restrict__ tasks,
                                                    const Rec* __restrict__ rec0,
                                                    const Rec* __restrict__ rec1, Params P, Out O) {
     __shared__ XRec xchg[8][32];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    const uint32_t w = blockIdx.x * 8 + wib;
-    if (w >= n_tasks) return;
-    const Task t = tasks[w];
-    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
-    float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
-    uint32_t id = 0;
-    if (lane < t.len) {
-        const Rec r = src[lane];
-        lo[0] = r.lo.x;
-        lo[1] = r.lo.y;
-        lo[2] = r.lo.z;
-        id = __float_as_uint(r.lo.w);
-        hi[0] = r.hi.x;
-        hi[1] = r.hi.y;
-        hi[2] = r.hi.z;
+    const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
+    for (uint32_t w = blockIdx.x * 8 + wib; w < n_tasks; w += gridDim.x * 8) {
+        const Task t = tasks[w];
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+        float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+        uint32_t id = 0;
+        if (lane < t.len) {
+            const Rec r = src[lane];
+            lo[0] = r.lo.x;
+            lo[1] = r.lo.y;
+            lo[2] = r.lo.z;
+            id = __float_as_uint(r.lo.w);
+            hi[0] = r.hi.x;
+            hi[1] = r.hi.y;
+            hi[2] = r.hi.z;
+        }
+        const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+        warp_build(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O, xchg[wib]);
     }
-    const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-    warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O, xchg[wib]);
 }
 
 // ---------------------------------------------------------------- compaction
@@ -1044,6 +1068,7 @@ struct DevBuf {
 
 struct mgbvh_ctx {
     int device = 0;
+    int sm_count = 148;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp[3] = {nullptr, nullptr, nullptr};
@@ -1095,7 +1120,7 @@ Caps caps_for(uint32_t n) {
     c.tasks = n / (kMediumMax + 1) + 2;
     c.tiles = n / kTile + c.tasks + 2;
     c.medium = 4 * (n / kMediumMax) + 8;
-    c.small = c.medium;
+    c.small = n / 2 + 8;
     c.nodes = 2 * n - 1;
     return c;
 }
@@ -1270,16 +1295,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     if (!ctx->h_ctr->error) {
         const uint32_t n_medium = ctx->h_ctr->n_medium, n_small = ctx->h_ctr->n_small;
         if (n_medium > 0) {
-            medium_kernel<<<n_medium, kMediumThreads, sizeof(MediumSmem), sm>>>(P_<Task>(ctx->medium),
-                                                                                 rec0, rec1, P, O);
+            medium_kernel<<<n_medium, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O);
             launches++;
         }
         MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
-        if (n_small > 0) {
-            small_kernel<<<(n_small + 7) / 8, 256, 0, sm>>>(P_<Task>(ctx->small), n_small, rec0, rec1,
-                                                             P, O);
-            launches++;
-        }
+        // small subtrees: count read on the device; grid sized for full occupancy
+        small_kernel<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
+        launches++;
         MG_CUDA(cudaGetLastError());
     } else {
         MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
@@ -1522,6 +1545,7 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
     if (cudaSetDevice(device) != cudaSuccess) return MGBVH_ERR_CUDA;
     mgbvh_ctx* ctx = new mgbvh_ctx();
     ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaEventCreate(&ctx->evp[0]) != cudaSuccess || cudaEventCreate(&ctx->evp[1]) != cudaSuccess ||

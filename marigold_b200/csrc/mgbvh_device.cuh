@@ -535,4 +535,278 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
     }
 }
 
+// Lanes [s, s+n) as a mask.
+__device__ __forceinline__ uint32_t seg_mask(uint32_t s, uint32_t n) {
+    return n >= 32u ? kFull : (((1u << n) - 1u) << s);
+}
+
+// Writes one node from a single lane (two 16-byte stores).
+__device__ __forceinline__ void lane_store_node(const Out& o, uint32_t slot, const float* b,
+                                                uint32_t start, uint32_t len, uint32_t child) {
+    if (slot >= o.node_cap) {
+        set_error(o.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+        return;
+    }
+    float4* p = reinterpret_cast<float4*>(o.nodes + slot);
+    p[0] = make_float4(b[0], b[1], b[2], __uint_as_float(start));
+    p[1] = make_float4(b[3], b[4], b[5], __uint_as_float(child));
+    o.lens[slot] = len;
+    o.used[slot] = 1;
+}
+
+// Moves this lane's object to lane `dst` (a permutation of the warp).
+__device__ __forceinline__ void warp_exchange(uint32_t dst, uint32_t lane, float* lo, float* hi,
+                                              uint32_t& id, XRec* x) {
+    x[dst].lo = make_float4(lo[0], lo[1], lo[2], __uint_as_float(id));
+    x[dst].hi = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    __syncwarp();
+    const float4 a = x[lane].lo, b = x[lane].hi;
+    lo[0] = a.x;
+    lo[1] = a.y;
+    lo[2] = a.z;
+    id = __float_as_uint(a.w);
+    hi[0] = b.x;
+    hi[1] = b.y;
+    hi[2] = b.z;
+    __syncwarp();
+}
+
+// Level-synchronous form of warp_build_subtree: every node of one depth of
+// the subtree is evaluated at the same time, each on its own lane range
+// (segment), with segmented warp reductions. Valid when every node of the
+// subtree uses the adaptive sweep with one threshold per object: the
+// reference profile (steps = len.clamp(8,32) = len for 8 <= len <= 32, one
+// centroid per object below 8; bvh/src/lib.rs:417-437).
+__device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id, uint32_t n0,
+                                          uint32_t base, uint32_t slot0, uint32_t pair0,
+                                          uint32_t depth0, const float* bounds0, const Params& P,
+                                          const Out& O, XRec* xchg) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t s = 0, n = n0, slot = slot0, pair = pair0, depth = depth0;
+    float nb[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) nb[i] = bounds0[i];
+    bool live = lane < n0;
+    uint32_t hmax = 0, n_median = 0, n_holes = 0, n_capped = 0;
+    bool any_split = false;
+
+    while (__any_sync(kFull, live)) {
+        const uint32_t m = live ? seg_mask(s, n) : (1u << lane);
+        const bool leader = live && lane == s;
+        bool leaf = n <= 1u || depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf);
+        const bool work = live && !leaf;
+        float c[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) c[a] = center_of(lo[a], hi[a]);
+        // centroid bounds of each segment (bvh/src/lib.rs:499-509)
+        float cmn[3], ext[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            cmn[a] = funkey(__reduce_min_sync(m, work ? fkey(c[a]) : kKeyPosInf));
+            const float cmx = funkey(__reduce_max_sync(m, work ? fkey(c[a]) : kKeyNegInf));
+            ext[a] = __fsub_rn(cmx, cmn[a]);
+        }
+        const float sa_p = surface_area6(nb);
+        const bool exact = n < 8u;
+        const uint32_t k = lane - s;
+        float thr[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float step = __fdiv_rn(ext[a], __uint2float_rn(n));
+            thr[a] = exact ? c[a] : adaptive_threshold(cmn[a], step, k);
+        }
+        float blt[3][6], bgt[3][6];
+        uint32_t nlt[3] = {0, 0, 0};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            box_empty(blt[a]);
+            box_empty(bgt[a]);
+        }
+        const uint32_t maxn = __reduce_max_sync(kFull, work ? n : 0u);
+        for (uint32_t r = 0; r < maxn; ++r) {
+            const bool use = work && r < n;
+            const uint32_t src = use ? s + r : lane;
+            const float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
+                        jl2 = __shfl_sync(kFull, lo[2], src);
+            const float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
+                        jh2 = __shfl_sync(kFull, hi[2], src);
+            if (use) {
+                const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    if (jc[a] < thr[a]) {  // bvh/src/lib.rs:308
+                        box_grow(blt[a], jl0, jl1, jl2, jh0, jh1, jh2);
+                        nlt[a]++;
+                    } else {
+                        box_grow(bgt[a], jl0, jl1, jl2, jh0, jh1, jh2);
+                    }
+                }
+            }
+        }
+        Cand best;
+        best.key = ~0ull;
+        best.n_lt = 0;
+        best.thr = 0.0f;
+        if (work) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const uint32_t ng = n - nlt[a];
+                if (nlt[a] >= P.min_leaf && ng >= P.min_leaf) {  // :407
+                    const float cost =
+                        split_cost(surface_area6(blt[a]), surface_area6(bgt[a]), sa_p, nlt[a], ng);
+                    const uint64_t key = cand_key(cost, a, k);
+                    if (key < best.key) {
+                        best.key = key;
+                        best.n_lt = nlt[a];
+                        best.thr = thr[a];
+                        for (int i = 0; i < 6; ++i) {
+                            best.lt[i] = blt[a][i];
+                            best.gt[i] = bgt[a][i];
+                        }
+                    }
+                }
+            }
+        }
+        // first minimum per segment: (cost, axis, threshold index)
+        const uint32_t bh = static_cast<uint32_t>(best.key >> 32);
+        const uint32_t bl = static_cast<uint32_t>(best.key);
+        const uint32_t mh = __reduce_min_sync(m, bh);
+        const uint32_t ml = __reduce_min_sync(m, bh == mh ? bl : kNoKey);
+        const bool found = work && ml != kNoKey;
+        bool median = false;
+        uint32_t axis = 0, n_lt = 0;
+        Cand win = best;
+        shfl_cand(win, found ? s + (ml & 0xFFu) : lane);
+        if (work && !found) {
+            if (n > P.max_leaf)
+                median = true;  // bvh/src/lib.rs:527-531
+            else
+                leaf = true;  // :576-579
+        }
+        if (found) {
+            axis = (ml >> 8) & 3u;
+            n_lt = win.n_lt;
+            if (n <= P.max_leaf && funkey(mh) >= leaf_cost(n)) leaf = true;  // :583
+        }
+        if (__any_sync(kFull, median)) {
+            // median_split on axes 0, 1, 2 over the same list (:444-491, :528-530)
+            const uint32_t half = n / 2u;
+            uint32_t best_ck = 0;
+            for (uint32_t a = 0; a < 3; ++a) {
+                const uint32_t key = fkey(center_of(lo[a], hi[a]));
+                uint32_t rank = 0;
+                for (uint32_t r = 0; r < maxn; ++r) {
+                    const bool use = median && r < n;
+                    const uint32_t kj = __shfl_sync(kFull, key, use ? s + r : lane);
+                    if (use) rank += (kj < key || (kj == key && s + r < lane)) ? 1u : 0u;
+                }
+                const bool pr = median && rank < half;
+                const uint32_t ltm = __ballot_sync(kFull, pr);
+                const uint32_t dst = median ? (pr ? s + __popc(ltm & m & below)
+                                                  : s + half + __popc(m & ~ltm & below))
+                                            : lane;
+                warp_exchange(dst, lane, lo, hi, id, xchg);
+                const bool in_lt = median && lane < s + half;
+                const bool in_gt = median && lane >= s + half;
+                float ml6[6], mg6[6];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    ml6[i] = funkey(__reduce_min_sync(m, in_lt ? fkey(lo[i]) : kKeyPosInf));
+                    mg6[i] = funkey(__reduce_min_sync(m, in_gt ? fkey(lo[i]) : kKeyPosInf));
+                    ml6[3 + i] = funkey(__reduce_max_sync(m, in_lt ? fkey(hi[i]) : kKeyNegInf));
+                    mg6[3 + i] = funkey(__reduce_max_sync(m, in_gt ? fkey(hi[i]) : kKeyNegInf));
+                }
+                if (median) {
+                    const uint32_t ck =
+                        fkey(split_cost(surface_area6(ml6), surface_area6(mg6), sa_p, half, n - half));
+                    if (a == 0 || ck < best_ck) {
+                        best_ck = ck;
+                        axis = a;
+                        for (int i = 0; i < 6; ++i) {
+                            win.lt[i] = ml6[i];
+                            win.gt[i] = mg6[i];
+                        }
+                    }
+                }
+            }
+            if (median) n_lt = half;
+            if (median && leader) n_median++;
+        }
+        // leaves of this level
+        if (live && leaf) {
+            if (leader) {
+                lane_store_node(O, slot, nb, base + s, n, 0u);
+                if (n > 1u) {
+                    n_holes++;
+                    if (depth == P.max_depth) n_capped++;
+                }
+            }
+            O.perm[base + lane] = id;
+        }
+        const bool split = work && !leaf;
+        // partition (bvh/src/lib.rs:597-612), stable; containment (:637-646)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) c[a] = center_of(lo[a], hi[a]);
+        const float ca = axis == 0 ? c[0] : (axis == 1 ? c[1] : c[2]);
+        const bool pred = median ? lane < s + n_lt : ca < win.thr;
+        const uint32_t ltm = __ballot_sync(kFull, split && pred);
+        if (split && lane == s && static_cast<uint32_t>(__popc(ltm & m)) != n_lt)
+            set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
+        const bool ok = !split || box_contains(pred ? win.lt : win.gt, c[0], c[1], c[2]);
+        if (__any_sync(kFull, !ok) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+        if (split && leader) {
+            lane_store_node(O, slot, nb, base + s, n, pair);
+            any_split = true;
+            hmax = max(hmax, depth);
+        }
+        const uint32_t dst =
+            split ? (pred ? s + __popc(ltm & m & below) : s + n_lt + __popc(m & ~ltm & below)) : lane;
+        warp_exchange(dst, lane, lo, hi, id, xchg);
+        if (split) {
+            const uint32_t n_gt = n - n_lt;
+            if (lane < s + n_lt) {
+                n = n_lt;
+                slot = pair + 1u;
+                pair = pair + 2u * n_gt;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) nb[i] = win.lt[i];
+            } else {
+                s = s + n_lt;
+                n = n_gt;
+                slot = pair;
+                pair = pair + 2u;
+#pragma unroll
+                for (int i = 0; i < 6; ++i) nb[i] = win.gt[i];
+            }
+            depth++;
+        }
+        if (leaf) live = false;
+    }
+    // counters: one atomic per warp
+    const uint32_t hm = __reduce_max_sync(kFull, any_split ? hmax : 0u);
+    const bool anys = __any_sync(kFull, any_split);
+    const uint32_t med = __reduce_add_sync(kFull, n_median);
+    const uint32_t hol = __reduce_add_sync(kFull, n_holes);
+    const uint32_t cap = __reduce_add_sync(kFull, n_capped);
+    if (lane == 0) {
+        if (anys) atomicMax(&O.ctr->height, hm);
+        if (med) atomicAdd(&O.ctr->median_splits, med);
+        if (hol) atomicAdd(&O.ctr->holes, hol);
+        if (cap) atomicAdd(&O.ctr->depth_capped, cap);
+    }
+}
+
+// Subtree of <= 32 objects: the level-synchronous form when every node in it
+// is an adaptive node with one threshold per object, else depth first.
+__device__ __forceinline__ void warp_build(float lo[3], float hi[3], uint32_t id, uint32_t n0,
+                                           uint32_t base, uint32_t slot0, uint32_t pair0,
+                                           uint32_t depth0, const float* bounds0, const Params& P,
+                                           const Out& O, XRec* xchg) {
+    if (P.adaptive_steps == 0 && n0 <= P.adaptive_max_n)
+        warp_build_subtree_levels(lo, hi, id, n0, base, slot0, pair0, depth0, bounds0, P, O, xchg);
+    else
+        warp_build_subtree(lo, hi, id, n0, base, slot0, pair0, depth0, bounds0, P, O, xchg);
+}
+
 }  // namespace mgbvh
