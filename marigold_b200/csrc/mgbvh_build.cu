@@ -256,7 +256,11 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
         }
         return;
     }
-    if (gtid == 0) large[0] = t;
+    if (gtid == 0) {
+        large[0] = t;
+        O.ctr->lvl[0][0] = 1;
+        O.ctr->lvl[0][1] = ntiles;
+    }
     if (blockIdx.x == 0) init_task_bins(bins, threadIdx.x, blockDim.x);
     if (gtid < 6) cbkeys[gtid] = O.ctr->root_keys[6 + gtid];
     for (uint32_t i = gtid; i < ntiles; i += gsz) {
@@ -267,63 +271,70 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
 
 // ---------------------------------------------------------------- large level
 
+// Per-tile bin histograms (count + AABB per axis and bin) of the large nodes
+// with shared-memory atomics, merged into the node's global bins. Grid-stride over
+// the level's tiles; the tile count is read on the device.
 __global__ void __launch_bounds__(kTileThreads) lvl_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* __restrict__ bins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
-    uint32_t* __restrict__ tile_hist, const Rec* __restrict__ rec0, const Rec* __restrict__ rec1,
-    Params P) {
+    uint32_t* __restrict__ tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
+    const Rec* __restrict__ rec1, const Counters* __restrict__ ctr, uint32_t lv, Params P) {
     __shared__ uint32_t sb[kBinWords];
-    const uint32_t tile = blockIdx.x;
-    const uint32_t ti = tile_task[tile];
-    const Task& t = tasks[ti];
-    const uint32_t begin = tile_begin[tile];
-    const uint32_t cnt = min(kTile, t.len - begin);
-    const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
-    init_task_bins(sb, threadIdx.x, blockDim.x);
-    float cmn[3], ext[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        cmn[a] = funkey(cbkeys[6 * ti + a]);
-        ext[a] = __fsub_rn(funkey(cbkeys[6 * ti + 3 + a]), cmn[a]);
-    }
+    const uint32_t ntiles = ctr->lvl[lv][1];
     const uint32_t B = P.bins ? P.bins : 32u;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-        const float4 lo = src[i].lo, hi = src[i].hi;
-        const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        __syncthreads();
+        init_task_bins(sb, threadIdx.x, blockDim.x);
+        const uint32_t ti = tile_task[tile];
+        const Task& t = tasks[ti];
+        const uint32_t begin = tile_begin[tile];
+        const uint32_t cnt = min(kTile, t.len - begin);
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+        float cmn[3], ext[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            if (ext[a] == 0.0f) continue;
-            const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
-            uint32_t* w = sb + (a * 32 + b) * 7;
-            atomicAdd(w, 1u);
-            atomicMin(w + 1, fkey(l[0]));
-            atomicMin(w + 2, fkey(l[1]));
-            atomicMin(w + 3, fkey(l[2]));
-            atomicMax(w + 4, fkey(h[0]));
-            atomicMax(w + 5, fkey(h[1]));
-            atomicMax(w + 6, fkey(h[2]));
+            cmn[a] = funkey(cbkeys[6 * ti + a]);
+            ext[a] = __fsub_rn(funkey(cbkeys[6 * ti + 3 + a]), cmn[a]);
         }
-    }
-    __syncthreads();
-    for (uint32_t w = threadIdx.x; w < 96; w += blockDim.x) tile_hist[tile * 96 + w] = sb[w * 7];
-    uint32_t* gb = bins + (size_t)ti * kBinWords;
-    for (uint32_t k = threadIdx.x; k < kBinWords; k += blockDim.x) {
-        const uint32_t bin = k / 7u, f = k % 7u;
-        const uint32_t v = sb[k];
-        if (sb[bin * 7] == 0) continue;
-        if (f == 0)
-            atomicAdd(gb + k, v);
-        else if (f <= 3)
-            atomicMin(gb + k, v);
-        else
-            atomicMax(gb + k, v);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const float4 lo = src[i].lo, hi = src[i].hi;
+            const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (ext[a] == 0.0f) continue;  // block-uniform
+                const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
+                uint32_t* w = sb + (a * 32 + b) * 7;
+                atomicAdd(w, 1u);
+                atomicMin(w + 1, fkey(l[0]));
+                atomicMin(w + 2, fkey(l[1]));
+                atomicMin(w + 3, fkey(l[2]));
+                atomicMax(w + 4, fkey(h[0]));
+                atomicMax(w + 5, fkey(h[1]));
+                atomicMax(w + 6, fkey(h[2]));
+            }
+        }
+        __syncthreads();
+        for (uint32_t w = threadIdx.x; w < 96; w += blockDim.x)
+            tile_hist[(size_t)w * cap_tiles + tile] = sb[w * 7];
+        uint32_t* gb = bins + (size_t)ti * kBinWords;
+        for (uint32_t k = threadIdx.x; k < kBinWords; k += blockDim.x) {
+            const uint32_t bin = k / 7u, f = k % 7u;
+            const uint32_t v = sb[k];
+            if (sb[bin * 7] == 0) continue;
+            if (f == 0)
+                atomicAdd(gb + k, v);
+            else if (f <= 3)
+                atomicMin(gb + k, v);
+            else
+                atomicMax(gb + k, v);
+        }
     }
 }
 
 struct EvalArgs {
     const Task* tasks;
-    uint32_t n_tasks;
+    uint32_t lv;  // level parity: counts in ctr->lvl[lv], next level's in ctr->lvl[lv ^ 1]
     const uint32_t* bins;
     const uint32_t* cbkeys;
     const uint32_t* tile_hist;
@@ -339,10 +350,7 @@ struct EvalArgs {
     uint32_t cap_tasks, cap_tiles, cap_medium, cap_small;
 };
 
-__global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= A.n_tasks) return;
+__device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
     const Task t = A.tasks[w];
     const uint32_t* tb = A.bins + (size_t)w * kBinWords;
     float cmn[3], ext[3];
@@ -419,8 +427,8 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
         const uint32_t ti = b0 + lane;
         uint32_t v = 0;
         if (ti < t.ntiles) {
-            const uint32_t* h = A.tile_hist + (size_t)(t.tile0 + ti) * 96 + d.axis * 32;
-            for (uint32_t b = 0; b < d.split_bin; ++b) v += h[b];
+            const uint32_t* h = A.tile_hist + (size_t)(d.axis * 32) * A.cap_tiles + t.tile0 + ti;
+            for (uint32_t b = 0; b < d.split_bin; ++b) v += h[(size_t)b * A.cap_tiles];
         }
         uint32_t inc = v;
 #pragma unroll
@@ -467,8 +475,8 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
             const uint32_t nt = (len + kTile - 1) / kTile;
             uint32_t ti = 0, t0 = 0;
             if (lane == 0) {
-                ti = atomicAdd(&O.ctr->n_next_large, 1u);
-                t0 = atomicAdd(&O.ctr->n_next_tiles, nt);
+                ti = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][0], 1u);
+                t0 = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][1], nt);
             }
             ti = __shfl_sync(kFull, ti, 0);
             t0 = __shfl_sync(kFull, t0, 0);
@@ -509,103 +517,117 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
     if (lane == 0) A.dec[w] = d;
 }
 
+__global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_tasks; w += nwarps)
+        eval_task(A, P, O, w, lane);
+}
+
+// Stable partition of the large nodes' records into the other buffer: lt
+// records to the front of the node in order, gt records after them in order,
+// one block scan per round of 256 records. Grid-stride over the level's tiles;
+// also reduces the large children's centroid bounds.
 __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
     const Task* __restrict__ tasks, const Decision* __restrict__ dec,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
-    const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, uint32_t* next_cbkeys, Out O) {
+    const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, uint32_t* next_cbkeys, uint32_t lv,
+    Out O) {
     __shared__ uint32_t wcnt[kTileThreads / 32];
     __shared__ uint32_t sk[12];
-    const uint32_t tile = blockIdx.x;
-    const uint32_t ti = tile_task[tile];
-    const Task t = tasks[ti];
-    const Decision d = dec[ti];
-    const uint32_t begin = tile_begin[tile];
-    const uint32_t cnt = min(kTile, t.len - begin);
-    const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
-    Rec* dst = t.buf ? rec0 : rec1;
-    if (d.kind == 1) {
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-            O.perm[t.start + begin + i] = __float_as_uint(src[i].lo.w);
-        return;
-    }
+    const uint32_t ntiles = O.ctr->lvl[lv][1];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
-    const uint32_t lt_off = tile_lt[tile];
-    const uint32_t lt_base = t.start + lt_off;
-    const uint32_t gt_base = t.start + d.n_lt + (begin - lt_off);
-    // child centroid bounds: k[0..5] lt (min xyz, max xyz), k[6..11] gt
-    uint32_t k[12];
-    init_key12(k);
-    if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
-    bool bad = false;
-    uint32_t run_lt = 0;
-    for (uint32_t r = 0; r < cnt; r += blockDim.x) {
-        const uint32_t i = r + threadIdx.x;
-        const bool valid = i < cnt;
-        Rec rec;
-        rec.lo = rec.hi = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) rec = src[i];
-        const float c[3] = {center_of(rec.lo.x, rec.hi.x), center_of(rec.lo.y, rec.hi.y),
-                            center_of(rec.lo.z, rec.hi.z)};
-        const float ca = d.axis == 0 ? c[0] : (d.axis == 1 ? c[1] : c[2]);
-        const bool pred = valid && bin_of(ca, d.cmin, d.ext, d.bins) < d.split_bin;
-        const uint32_t m = __ballot_sync(kFull, pred);
-        if (lane == 0) wcnt[warp] = __popc(m);
-        __syncthreads();
-        uint32_t wpre = 0, tot = 0;
-        for (uint32_t q = 0; q < blockDim.x / 32; ++q) {
-            const uint32_t v = wcnt[q];
-            if (q < warp) wpre += v;
-            tot += v;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t ti = tile_task[tile];
+        const Task t = tasks[ti];
+        const Decision d = dec[ti];
+        const uint32_t begin = tile_begin[tile];
+        const uint32_t cnt = min(kTile, t.len - begin);
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+        Rec* dst = t.buf ? rec0 : rec1;
+        if (d.kind == 1) {
+            for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+                O.perm[t.start + begin + i] = __float_as_uint(src[i].lo.w);
+            continue;
         }
-        __syncthreads();
-        if (valid) {
-            const uint32_t ltr = run_lt + wpre + __popc(m & below);
-            const uint32_t side = pred ? 1u : 0u;  // child index: 0 gt, 1 lt
-            const uint32_t dest = pred ? lt_base + ltr : gt_base + (i - ltr);
-            if (dest - t.start < t.len) {
-                dst[dest] = rec;
-                if (d.child_leaf[side]) O.perm[dest] = __float_as_uint(rec.lo.w);
-            } else {
-                bad = true;  // inconsistent counts; never write outside the node
+        const uint32_t lt_off = tile_lt[tile];
+        const uint32_t lt_base = t.start + lt_off;
+        const uint32_t gt_base = t.start + d.n_lt + (begin - lt_off);
+        uint32_t k[12];
+        init_key12(k);
+        if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+        bool bad = false;
+        uint32_t run_lt = 0;
+        for (uint32_t r = 0; r < cnt; r += blockDim.x) {
+            const uint32_t i = r + threadIdx.x;
+            const bool valid = i < cnt;
+            Rec rec;
+            rec.lo = rec.hi = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (valid) rec = src[i];
+            const float c[3] = {center_of(rec.lo.x, rec.hi.x), center_of(rec.lo.y, rec.hi.y),
+                                center_of(rec.lo.z, rec.hi.z)};
+            const float ca = d.axis == 0 ? c[0] : (d.axis == 1 ? c[1] : c[2]);
+            const bool pred = valid && bin_of(ca, d.cmin, d.ext, d.bins) < d.split_bin;
+            const uint32_t m = __ballot_sync(kFull, pred);
+            if (lane == 0) wcnt[warp] = __popc(m);
+            __syncthreads();
+            uint32_t wpre = 0, tot = 0;
+            for (uint32_t q = 0; q < blockDim.x / 32; ++q) {
+                const uint32_t v = wcnt[q];
+                if (q < warp) wpre += v;
+                tot += v;
             }
-            bad |= !box_contains(pred ? d.ltb : d.gtb, c[0], c[1], c[2]);
-            uint32_t* kk = pred ? k : k + 6;
+            __syncthreads();
+            if (valid) {
+                const uint32_t ltr = run_lt + wpre + __popc(m & below);
+                const uint32_t side = pred ? 1u : 0u;  // child index: 0 gt, 1 lt
+                const uint32_t dest = pred ? lt_base + ltr : gt_base + (i - ltr);
+                if (dest - t.start < t.len) {
+                    dst[dest] = rec;
+                    if (d.child_leaf[side]) O.perm[dest] = __float_as_uint(rec.lo.w);
+                } else {
+                    bad = true;  // inconsistent counts; never write outside the node
+                }
+                bad |= !box_contains(pred ? d.ltb : d.gtb, c[0], c[1], c[2]);
+                uint32_t* kk = pred ? k : k + 6;
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                kk[a] = min(kk[a], fkey(c[a]));
-                kk[3 + a] = max(kk[3 + a], fkey(c[a]));
+                for (int a = 0; a < 3; ++a) {
+                    kk[a] = min(kk[a], fkey(c[a]));
+                    kk[3 + a] = max(kk[3 + a], fkey(c[a]));
+                }
             }
+            run_lt += tot;
         }
-        run_lt += tot;
-    }
-    if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
-    // centroid bounds of the large children
-    const bool need_lt = d.child_task[1] != kNone, need_gt = d.child_task[0] != kNone;
-    if (need_lt || need_gt) {
+        if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+        const bool need_lt = d.child_task[1] != kNone, need_gt = d.child_task[0] != kNone;
+        if (need_lt || need_gt) {
 #pragma unroll
-        for (int q = 0; q < 12; ++q) {
-            const bool is_min = (q % 6) < 3;
-            const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
-            if (lane == 0) {
-                if (is_min)
-                    atomicMin(&sk[q], v);
-                else
-                    atomicMax(&sk[q], v);
+            for (int q = 0; q < 12; ++q) {
+                const bool is_min = (q % 6) < 3;
+                const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+                if (lane == 0) {
+                    if (is_min)
+                        atomicMin(&sk[q], v);
+                    else
+                        atomicMax(&sk[q], v);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < 12) {
+                const uint32_t q = threadIdx.x;
+                const uint32_t child = q < 6 ? d.child_task[1] : d.child_task[0];
+                if (child != kNone) {
+                    uint32_t* g = next_cbkeys + 6 * child + (q % 6);
+                    if ((q % 6) < 3)
+                        atomicMin(g, sk[q]);
+                    else
+                        atomicMax(g, sk[q]);
+                }
             }
         }
-        __syncthreads();
-        if (threadIdx.x < 12) {
-            const uint32_t q = threadIdx.x;
-            const uint32_t child = q < 6 ? d.child_task[1] : d.child_task[0];
-            if (child != kNone) {
-                uint32_t* g = next_cbkeys + 6 * child + (q % 6);
-                if ((q % 6) < 3)
-                    atomicMin(g, sk[q]);
-                else
-                    atomicMax(g, sk[q]);
-            }
-        }
+        __syncthreads();  // sk and wcnt are rewritten by the next tile
     }
 }
 
@@ -713,13 +735,11 @@ __device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
         k[q] = ((q % 6) < 3) ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
 }
 
-__global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
-                                                                Rec* rec0, Rec* rec1, Task* small,
-                                                                uint32_t cap_small, Params P, Out O) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
+// One CTA builds the subtree of one medium node (33..1024 objects).
+__device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* rec0, Rec* rec1,
+                                            Task* small, uint32_t cap_small, const Params& P,
+                                            const Out& O) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const Task t = tasks[blockIdx.x];
     Rec* src = (t.buf ? rec1 : rec0) + t.start;
     const uint32_t base = t.start;
     uint32_t k[12];
@@ -1003,9 +1023,25 @@ __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __re
     }
 }
 
+__global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
+                                                                Rec* rec0, Rec* rec1, Task* small,
+                                                                uint32_t cap_small, Params P, Out O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
+    const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
+    for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
+        __syncthreads();
+        medium_task(S, tasks[ti], rec0, rec1, small, cap_small, P, O);
+    }
+}
+
 // ---------------------------------------------------------------- small
 
-__global__ void __launch_bounds__(256, 2) small_kernel(const Task* __restrict__ tasks,
+// One warp per subtree of <= 32 objects. kLevels: the level-synchronous
+// builder (every node adaptive with one threshold per object); otherwise the
+// depth-first builder that also covers binned nodes and fixed step counts.
+template <bool kLevels>
+__global__ void __launch_bounds__(256) small_kernel(const Task* __restrict__ tasks,
                                                    const Rec* __restrict__ rec0,
                                                    const Rec* __restrict__ rec1, Params P, Out O) {
     __shared__ XRec xchg[8][32];
@@ -1027,7 +1063,12 @@ __global__ void __launch_bounds__(256, 2) small_kernel(const Task* __restrict__ 
             hi[2] = r.hi.z;
         }
         const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-        warp_build(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O, xchg[wib]);
+        if constexpr (kLevels)
+            warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O,
+                                      xchg[wib]);
+        else
+            warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O,
+                               xchg[wib]);
     }
 }
 
@@ -1069,6 +1110,7 @@ struct DevBuf {
 struct mgbvh_ctx {
     int device = 0;
     int sm_count = 148;
+    uint32_t levels_hint = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp[3] = {nullptr, nullptr, nullptr};
@@ -1186,7 +1228,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
         ENS(ctx->tile_task[i], 4ull * C.tiles);
         ENS(ctx->tile_begin[i], 4ull * C.tiles);
     }
-    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);
+    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);  // [axis][bin][tile]
     ENS(ctx->tile_lt, 4ull * C.tiles);
     ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
     ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
@@ -1245,63 +1287,77 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
     uint32_t launches = 2, levels = 0;
+    (void)ntiles0;
 
-    uint32_t n_tasks = cls == 3 ? 1u : 0u, n_tiles = ntiles0;
-    uint32_t cur = 0;
-    while (n_tasks > 0) {
-        launches += 3;
-        levels++;
-        const uint32_t nx = cur ^ 1u;
-        lvl_bin_kernel<<<n_tiles, kTileThreads, 0, sm>>>(
-            P_<Task>(ctx->tasks[cur]), P_<uint32_t>(ctx->cbkeys[cur]), P_<uint32_t>(ctx->bins[cur]),
-            P_<uint32_t>(ctx->tile_task[cur]), P_<uint32_t>(ctx->tile_begin[cur]),
-            P_<uint32_t>(ctx->tile_hist), rec0, rec1, P);
-        MG_CUDA(cudaMemsetAsync(&d_ctr->n_next_large, 0, 8, sm));
-        EvalArgs A;
-        A.tasks = P_<Task>(ctx->tasks[cur]);
-        A.n_tasks = n_tasks;
-        A.bins = P_<uint32_t>(ctx->bins[cur]);
-        A.cbkeys = P_<uint32_t>(ctx->cbkeys[cur]);
-        A.tile_hist = P_<uint32_t>(ctx->tile_hist);
-        A.tile_lt = P_<uint32_t>(ctx->tile_lt);
-        A.dec = P_<Decision>(ctx->dec);
-        A.next_tasks = P_<Task>(ctx->tasks[nx]);
-        A.next_bins = P_<uint32_t>(ctx->bins[nx]);
-        A.next_cbkeys = P_<uint32_t>(ctx->cbkeys[nx]);
-        A.next_tile_task = P_<uint32_t>(ctx->tile_task[nx]);
-        A.next_tile_begin = P_<uint32_t>(ctx->tile_begin[nx]);
-        A.medium = P_<Task>(ctx->medium);
-        A.small = P_<Task>(ctx->small);
-        A.cap_tasks = C.tasks;
-        A.cap_tiles = C.tiles;
-        A.cap_medium = C.medium;
-        A.cap_small = C.small;
-        lvl_eval_kernel<<<(n_tasks + 3) / 4, 128, 0, sm>>>(A, P, O);
-        lvl_part_kernel<<<n_tiles, kTileThreads, 0, sm>>>(
-            P_<Task>(ctx->tasks[cur]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[cur]),
-            P_<uint32_t>(ctx->tile_begin[cur]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
-            P_<uint32_t>(ctx->cbkeys[nx]), O);
+    // Level passes over the large nodes. Kernels read their task and tile
+    // counts on the device, so levels are launched in batches and the host
+    // reads the next level's count only at the end of a batch.
+    const int tile_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * 4u);
+    const int eval_grid = (int)std::min<uint32_t>((C.tasks + 3) / 4, (uint32_t)ctx->sm_count * 4u);
+    uint32_t level = 0;
+    bool more = cls == 3;
+    ctx->h_ctr->error = 0;
+    bool first_batch = true;
+    while (more) {
+        const uint32_t batch = first_batch ? std::max(ctx->levels_hint, 4u) : 2u;
+        first_batch = false;
+        for (uint32_t bl = 0; bl < batch; ++bl, ++level) {
+            const uint32_t lv = level & 1u, nx = lv ^ 1u;
+            launches += 3;
+            lvl_bin_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+                P_<Task>(ctx->tasks[lv]), P_<uint32_t>(ctx->cbkeys[lv]), P_<uint32_t>(ctx->bins[lv]),
+                P_<uint32_t>(ctx->tile_task[lv]), P_<uint32_t>(ctx->tile_begin[lv]),
+                P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, d_ctr, lv, P);
+            MG_CUDA(cudaMemsetAsync(&d_ctr->lvl[nx][0], 0, 8, sm));
+            EvalArgs A;
+            A.tasks = P_<Task>(ctx->tasks[lv]);
+            A.lv = lv;
+            A.bins = P_<uint32_t>(ctx->bins[lv]);
+            A.cbkeys = P_<uint32_t>(ctx->cbkeys[lv]);
+            A.tile_hist = P_<uint32_t>(ctx->tile_hist);
+            A.tile_lt = P_<uint32_t>(ctx->tile_lt);
+            A.dec = P_<Decision>(ctx->dec);
+            A.next_tasks = P_<Task>(ctx->tasks[nx]);
+            A.next_bins = P_<uint32_t>(ctx->bins[nx]);
+            A.next_cbkeys = P_<uint32_t>(ctx->cbkeys[nx]);
+            A.next_tile_task = P_<uint32_t>(ctx->tile_task[nx]);
+            A.next_tile_begin = P_<uint32_t>(ctx->tile_begin[nx]);
+            A.medium = P_<Task>(ctx->medium);
+            A.small = P_<Task>(ctx->small);
+            A.cap_tasks = C.tasks;
+            A.cap_tiles = C.tiles;
+            A.cap_medium = C.medium;
+            A.cap_small = C.small;
+            lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+            lvl_part_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+                P_<Task>(ctx->tasks[lv]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[lv]),
+                P_<uint32_t>(ctx->tile_begin[lv]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
+                P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
+        }
         MG_CUDA(cudaGetLastError());
         MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
         MG_CUDA(cudaStreamSynchronize(sm));
         if (ctx->h_ctr->error) break;
-        n_tasks = ctx->h_ctr->n_next_large;
-        n_tiles = ctx->h_ctr->n_next_tiles;
-        cur = nx;
+        more = ctx->h_ctr->lvl[level & 1u][0] > 0;
     }
-    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
-    MG_CUDA(cudaStreamSynchronize(sm));
+    if (cls == 3) {
+        // levels that did work: the count of the last non-empty level
+        ctx->levels_hint = level;
+        levels = level;
+    }
     MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
     if (!ctx->h_ctr->error) {
-        const uint32_t n_medium = ctx->h_ctr->n_medium, n_small = ctx->h_ctr->n_small;
-        if (n_medium > 0) {
-            medium_kernel<<<n_medium, kMediumThreads, sizeof(MediumSmem), sm>>>(
-                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O);
-            launches++;
-        }
+        // medium subtrees: count read on the device
+        const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
+        medium_kernel<<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+            P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O);
+        launches++;
         MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
         // small subtrees: count read on the device; grid sized for full occupancy
-        small_kernel<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
+        if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
+            small_kernel<true><<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
+        else
+            small_kernel<false><<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
         launches++;
         MG_CUDA(cudaGetLastError());
     } else {

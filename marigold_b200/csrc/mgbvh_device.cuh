@@ -38,12 +38,10 @@ struct Counters {
     uint32_t median_splits;
     uint32_t depth_capped;  // leaves cut by max_depth holding > 1 object
     uint32_t holes;         // leaves holding > 1 object (node slots to compact)
-    uint32_t n_next_large;
-    uint32_t n_next_tiles;
+    uint32_t lvl[2][2];     // [level & 1] {large tasks, tiles} of a level pass
     uint32_t n_medium;
     uint32_t n_small;
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
-    uint32_t pad[2];
 };
 
 enum ErrorSite : uint32_t {
@@ -535,6 +533,44 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
     }
 }
 
+// Segmented reductions over contiguous lane ranges [s, end): shuffle-down
+// tree bounded by the segment end, then a broadcast from the segment's first
+// lane. Every lane takes part with full masks (no per-segment masks, which
+// would split the warp).
+__device__ __forceinline__ uint32_t seg_min(uint32_t v, uint32_t lane, uint32_t s, uint32_t end) {
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t u = __shfl_down_sync(kFull, v, d);
+        if (lane + d < end) v = min(v, u);
+    }
+    return __shfl_sync(kFull, v, s);
+}
+
+__device__ __forceinline__ uint32_t seg_max(uint32_t v, uint32_t lane, uint32_t s, uint32_t end) {
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t u = __shfl_down_sync(kFull, v, d);
+        if (lane + d < end) v = max(v, u);
+    }
+    return __shfl_sync(kFull, v, s);
+}
+
+// Lexicographic (hi, lo) minimum over the segment.
+__device__ __forceinline__ void seg_min2(uint32_t& hi, uint32_t& lo, uint32_t lane, uint32_t s,
+                                         uint32_t end) {
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t uh = __shfl_down_sync(kFull, hi, d);
+        const uint32_t ul = __shfl_down_sync(kFull, lo, d);
+        if (lane + d < end && (uh < hi || (uh == hi && ul < lo))) {
+            hi = uh;
+            lo = ul;
+        }
+    }
+    hi = __shfl_sync(kFull, hi, s);
+    lo = __shfl_sync(kFull, lo, s);
+}
+
 // Lanes [s, s+n) as a mask.
 __device__ __forceinline__ uint32_t seg_mask(uint32_t s, uint32_t n) {
     return n >= 32u ? kFull : (((1u << n) - 1u) << s);
@@ -593,6 +629,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
 
     while (__any_sync(kFull, live)) {
         const uint32_t m = live ? seg_mask(s, n) : (1u << lane);
+        const uint32_t ss = live ? s : lane, se = live ? s + n : lane + 1u;  // reduction range
         const bool leader = live && lane == s;
         bool leaf = n <= 1u || depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf);
         const bool work = live && !leaf;
@@ -603,8 +640,8 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         float cmn[3], ext[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            cmn[a] = funkey(__reduce_min_sync(m, work ? fkey(c[a]) : kKeyPosInf));
-            const float cmx = funkey(__reduce_max_sync(m, work ? fkey(c[a]) : kKeyNegInf));
+            cmn[a] = funkey(seg_min(work ? fkey(c[a]) : kKeyPosInf, lane, ss, se));
+            const float cmx = funkey(seg_max(work ? fkey(c[a]) : kKeyNegInf, lane, ss, se));
             ext[a] = __fsub_rn(cmx, cmn[a]);
         }
         const float sa_p = surface_area6(nb);
@@ -624,24 +661,39 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             box_empty(bgt[a]);
         }
         const uint32_t maxn = __reduce_max_sync(kFull, work ? n : 0u);
+        const float kInf = __int_as_float(0x7F800000), kNegInf = __int_as_float(0xFF800000);
         for (uint32_t r = 0; r < maxn; ++r) {
             const bool use = work && r < n;
             const uint32_t src = use ? s + r : lane;
-            const float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
-                        jl2 = __shfl_sync(kFull, lo[2], src);
-            const float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
-                        jh2 = __shfl_sync(kFull, hi[2], src);
-            if (use) {
-                const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
+            float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
+                  jl2 = __shfl_sync(kFull, lo[2], src);
+            float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
+                  jh2 = __shfl_sync(kFull, hi[2], src);
+            // an unused slot becomes the empty box: its centroid is NaN, so it
+            // lands on the gt side and merging it changes nothing
+            jl0 = use ? jl0 : kInf;
+            jl1 = use ? jl1 : kInf;
+            jl2 = use ? jl2 : kInf;
+            jh0 = use ? jh0 : kNegInf;
+            jh1 = use ? jh1 : kNegInf;
+            jh2 = use ? jh2 : kNegInf;
+            const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    if (jc[a] < thr[a]) {  // bvh/src/lib.rs:308
-                        box_grow(blt[a], jl0, jl1, jl2, jh0, jh1, jh2);
-                        nlt[a]++;
-                    } else {
-                        box_grow(bgt[a], jl0, jl1, jl2, jh0, jh1, jh2);
-                    }
-                }
+            for (int a = 0; a < 3; ++a) {
+                const bool L = jc[a] < thr[a];  // bvh/src/lib.rs:308
+                blt[a][0] = fminf(blt[a][0], L ? jl0 : kInf);
+                blt[a][1] = fminf(blt[a][1], L ? jl1 : kInf);
+                blt[a][2] = fminf(blt[a][2], L ? jl2 : kInf);
+                blt[a][3] = fmaxf(blt[a][3], L ? jh0 : kNegInf);
+                blt[a][4] = fmaxf(blt[a][4], L ? jh1 : kNegInf);
+                blt[a][5] = fmaxf(blt[a][5], L ? jh2 : kNegInf);
+                bgt[a][0] = fminf(bgt[a][0], L ? kInf : jl0);
+                bgt[a][1] = fminf(bgt[a][1], L ? kInf : jl1);
+                bgt[a][2] = fminf(bgt[a][2], L ? kInf : jl2);
+                bgt[a][3] = fmaxf(bgt[a][3], L ? kNegInf : jh0);
+                bgt[a][4] = fmaxf(bgt[a][4], L ? kNegInf : jh1);
+                bgt[a][5] = fmaxf(bgt[a][5], L ? kNegInf : jh2);
+                nlt[a] += L ? 1u : 0u;
             }
         }
         Cand best;
@@ -669,10 +721,9 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             }
         }
         // first minimum per segment: (cost, axis, threshold index)
-        const uint32_t bh = static_cast<uint32_t>(best.key >> 32);
-        const uint32_t bl = static_cast<uint32_t>(best.key);
-        const uint32_t mh = __reduce_min_sync(m, bh);
-        const uint32_t ml = __reduce_min_sync(m, bh == mh ? bl : kNoKey);
+        uint32_t mh = static_cast<uint32_t>(best.key >> 32);
+        uint32_t ml = static_cast<uint32_t>(best.key);
+        seg_min2(mh, ml, lane, ss, se);
         const bool found = work && ml != kNoKey;
         bool median = false;
         uint32_t axis = 0, n_lt = 0;
@@ -712,10 +763,10 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
                 float ml6[6], mg6[6];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    ml6[i] = funkey(__reduce_min_sync(m, in_lt ? fkey(lo[i]) : kKeyPosInf));
-                    mg6[i] = funkey(__reduce_min_sync(m, in_gt ? fkey(lo[i]) : kKeyPosInf));
-                    ml6[3 + i] = funkey(__reduce_max_sync(m, in_lt ? fkey(hi[i]) : kKeyNegInf));
-                    mg6[3 + i] = funkey(__reduce_max_sync(m, in_gt ? fkey(hi[i]) : kKeyNegInf));
+                    ml6[i] = funkey(seg_min(in_lt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se));
+                    mg6[i] = funkey(seg_min(in_gt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se));
+                    ml6[3 + i] = funkey(seg_max(in_lt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se));
+                    mg6[3 + i] = funkey(seg_max(in_gt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se));
                 }
                 if (median) {
                     const uint32_t ck =
