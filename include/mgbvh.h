@@ -65,8 +65,12 @@ typedef enum mgbvh_status {
        (bvh/src/lib.rs:588, 618-646): child counts or centroid containment. */
     MGBVH_ERR_ASSERT = -5,
     MGBVH_ERR_UNSUPPORTED = -6, /* a knob or size outside this build's limits */
-    MGBVH_ERR_NO_DEVICE = -7
+    MGBVH_ERR_NO_DEVICE = -7,
+    MGBVH_ERR_TOO_LARGE = -8    /* above MGBVH_NOALLOC_MAX_OBJECTS (allocation-free build) */
 } mgbvh_status;
+
+/* Largest object count mgbvh_build_aabbs_noalloc accepts. */
+#define MGBVH_NOALLOC_MAX_OBJECTS 1024
 
 /* One node, 32 bytes. For MAX_LEAF_OBJECTS == 1 these are exactly the bytes
    AsGpuBytes writes (bvh/src/lib.rs:163-169) and scene.slang's BvhNode reads.
@@ -184,6 +188,37 @@ MGBVH_API int mgbvh_build_aabbs_dev(mgbvh_ctx* ctx, const float* d_aabbs, uint32
                           const mgbvh_settings* settings, mgbvh_node* d_out_nodes,
                           uint32_t node_capacity, uint32_t* out_node_count, uint32_t* d_out_lens,
                           uint32_t* d_out_perm, mgbvh_stats* out_stats);
+
+/*
+ * Allocation-free build over device-resident AABBs. This entry point has no
+ * counterpart in the reference. It exists for callers that must not allocate
+ * while they build: a render loop that rebuilds its TLAS every frame (as
+ * marigold does over its instances) cannot afford cudaMalloc/cudaFree there,
+ * because those calls can synchronize the whole device and stall the frame,
+ * and a host engine that hands all device memory out through its own pool
+ * may not allocate behind its back. mgbvh_build_aabbs_dev needs an mgbvh_ctx,
+ * whose creation and growth allocate; this call needs no context.
+ *
+ * Limits: count <= MGBVH_NOALLOC_MAX_OBJECTS (1024), else
+ * MGBVH_ERR_TOO_LARGE. Scratch is one fixed array inside the library (about
+ * 140 KB of device memory on every device that loads the library, held until
+ * the process exits), shared by all calls: calls whose work overlaps on the
+ * GPU (several host threads, or several streams) race on it and must be
+ * serialized by the caller. The first call on each device does a one-time
+ * set-up on the current device (looks up the array's device address, sets a
+ * kernel attribute), so make that first call before any stream capture.
+ *
+ * Same tree, permutation and status codes as mgbvh_build_aabbs_dev.
+ * d_aabbs, d_out_nodes, d_out_lens (nullable) and d_out_perm are device
+ * pointers on the current device; out_node_count is a host pointer. Runs on
+ * cuda_stream (cudaStream_t, NULL = legacy default stream) and returns after
+ * the build has finished. Calls no allocating routine of CUDA or any library.
+ */
+MGBVH_API int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count,
+                                        const mgbvh_settings* settings, mgbvh_node* d_out_nodes,
+                                        uint32_t node_capacity, uint32_t* out_node_count,
+                                        uint32_t* d_out_lens, uint32_t* d_out_perm,
+                                        void* cuda_stream);
 
 /*
  * AsGpuBytes for BvhNode (bvh/src/lib.rs:157-212), host side: 8 u32 words per

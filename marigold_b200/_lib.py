@@ -22,13 +22,15 @@ ERR_TIMEOUT = -4
 ERR_ASSERT = -5
 ERR_UNSUPPORTED = -6
 ERR_NO_DEVICE = -7
+ERR_TOO_LARGE = -8
+NOALLOC_MAX_OBJECTS = 1024
 
 # every entry point declared in include/mgbvh.h
 EXPORTED = (
     "mgbvh_default_settings", "mgbvh_create", "mgbvh_destroy", "mgbvh_set_stream",
     "mgbvh_last_error", "mgbvh_status_string", "mgbvh_build_indexed", "mgbvh_build_aabbs",
     "mgbvh_build_indexed_dev", "mgbvh_build_aabbs_dev", "mgbvh_encode_gpu_bytes",
-    "mgbvh_sah_cost",
+    "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc",
 )
 
 
@@ -128,6 +130,9 @@ def load():
         L.mgbvh_build_aabbs_dev.restype = ctypes.c_int
         L.mgbvh_encode_gpu_bytes.argtypes = [P, P, u32, u32, P]
         L.mgbvh_encode_gpu_bytes.restype = ctypes.c_int
+        L.mgbvh_build_aabbs_noalloc.argtypes = [P, u32, ctypes.POINTER(Settings), P, u32, pu32, P,
+                                                P, P]
+        L.mgbvh_build_aabbs_noalloc.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]
         L.mgbvh_sah_cost.restype = ctypes.c_double
         _lib = L

@@ -25,6 +25,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -1092,6 +1094,86 @@ __global__ void compact_kernel(const mgbvh_node* __restrict__ src, const uint32_
     }
 }
 
+
+// ---------------------------------------------------------------- allocation-free build
+//
+// Scratch of mgbvh_build_aabbs_noalloc lives in this file-scope device array,
+// part of the library image: every device that loads the library holds it
+// (about 140 KB) until the process exits. All calls share it, so calls that
+// overlap on the GPU race on it; each call clears what must start at zero.
+constexpr uint32_t kNoAllocMax = 1024;  // objects per allocation-free build (= kMediumMax)
+
+struct NoAllocScratch {
+    Rec rec[kNoAllocMax];
+    Task medium[1];
+    Task small[kNoAllocMax / 2 + 8];
+    mgbvh_node nodes[2 * kNoAllocMax - 1];
+    uint32_t lens[2 * kNoAllocMax - 1];
+    uint8_t used[2 * kNoAllocMax];
+    Counters ctr;
+    uint32_t count;  // nodes written to the caller's array
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// Counters to their initial state and every node slot of this build unused.
+__global__ void noalloc_init_kernel(NoAllocScratch* S, uint32_t slots) {
+    for (uint32_t i = threadIdx.x; i < slots; i += blockDim.x) S->used[i] = 0;
+    uint32_t* c = reinterpret_cast<uint32_t*>(&S->ctr);
+    for (uint32_t i = threadIdx.x; i < sizeof(Counters) / 4; i += blockDim.x) c[i] = 0;
+    __syncthreads();
+    if (threadIdx.x < 12) S->ctr.root_keys[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    if (threadIdx.x == 0) S->count = 0;
+}
+
+// Drops unused slots (leaves holding more than one object leave holes) and
+// writes the nodes, with remapped child links, to the caller's array.
+__global__ void __launch_bounds__(1024) noalloc_finish_kernel(NoAllocScratch* S, uint32_t slots,
+                                                              mgbvh_node* out, uint32_t* out_lens,
+                                                              uint32_t cap) {
+    __shared__ uint32_t newidx[2 * kNoAllocMax];
+    __shared__ uint32_t wsum[32];
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const uint32_t u0 = (2 * t < slots) ? S->used[2 * t] : 0u;
+    const uint32_t u1 = (2 * t + 1 < slots) ? S->used[2 * t + 1] : 0u;
+    const uint32_t v = u0 + u1;
+    uint32_t inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t x = __shfl_up_sync(kFull, inc, d);
+        if (lane >= static_cast<uint32_t>(d)) inc += x;
+    }
+    if (lane == 31) wsum[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = wsum[lane];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t x = __shfl_up_sync(kFull, w, d);
+            if (lane >= static_cast<uint32_t>(d)) w += x;
+        }
+        wsum[lane] = w;  // inclusive
+    }
+    __syncthreads();
+    const uint32_t excl = (warp ? wsum[warp - 1] : 0u) + inc - v;
+    newidx[2 * t] = excl;
+    newidx[2 * t + 1] = excl + u0;
+    const uint32_t total = wsum[31];
+    __syncthreads();
+    if (t == 0) S->count = total;
+    if (total > cap) {
+        if (t == 0) set_error(&S->ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+        return;
+    }
+    for (uint32_t s = t; s < slots; s += blockDim.x) {
+        if (!S->used[s]) continue;
+        mgbvh_node nd = S->nodes[s];
+        if (nd.child_node) nd.child_node = newidx[nd.child_node];
+        out[newidx[s]] = nd;
+        if (out_lens) out_lens[newidx[s]] = S->lens[s];
+    }
+}
+
 }  // namespace mgbvh
 
 // =================================================================== host
@@ -1666,6 +1748,8 @@ const char* mgbvh_status_string(int status) {
         case MGBVH_ERR_ASSERT: return "reference assertion would fail";
         case MGBVH_ERR_UNSUPPORTED: return "unsupported";
         case MGBVH_ERR_NO_DEVICE: return "no CUDA device";
+        case MGBVH_ERR_TOO_LARGE:
+            return "more objects than the allocation-free build holds (1024)";
         default: return "unknown status";
     }
 }
@@ -1759,6 +1843,104 @@ double mgbvh_sah_cost(const mgbvh_node* nodes, const uint32_t* lens, uint32_t co
         c += nodes[i].child_node ? (double)kDepthCost * r : (double)kObjectCost * lens[i] * r;
     }
     return c;
+}
+
+
+// Allocation-free build (see include/mgbvh.h). Per-device set-up, done by the
+// first call on each device: the scratch array's device address and the
+// medium kernel's shared-memory limit.
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+int g_noalloc_sms[64] = {};
+}  // namespace
+
+int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_settings* settings,
+                              mgbvh_node* d_out_nodes, uint32_t node_capacity,
+                              uint32_t* out_node_count, uint32_t* d_out_lens, uint32_t* d_out_perm,
+                              void* cuda_stream) {
+    if (!out_node_count) return MGBVH_ERR_INVALID_ARG;
+    *out_node_count = 0;
+    int rc = validate_settings(nullptr, settings);
+    if (rc != MGBVH_OK) return rc;
+    if (count == 0) return MGBVH_WARN_EMPTY;
+    if (count > kNoAllocMax) return MGBVH_ERR_TOO_LARGE;
+    if (!d_aabbs || !d_out_nodes || !d_out_perm) return MGBVH_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MGBVH_ERR_NO_DEVICE;
+    void* addr = nullptr;
+    int sms = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MGBVH_ERR_CUDA;
+            if (cudaFuncSetAttribute(medium_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(MediumSmem)) != cudaSuccess)
+                return MGBVH_ERR_CUDA;
+            int n_sm = 0;
+            if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+                return MGBVH_ERR_CUDA;
+            g_noalloc_addr[dev] = p;
+            g_noalloc_sms[dev] = n_sm;
+        }
+        addr = g_noalloc_addr[dev];
+        sms = g_noalloc_sms[dev];
+    }
+    NoAllocScratch* S = reinterpret_cast<NoAllocScratch*>(addr);
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(cuda_stream);
+    const mgbvh_settings* st = settings;
+    const uint32_t n = count, slots = 2 * n - 1;
+    Params P;
+    P.min_leaf = st->min_leaf_objects;
+    P.max_leaf = st->max_leaf_objects;
+    P.max_depth = st->max_depth;
+    P.bins = st->bins;
+    P.adaptive_max_n = st->adaptive_max_n;
+    P.adaptive_steps = st->adaptive_steps;
+    Out O;
+    O.nodes = S->nodes;
+    O.lens = S->lens;
+    O.used = S->used;
+    O.perm = d_out_perm;
+    O.ctr = &S->ctr;
+    O.node_cap = slots;
+    noalloc_init_kernel<<<1, 256, 0, sm>>>(S, slots);
+    prep_aabbs_kernel<<<(n + 255) / 256, 256, 0, sm>>>(d_aabbs, n, S->rec, &S->ctr);
+    const bool root_leaf = n <= 1 || st->max_depth == 0 ||
+                           (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
+    const uint32_t cls = root_leaf ? 0u : (n <= kSmallMax ? 1u : 2u);
+    const float* bb = st->bounds;
+    init_root_kernel<<<(n + 255) / 256, 256, 0, sm>>>(n, cls, st->has_bounds, bb[0], bb[1], bb[2],
+                                                      bb[3], bb[4], bb[5], nullptr, nullptr, nullptr,
+                                                      nullptr, nullptr, S->medium, S->small, O, 0u,
+                                                      st->max_depth);
+    if (cls == 2)
+        medium_kernel<<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
+            S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O);
+    if (cls != 0) {
+        const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
+        if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
+            small_kernel<true><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O);
+        else
+            small_kernel<false><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O);
+    }
+    noalloc_finish_kernel<<<1, 1024, 0, sm>>>(S, slots, d_out_nodes, d_out_lens, node_capacity);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    struct {
+        Counters c;
+        uint32_t count;
+    } h;
+    static_assert(offsetof(NoAllocScratch, count) == offsetof(NoAllocScratch, ctr) + sizeof(Counters),
+                  "count follows the counters");
+    if (cudaMemcpyAsync(&h, &S->ctr, sizeof(Counters) + 4, cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (h.c.error) return (int)h.c.error;
+    *out_node_count = h.count;
+    const uint32_t MIN = st->min_leaf_objects, MAX = st->max_leaf_objects;
+    const bool feasible = (MIN == MAX) ? (n % MIN == 0) : (MAX >= 2 * MIN - 1);
+    return feasible ? MGBVH_OK : MGBVH_WARN_INFEASIBLE;
 }
 
 }  // extern "C"

@@ -56,7 +56,7 @@ def test_default_settings_are_the_reference_profile():
 
 
 def test_status_strings():
-    for rc in (0, 1, 2, -1, -2, -3, -4, -5, -6, -7):
+    for rc in (0, 1, 2, -1, -2, -3, -4, -5, -6, -7, -8):
         assert _lib.status_string(rc) != "unknown status"
 
 
