@@ -528,9 +528,14 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
 }
 
 // Stable partition of the large nodes' records into the other buffer: lt
-// records to the front of the node in order, gt records after them in order,
-// one block scan per round of 256 records. Grid-stride over the level's tiles;
-// also reduces the large children's centroid bounds.
+// records to the front of the node in order, gt records after them in order.
+// Each warp owns 256 consecutive records of the tile: a first pass computes
+// the side of each record (kept as 8 ballot words), one barrier publishes the
+// per-warp lt counts, and a second pass re-reads the records (cache hits) and
+// scatters them. Grid-stride over the level's tiles; also reduces the large
+// children's centroid bounds.
+constexpr uint32_t kPartPerLane = kTile / kTileThreads;  // 8
+
 __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
     const Task* __restrict__ tasks, const Decision* __restrict__ dec,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
@@ -538,71 +543,83 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
     Out O) {
     __shared__ uint32_t wcnt[kTileThreads / 32];
     __shared__ uint32_t sk[12];
+    __shared__ int sbad;
     const uint32_t ntiles = O.ctr->lvl[lv][1];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const uint32_t ti = tile_task[tile];
-        const Task t = tasks[ti];
-        const Decision d = dec[ti];
+        const Task& t = tasks[ti];
+        const Decision& d = dec[ti];
         const uint32_t begin = tile_begin[tile];
-        const uint32_t cnt = min(kTile, t.len - begin);
-        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+        const uint32_t tstart = t.start, tlen = t.len;
+        const uint32_t cnt = min(kTile, tlen - begin);
+        const Rec* src = (t.buf ? rec1 : rec0) + tstart + begin;
         Rec* dst = t.buf ? rec0 : rec1;
         if (d.kind == 1) {
             for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-                O.perm[t.start + begin + i] = __float_as_uint(src[i].lo.w);
+                O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
             continue;
         }
+        const uint32_t axis = d.axis, split_bin = d.split_bin, nbins = d.bins, n_lt = d.n_lt;
+        const float cmin = d.cmin, ext = d.ext;
+        if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+        if (threadIdx.x == 0) sbad = 0;
+        const uint32_t w0 = warp * (32u * kPartPerLane);
+        // pass 1: sides
+        uint32_t bal[kPartPerLane];
+        uint32_t lt_w = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerLane; ++j) {
+            const uint32_t i = w0 + j * 32u + lane;
+            bool pred = false;
+            if (i < cnt) {
+                const float* lo = reinterpret_cast<const float*>(&src[i].lo);
+                const float* hi = reinterpret_cast<const float*>(&src[i].hi);
+                pred = bin_of(center_of(lo[axis], hi[axis]), cmin, ext, nbins) < split_bin;
+            }
+            bal[j] = __ballot_sync(kFull, pred);
+            lt_w += __popc(bal[j]);
+        }
+        if (lane == 0) wcnt[warp] = lt_w;
+        __syncthreads();
+        uint32_t run = 0;
+        for (uint32_t q = 0; q < warp; ++q) run += wcnt[q];
         const uint32_t lt_off = tile_lt[tile];
-        const uint32_t lt_base = t.start + lt_off;
-        const uint32_t gt_base = t.start + d.n_lt + (begin - lt_off);
+        const uint32_t lt_base = tstart + lt_off;
+        const uint32_t gt_base = tstart + n_lt + (begin - lt_off);
+        const bool leaf_lt = d.child_leaf[1] != 0, leaf_gt = d.child_leaf[0] != 0;
         uint32_t k[12];
         init_key12(k);
-        if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
         bool bad = false;
-        uint32_t run_lt = 0;
-        for (uint32_t r = 0; r < cnt; r += blockDim.x) {
-            const uint32_t i = r + threadIdx.x;
-            const bool valid = i < cnt;
-            Rec rec;
-            rec.lo = rec.hi = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (valid) rec = src[i];
-            const float c[3] = {center_of(rec.lo.x, rec.hi.x), center_of(rec.lo.y, rec.hi.y),
-                                center_of(rec.lo.z, rec.hi.z)};
-            const float ca = d.axis == 0 ? c[0] : (d.axis == 1 ? c[1] : c[2]);
-            const bool pred = valid && bin_of(ca, d.cmin, d.ext, d.bins) < d.split_bin;
-            const uint32_t m = __ballot_sync(kFull, pred);
-            if (lane == 0) wcnt[warp] = __popc(m);
-            __syncthreads();
-            uint32_t wpre = 0, tot = 0;
-            for (uint32_t q = 0; q < blockDim.x / 32; ++q) {
-                const uint32_t v = wcnt[q];
-                if (q < warp) wpre += v;
-                tot += v;
-            }
-            __syncthreads();
-            if (valid) {
-                const uint32_t ltr = run_lt + wpre + __popc(m & below);
-                const uint32_t side = pred ? 1u : 0u;  // child index: 0 gt, 1 lt
+        // pass 2: scatter
+#pragma unroll 2
+        for (uint32_t j = 0; j < kPartPerLane; ++j) {
+            const uint32_t i = w0 + j * 32u + lane;
+            if (i < cnt) {
+                const Rec r = src[i];
+                const bool pred = (bal[j] >> lane) & 1u;
+                const uint32_t ltr = run + __popc(bal[j] & below);
                 const uint32_t dest = pred ? lt_base + ltr : gt_base + (i - ltr);
-                if (dest - t.start < t.len) {
-                    dst[dest] = rec;
-                    if (d.child_leaf[side]) O.perm[dest] = __float_as_uint(rec.lo.w);
+                const float c0 = center_of(r.lo.x, r.hi.x), c1 = center_of(r.lo.y, r.hi.y),
+                            c2 = center_of(r.lo.z, r.hi.z);
+                if (dest - tstart < tlen) {
+                    dst[dest] = r;
+                    if (pred ? leaf_lt : leaf_gt) O.perm[dest] = __float_as_uint(r.lo.w);
                 } else {
                     bad = true;  // inconsistent counts; never write outside the node
                 }
-                bad |= !box_contains(pred ? d.ltb : d.gtb, c[0], c[1], c[2]);
+                bad |= !box_contains(pred ? d.ltb : d.gtb, c0, c1, c2);
                 uint32_t* kk = pred ? k : k + 6;
-#pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    kk[a] = min(kk[a], fkey(c[a]));
-                    kk[3 + a] = max(kk[3 + a], fkey(c[a]));
-                }
+                kk[0] = min(kk[0], fkey(c0));
+                kk[1] = min(kk[1], fkey(c1));
+                kk[2] = min(kk[2], fkey(c2));
+                kk[3] = max(kk[3], fkey(c0));
+                kk[4] = max(kk[4], fkey(c1));
+                kk[5] = max(kk[5], fkey(c2));
             }
-            run_lt += tot;
+            run += __popc(bal[j]);
         }
-        if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
         const bool need_lt = d.child_task[1] != kNone, need_gt = d.child_task[0] != kNone;
         if (need_lt || need_gt) {
 #pragma unroll
@@ -616,20 +633,22 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
                         atomicMax(&sk[q], v);
                 }
             }
-            __syncthreads();
-            if (threadIdx.x < 12) {
-                const uint32_t q = threadIdx.x;
-                const uint32_t child = q < 6 ? d.child_task[1] : d.child_task[0];
-                if (child != kNone) {
-                    uint32_t* g = next_cbkeys + 6 * child + (q % 6);
-                    if ((q % 6) < 3)
-                        atomicMin(g, sk[q]);
-                    else
-                        atomicMax(g, sk[q]);
-                }
+        }
+        if (__any_sync(kFull, bad) && lane == 0) sbad = 1;
+        __syncthreads();
+        if (threadIdx.x == 0 && sbad) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+        if ((need_lt || need_gt) && threadIdx.x < 12) {
+            const uint32_t q = threadIdx.x;
+            const uint32_t child = q < 6 ? d.child_task[1] : d.child_task[0];
+            if (child != kNone) {
+                uint32_t* g = next_cbkeys + 6 * child + (q % 6);
+                if ((q % 6) < 3)
+                    atomicMin(g, sk[q]);
+                else
+                    atomicMax(g, sk[q]);
             }
         }
-        __syncthreads();  // sk and wcnt are rewritten by the next tile
+        __syncthreads();  // wcnt/sk/sbad are rewritten by the next tile
     }
 }
 
