@@ -1393,7 +1393,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     // Level passes over the large nodes. Kernels read their task and tile
     // counts on the device, so levels are launched in batches and the host
     // reads the next level's count only at the end of a batch.
-    const int tile_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * 4u);
+    const int tile_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * 8u);
     const int eval_grid = (int)std::min<uint32_t>((C.tasks + 3) / 4, (uint32_t)ctx->sm_count * 4u);
     uint32_t level = 0;
     bool more = cls == 3;
