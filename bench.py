@@ -53,6 +53,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="icosphere", choices=["icosphere", "mixed"],
+                   help="icosphere: the headline build; mixed: 16.8M-triangle scene + 8M rays")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-pointer (e2e) leg")
     p.add_argument("--profile-steps", type=int, default=None, help=argparse.SUPPRESS)
@@ -363,9 +365,103 @@ def run_reference(args):
     print(json.dumps(out), flush=True)
 
 
+def run_mixed(args):
+    """The large mixed scene: 16,777,216 triangles (8,388,608 in 64 Gaussian
+    blobs, a 2048 x 1024-quad ground grid, 4,194,304 thin 1:200 triangles),
+    built with the reference profile, then 8,388,608 closest-hit rays with
+    origins uniform in the scene box grown by 10% and uniform directions. The
+    traversal is checked hit for hit against GPU brute force on a
+    65,536-ray subset and the brute force against the CPU oracle on 16 rays."""
+    import ctypes
+    import torch
+    from marigold_b200 import BvhSettings, _lib, build_device, synth
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    v, t = synth.mixed_scene()
+    n = t.shape[0]
+    rays = synth.rays_in_box(8388608, v.min(0), v.max(0))
+    gen_s = time.perf_counter() - t0
+    ctx = _lib.Context(0)
+    dv = torch.from_numpy(v).cuda()
+    dt = torch.from_numpy(t.view(np.int32)).cuda()
+    cap = 2 * n - 1
+    d_nodes = torch.empty(cap * 8, dtype=torch.int32, device="cuda")
+    d_lens = torch.empty(cap, dtype=torch.int32, device="cuda")
+    d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    settings = BvhSettings(name="mixed", max_depth=32)
+    build_ms, count, st = [], 0, {}
+    for k in range(max(args.warmup, 1) + args.steps):
+        flush.fill_(k & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        count, rc, st = build_device(ctx, settings, d_nodes, d_perm, vertices=dv, triangles=dt,
+                                     out_lens=d_lens, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= max(args.warmup, 1):
+            build_ms.append(e0.elapsed_time(e1))
+    tr = _lib.Tracer(0)
+    L = tr.L
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    vp = lambda x: ctypes.c_void_p(x.data_ptr())
+    tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 12, v.shape[0],
+                                         vp(dt), vp(d_perm), n, sp))
+    dr = torch.from_numpy(rays).cuda()
+    m = rays.shape[0]
+    ht = torch.empty(m, dtype=torch.float32, device="cuda")
+    hp = torch.empty(m, dtype=torch.int32, device="cuda")
+    counts = (ctypes.c_uint64 * 3)()
+    secs = ctypes.c_double(0)
+    trace_ms = []
+    for k in range(max(args.warmup, 1) + args.steps):
+        flush.fill_(k & 0xFF)
+        tr.check(L.mgbvh_trace_closest_dev(tr.ptr, vp(dr), m, vp(ht), vp(hp), counts,
+                                           ctypes.byref(secs), sp))
+        if k >= max(args.warmup, 1):
+            trace_ms.append(secs.value * 1e3)
+    # check: 65,536-ray subset against GPU brute force, 16 rays against the CPU
+    sub = 65536
+    bt = torch.empty(sub, dtype=torch.float32, device="cuda")
+    bp = torch.empty(sub, dtype=torch.int32, device="cuda")
+    tb = time.perf_counter()
+    tr.check(L.mgbvh_trace_bruteforce_dev(tr.ptr, vp(dr), sub, vp(bt), vp(bp), sp))
+    brute_s = time.perf_counter() - tb
+    gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
+    btn, bpn = bt.cpu().numpy(), bp.cpu().numpy().view(np.uint32)
+    mism = int(((gp != bpn) | (gt.view(np.uint32) != btn.view(np.uint32))).sum())
+    from oracle import oracle as orc
+    ct, cp = orc.trace_bruteforce(v, t, rays[:16])
+    cpu_mism = int(((cp != bpn[:16]) | (ct.view(np.uint32) != btn[:16].view(np.uint32))).sum())
+    hits = int((hp.cpu().numpy().view(np.uint32) != 0xFFFFFFFF).sum())
+    bms = float(np.mean(build_ms))
+    tms = float(np.mean(trace_ms))
+    out = {
+        "metric": "BVH build Mtri/s; closest-hit Mrays/s", "workload": "mixed scene",
+        "config": {"triangles": n, "rays": m, "blobs": 64, "grid_quads": [2048, 1024],
+                   "thin": 4194304, "max_depth": 32, "leaf": 1, "profile": "reference"},
+        "build": {"value": round(n / (bms * 1e-3) / 1e6, 2), "unit": "Mtri/s",
+                  "ms": round(bms, 3), "nodes": count, "height": st.get("height"),
+                  "phase_ms": [round(x * 1e3, 3) for x in st.get("phase_seconds", [])]},
+        "trace": {"value": round(m / (tms * 1e-3) / 1e6, 2), "unit": "Mrays/s",
+                  "ms": round(tms, 3), "hit_rays": hits,
+                  "nodes_visited": counts[0], "box_tests": counts[1], "triangle_tests": counts[2]},
+        "check": {"subset_rays": sub, "mismatches_vs_gpu_bruteforce": mism,
+                  "cpu_rays": 16, "mismatches_gpu_bruteforce_vs_cpu": cpu_mism,
+                  "bruteforce_s": round(brute_s, 2)},
+        "steps": args.steps, "warmup": args.warmup, "generation_s": round(gen_s, 1),
+        "l2": "flushed before every build and trace",
+    }
+    tr.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.workload == "mixed":
+        run_mixed(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

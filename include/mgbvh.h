@@ -221,6 +221,45 @@ MGBVH_API int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count,
                                         void* cuda_stream);
 
 /*
+ * Closest-hit traversal of a built BVH over triangles, restating the BLAS
+ * traversal math of marigold/assets/shaders/slang/lib/scene.slang:19-89
+ * (Moller-Trumbore, |det| < 1e-6 and t < 1e-6 reject), :143-220 (stack
+ * traversal, nearer child first) and :296-310 (slab test), as CUDA over device
+ * buffers (the shader itself needs a graphics stack). One mgbvh_tracer per
+ * calling thread.
+ *
+ * Rays: n_rays records of 8 floats (origin xyz, unused, direction xyz,
+ * unused). Results: hit distance in ray units (-1 for a miss) and the
+ * original triangle index (0xFFFFFFFF for a miss); equal distances resolve to
+ * the lowest triangle index. out_counts (host, nullable) receives the
+ * shader's traversal counters summed over all rays: nodes visited, box tests,
+ * triangle tests (scene.slang:108, 121, 208).
+ */
+typedef struct mgbvh_tracer mgbvh_tracer;
+MGBVH_API int mgbvh_tracer_create(int device, mgbvh_tracer** out);
+MGBVH_API void mgbvh_tracer_destroy(mgbvh_tracer* tracer);
+/* Binds a built BLAS: device nodes (and lens for leaves of several objects,
+   NULL = one object per leaf), the vertices/triangles it was built from and
+   the build's permutation. Gathers the triangles into leaf order; keeps the
+   node/len pointers, which must stay valid while tracing. */
+MGBVH_API int mgbvh_tracer_set_blas_dev(mgbvh_tracer* tracer, const mgbvh_node* d_nodes,
+                                        uint32_t node_count, const uint32_t* d_lens,
+                                        const float* d_vertices, uint32_t vertex_stride_bytes,
+                                        uint32_t vertex_count, const uint32_t* d_triangles,
+                                        const uint32_t* d_perm, uint32_t triangle_count,
+                                        void* cuda_stream);
+/* Closest hit of every ray through the BVH. out_seconds (host, nullable):
+   device time of the traversal kernel. */
+MGBVH_API int mgbvh_trace_closest_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
+                                      float* d_hit_t, uint32_t* d_hit_prim, uint64_t* out_counts,
+                                      double* out_seconds, void* cuda_stream);
+/* Closest hit of every ray against every triangle of the bound BLAS, with
+   the same triangle test: the check for mgbvh_trace_closest_dev. */
+MGBVH_API int mgbvh_trace_bruteforce_dev(mgbvh_tracer* tracer, const float* d_rays,
+                                         uint32_t n_rays, float* d_hit_t, uint32_t* d_hit_prim,
+                                         void* cuda_stream);
+
+/*
  * AsGpuBytes for BvhNode (bvh/src/lib.rs:157-212), host side: 8 u32 words per
  * node. For MAX_LEAF_OBJECTS == 1 this copies the node. For larger MAX the
  * last word packs len into the top ilog2(MAX.next_power_of_two()) bits and

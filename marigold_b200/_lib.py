@@ -30,7 +30,8 @@ EXPORTED = (
     "mgbvh_default_settings", "mgbvh_create", "mgbvh_destroy", "mgbvh_set_stream",
     "mgbvh_last_error", "mgbvh_status_string", "mgbvh_build_indexed", "mgbvh_build_aabbs",
     "mgbvh_build_indexed_dev", "mgbvh_build_aabbs_dev", "mgbvh_encode_gpu_bytes",
-    "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc",
+    "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc", "mgbvh_tracer_create", "mgbvh_tracer_destroy",
+    "mgbvh_tracer_set_blas_dev", "mgbvh_trace_closest_dev", "mgbvh_trace_bruteforce_dev",
 )
 
 
@@ -133,6 +134,17 @@ def load():
         L.mgbvh_build_aabbs_noalloc.argtypes = [P, u32, ctypes.POINTER(Settings), P, u32, pu32, P,
                                                 P, P]
         L.mgbvh_build_aabbs_noalloc.restype = ctypes.c_int
+        L.mgbvh_tracer_create.argtypes = [ctypes.c_int, ctypes.POINTER(P)]
+        L.mgbvh_tracer_create.restype = ctypes.c_int
+        L.mgbvh_tracer_destroy.argtypes = [P]
+        L.mgbvh_tracer_destroy.restype = None
+        L.mgbvh_tracer_set_blas_dev.argtypes = [P, P, u32, P, P, u32, u32, P, P, u32, P]
+        L.mgbvh_tracer_set_blas_dev.restype = ctypes.c_int
+        L.mgbvh_trace_closest_dev.argtypes = [P, P, u32, P, P, ctypes.POINTER(ctypes.c_uint64),
+                                              ctypes.POINTER(ctypes.c_double), P]
+        L.mgbvh_trace_closest_dev.restype = ctypes.c_int
+        L.mgbvh_trace_bruteforce_dev.argtypes = [P, P, u32, P, P, P]
+        L.mgbvh_trace_bruteforce_dev.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]
         L.mgbvh_sah_cost.restype = ctypes.c_double
         _lib = L
@@ -167,6 +179,33 @@ class Context:
     def close(self):
         if self.ptr:
             self.L.mgbvh_destroy(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Tracer:
+    """An mgbvh_tracer: closest-hit traversal of one built BLAS on one device."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.ptr = ctypes.c_void_p()
+        rc = self.L.mgbvh_tracer_create(device, ctypes.byref(self.ptr))
+        if rc != OK:
+            raise MgbvhError(rc, status_string(rc))
+
+    def check(self, rc: int) -> int:
+        if rc < 0:
+            raise MgbvhError(rc, status_string(rc))
+        return rc
+
+    def close(self):
+        if self.ptr:
+            self.L.mgbvh_tracer_destroy(self.ptr)
             self.ptr = ctypes.c_void_p()
 
     def __del__(self):

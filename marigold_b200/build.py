@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgbvh.so")
-SOURCES = ["mgbvh_build.cu"]
+SOURCES = ["mgbvh_build.cu", "mgbvh_trace.cu"]
 HEADERS = ["mgbvh_exact.cuh", "mgbvh_device.cuh"]
 
 NVCC_FLAGS = [

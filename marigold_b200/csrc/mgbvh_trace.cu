@@ -1,0 +1,381 @@
+// mgbvh_trace.cu — closest-hit traversal of a built BVH, and a brute-force
+// intersector to check it.
+//
+// Restates the closest-hit math of marigold's BLAS traversal
+// (marigold/assets/shaders/slang/lib/scene.slang:143-220, 296-310) as CUDA:
+//   * Moller-Trumbore ray/triangle test with the shader's thresholds:
+//     |det| < 1e-6 and t < 1e-6 reject (scene.slang:19-89);
+//   * stack traversal, both children tested, the nearer one popped first
+//     (far child pushed first, scene.slang:129-134 / 199-204);
+//   * leaves: child_node == 0, start_index = first object, one object per
+//     leaf unless per-node lengths are given.
+// Deliberate differences, so that the traversal can be checked hit for hit
+// against brute force: the slab test is conservative (t_far grown by
+// 2*gamma(3), PBRT's robust bound) and keeps boxes whose entry equals the
+// current closest t; equal hit distances resolve to the lowest triangle index
+// (the shader keeps the later-tested one, scene.slang:57-82 via
+// intersect.slang's Hit::merge). Hit distances are in ray units; the shader's
+// instance-scale quirk (scene.slang:168-169) does not arise in one level.
+//
+// The library is compiled with -fmad=false: every dot and cross product is
+// evaluated as written below, the same way as the CPU cross-check.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/mgbvh.h"
+
+namespace mgbvh_trace {
+
+constexpr uint32_t kFull = 0xFFFFFFFFu;
+constexpr int kStack = 64;  // scene.slang:5-7 (BVH_STACK_SIZE = 32 + 32)
+constexpr uint32_t kNoHit = 0xFFFFFFFFu;
+
+struct TriRec {  // one triangle in leaf order: v1 + original index, v2, v3
+    float4 a;    // v1.xyz, triangle index (bits)
+    float4 b;    // v2.xyz
+    float4 c;    // v3.xyz
+};
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+
+// Moller-Trumbore as scene.slang:19-89 evaluates it; returns t or -1 (miss).
+__device__ __forceinline__ float intersect_tri(float ox, float oy, float oz, float dx, float dy,
+                                               float dz, const TriRec& t) {
+    const float e1x = __fsub_rn(t.b.x, t.a.x), e1y = __fsub_rn(t.b.y, t.a.y),
+                e1z = __fsub_rn(t.b.z, t.a.z);
+    const float e2x = __fsub_rn(t.c.x, t.a.x), e2y = __fsub_rn(t.c.y, t.a.y),
+                e2z = __fsub_rn(t.c.z, t.a.z);
+    // h = cross(dir, edge2)
+    const float hx = __fsub_rn(__fmul_rn(dy, e2z), __fmul_rn(dz, e2y));
+    const float hy = __fsub_rn(__fmul_rn(dz, e2x), __fmul_rn(dx, e2z));
+    const float hz = __fsub_rn(__fmul_rn(dx, e2y), __fmul_rn(dy, e2x));
+    const float det = dot3(hx, hy, hz, e1x, e1y, e1z);
+    if (fabsf(det) < 1e-6f) return -1.0f;
+    const float f = __fdiv_rn(1.0f, det);
+    const float sx = __fsub_rn(ox, t.a.x), sy = __fsub_rn(oy, t.a.y), sz = __fsub_rn(oz, t.a.z);
+    const float u = __fmul_rn(f, dot3(sx, sy, sz, hx, hy, hz));
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    // q = cross(s, edge1)
+    const float qx = __fsub_rn(__fmul_rn(sy, e1z), __fmul_rn(sz, e1y));
+    const float qy = __fsub_rn(__fmul_rn(sz, e1x), __fmul_rn(sx, e1z));
+    const float qz = __fsub_rn(__fmul_rn(sx, e1y), __fmul_rn(sy, e1x));
+    const float v = __fmul_rn(f, dot3(dx, dy, dz, qx, qy, qz));
+    if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return -1.0f;
+    const float tt = __fmul_rn(f, dot3(e2x, e2y, e2z, qx, qy, qz));
+    if (tt < 1e-6f) return -1.0f;
+    return tt;
+}
+
+// Conservative slab test: the entry distance if the box can hold a hit at a
+// distance <= best, else +inf.
+__device__ __forceinline__ float box_entry(float ox, float oy, float oz, float ix, float iy, float iz,
+                                           const float4& lo, const float4& hi, float best) {
+    const float tx0 = (lo.x - ox) * ix, tx1 = (hi.x - ox) * ix;
+    const float ty0 = (lo.y - oy) * iy, ty1 = (hi.y - oy) * iy;
+    const float tz0 = (lo.z - oz) * iz, tz1 = (hi.z - oz) * iz;
+    const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+    float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
+    tf *= 1.0000003576278687f;  // 1 + 2 * gamma(3), gamma(n) = n*eps/(1 - n*eps)
+    return (tn <= tf && tn <= best) ? tn : __int_as_float(0x7F800000);
+}
+
+struct Counts {
+    unsigned long long nodes, boxes, tris;
+};
+
+template <bool kLens>
+__global__ void __launch_bounds__(128) trace_kernel(const float4* __restrict__ nodes,
+                                                    const uint32_t* __restrict__ lens,
+                                                    const TriRec* __restrict__ tris,
+                                                    const float4* __restrict__ rays, uint32_t n_rays,
+                                                    float* __restrict__ hit_t,
+                                                    uint32_t* __restrict__ hit_prim, Counts* counts,
+                                                    int* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
+    if (i < n_rays) {
+        const float4 o = rays[2 * i], d = rays[2 * i + 1];
+        const float ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
+        float best = __int_as_float(0x7F800000);
+        uint32_t best_prim = kNoHit;
+        uint32_t stack[kStack];
+        int sp = 0;
+        const float4 rlo = nodes[0], rhi = nodes[1];
+        c_boxes++;
+        if (box_entry(o.x, o.y, o.z, ix, iy, iz, rlo, rhi, best) <= best) stack[sp++] = 0;
+        while (sp > 0) {
+            const uint32_t ni = stack[--sp];
+            c_nodes++;
+            const float4 nhi = nodes[2 * ni + 1];
+            const uint32_t child = __float_as_uint(nhi.w);
+            if (child != 0) {
+                const float4 alo = nodes[2 * child], ahi = nodes[2 * child + 1];
+                const float4 blo = nodes[2 * child + 2], bhi = nodes[2 * child + 3];
+                c_boxes += 2;
+                const float da = box_entry(o.x, o.y, o.z, ix, iy, iz, alo, ahi, best);
+                const float db = box_entry(o.x, o.y, o.z, ix, iy, iz, blo, bhi, best);
+                const bool pa = da <= best, pb = db <= best;
+                if (sp + 2 > kStack) {  // cannot happen for depth <= 62; never overflow
+                    atomicExch(err, 1);
+                    break;
+                }
+                if (pa && pb) {
+                    const bool a_first = da < db;
+                    stack[sp++] = a_first ? child + 1 : child;
+                    stack[sp++] = a_first ? child : child + 1;
+                } else if (pa || pb) {
+                    stack[sp++] = pa ? child : child + 1;
+                }
+            } else {
+                const float4 nlo = nodes[2 * ni];
+                const uint32_t start = __float_as_uint(nlo.w);
+                const uint32_t len = kLens ? lens[ni] : 1u;
+                for (uint32_t k = start; k < start + len; ++k) {
+                    const TriRec t = tris[k];
+                    c_tris++;
+                    const float tt = intersect_tri(o.x, o.y, o.z, d.x, d.y, d.z, t);
+                    const uint32_t prim = __float_as_uint(t.a.w);
+                    if (tt >= 0.0f && (tt < best || (tt == best && prim < best_prim))) {
+                        best = tt;
+                        best_prim = prim;
+                    }
+                }
+            }
+        }
+        hit_t[i] = best_prim == kNoHit ? -1.0f : best;
+        hit_prim[i] = best_prim;
+    }
+    if (counts) {
+        // warp totals, one atomic per warp
+        unsigned long long a = c_nodes, b = c_boxes, c = c_tris;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(kFull, a, off);
+            b += __shfl_down_sync(kFull, b, off);
+            c += __shfl_down_sync(kFull, c, off);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicAdd(&counts->nodes, a);
+            atomicAdd(&counts->boxes, b);
+            atomicAdd(&counts->tris, c);
+        }
+    }
+}
+
+// Every ray against every triangle (shared-memory tiles of triangles).
+__global__ void __launch_bounds__(256) brute_kernel(const TriRec* __restrict__ tris, uint32_t n_tris,
+                                                    const float4* __restrict__ rays, uint32_t n_rays,
+                                                    float* __restrict__ hit_t,
+                                                    uint32_t* __restrict__ hit_prim) {
+    __shared__ TriRec tile[256];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = make_float4(0.f, 0.f, 1.f, 0.f);
+    if (i < n_rays) {
+        o = rays[2 * i];
+        d = rays[2 * i + 1];
+    }
+    float best = __int_as_float(0x7F800000);
+    uint32_t best_prim = kNoHit;
+    for (uint32_t base = 0; base < n_tris; base += 256) {
+        __syncthreads();
+        if (base + threadIdx.x < n_tris) tile[threadIdx.x] = tris[base + threadIdx.x];
+        __syncthreads();
+        const uint32_t m = min(256u, n_tris - base);
+        for (uint32_t k = 0; k < m; ++k) {
+            const TriRec& t = tile[k];
+            const float tt = intersect_tri(o.x, o.y, o.z, d.x, d.y, d.z, t);
+            const uint32_t prim = __float_as_uint(t.a.w);
+            if (tt >= 0.0f && (tt < best || (tt == best && prim < best_prim))) {
+                best = tt;
+                best_prim = prim;
+            }
+        }
+    }
+    if (i < n_rays) {
+        hit_t[i] = best_prim == kNoHit ? -1.0f : best;
+        hit_prim[i] = best_prim;
+    }
+}
+
+// Triangles in leaf order (the crate's permuted list) with their vertices.
+__global__ void gather_kernel(const float* __restrict__ verts, uint32_t stride_floats,
+                              uint32_t nverts, const uint32_t* __restrict__ tris,
+                              const uint32_t* __restrict__ perm, uint32_t n, TriRec* __restrict__ out,
+                              int* err) {
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t p = perm[k];
+        if (p >= n) {
+            atomicExch(err, 2);
+            continue;
+        }
+        uint32_t v[3] = {tris[3 * (size_t)p], tris[3 * (size_t)p + 1], tris[3 * (size_t)p + 2]};
+        if (v[0] >= nverts || v[1] >= nverts || v[2] >= nverts) {
+            atomicExch(err, 2);
+            continue;
+        }
+        const float* a = verts + (size_t)v[0] * stride_floats;
+        const float* b = verts + (size_t)v[1] * stride_floats;
+        const float* c = verts + (size_t)v[2] * stride_floats;
+        TriRec r;
+        r.a = make_float4(a[0], a[1], a[2], __uint_as_float(p));
+        r.b = make_float4(b[0], b[1], b[2], 0.0f);
+        r.c = make_float4(c[0], c[1], c[2], 0.0f);
+        out[k] = r;
+    }
+}
+
+}  // namespace mgbvh_trace
+
+using namespace mgbvh_trace;
+
+struct mgbvh_tracer {
+    int device = 0;
+    TriRec* tris = nullptr;
+    size_t tris_cap = 0;
+    uint32_t n_tris = 0;
+    const mgbvh_node* nodes = nullptr;
+    const uint32_t* lens = nullptr;
+    uint32_t node_count = 0;
+    Counts* d_counts = nullptr;
+    int* d_err = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.0f;
+};
+
+namespace {
+
+int trace_check(cudaError_t e) { return e == cudaSuccess ? MGBVH_OK : MGBVH_ERR_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+int mgbvh_tracer_create(int device, mgbvh_tracer** out) {
+    if (!out) return MGBVH_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return MGBVH_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev || cudaSetDevice(device) != cudaSuccess) return MGBVH_ERR_INVALID_ARG;
+    mgbvh_tracer* t = new mgbvh_tracer();
+    t->device = device;
+    if (cudaMalloc(&t->d_counts, sizeof(Counts)) != cudaSuccess ||
+        cudaMalloc(&t->d_err, sizeof(int)) != cudaSuccess || cudaEventCreate(&t->ev0) != cudaSuccess ||
+        cudaEventCreate(&t->ev1) != cudaSuccess) {
+        mgbvh_tracer_destroy(t);
+        return MGBVH_ERR_CUDA;
+    }
+    *out = t;
+    return MGBVH_OK;
+}
+
+void mgbvh_tracer_destroy(mgbvh_tracer* t) {
+    if (!t) return;
+    cudaSetDevice(t->device);
+    if (t->tris) cudaFree(t->tris);
+    if (t->d_counts) cudaFree(t->d_counts);
+    if (t->d_err) cudaFree(t->d_err);
+    if (t->ev0) cudaEventDestroy(t->ev0);
+    if (t->ev1) cudaEventDestroy(t->ev1);
+    delete t;
+}
+
+int mgbvh_tracer_set_blas_dev(mgbvh_tracer* t, const mgbvh_node* d_nodes, uint32_t node_count,
+                              const uint32_t* d_lens, const float* d_vertices,
+                              uint32_t vertex_stride_bytes, uint32_t vertex_count,
+                              const uint32_t* d_triangles, const uint32_t* d_perm,
+                              uint32_t triangle_count, void* stream) {
+    if (!t || !d_nodes || node_count == 0 || !d_vertices || !d_triangles || !d_perm ||
+        triangle_count == 0 || vertex_stride_bytes < 12 || vertex_stride_bytes % 4)
+        return MGBVH_ERR_INVALID_ARG;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    const size_t need = sizeof(TriRec) * (size_t)triangle_count;
+    if (t->tris_cap < need) {
+        if (t->tris) cudaFree(t->tris);
+        t->tris = nullptr;
+        t->tris_cap = 0;
+        if (cudaMalloc(&t->tris, need) != cudaSuccess) return MGBVH_ERR_CUDA;
+        t->tris_cap = need;
+    }
+    if (cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess) return MGBVH_ERR_CUDA;
+    gather_kernel<<<std::max(1u, std::min((triangle_count + 255) / 256, 148u * 16u)), 256, 0, sm>>>(
+        d_vertices, vertex_stride_bytes / 4, vertex_count, d_triangles, d_perm, triangle_count,
+        t->tris, t->d_err);
+    int herr = 0;
+    if (cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (herr) return MGBVH_ERR_INVALID_ARG;
+    t->nodes = d_nodes;
+    t->lens = d_lens;
+    t->node_count = node_count;
+    t->n_tris = triangle_count;
+    return MGBVH_OK;
+}
+
+int mgbvh_trace_closest_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_rays, float* d_hit_t,
+                            uint32_t* d_hit_prim, uint64_t* out_counts, double* out_seconds,
+                            void* stream) {
+    if (!t || !t->nodes || (n_rays && (!d_rays || !d_hit_t || !d_hit_prim))) return MGBVH_ERR_INVALID_ARG;
+    if (n_rays == 0) return MGBVH_OK;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(t->d_counts, 0, sizeof(Counts), sm) != cudaSuccess ||
+        cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    cudaEventRecord(t->ev0, sm);
+    const uint32_t grid = (n_rays + 127) / 128;
+    const float4* nodes = reinterpret_cast<const float4*>(t->nodes);
+    const float4* rays = reinterpret_cast<const float4*>(d_rays);
+    if (t->lens)
+        trace_kernel<true><<<grid, 128, 0, sm>>>(nodes, t->lens, t->tris, rays, n_rays, d_hit_t,
+                                                 d_hit_prim, out_counts ? t->d_counts : nullptr,
+                                                 t->d_err);
+    else
+        trace_kernel<false><<<grid, 128, 0, sm>>>(nodes, nullptr, t->tris, rays, n_rays, d_hit_t,
+                                                  d_hit_prim, out_counts ? t->d_counts : nullptr,
+                                                  t->d_err);
+    cudaEventRecord(t->ev1, sm);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    Counts hc;
+    int herr = 0;
+    if (cudaMemcpyAsync(&hc, t->d_counts, sizeof(Counts), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (herr) return MGBVH_ERR_CAPACITY;  // traversal stack would have overflowed
+    if (out_counts) {
+        out_counts[0] = hc.nodes;
+        out_counts[1] = hc.boxes;
+        out_counts[2] = hc.tris;
+    }
+    if (out_seconds) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t->ev0, t->ev1);
+        *out_seconds = ms * 1e-3;
+    }
+    return MGBVH_OK;
+}
+
+int mgbvh_trace_bruteforce_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_rays, float* d_hit_t,
+                               uint32_t* d_hit_prim, void* stream) {
+    if (!t || !t->tris || (n_rays && (!d_rays || !d_hit_t || !d_hit_prim))) return MGBVH_ERR_INVALID_ARG;
+    if (n_rays == 0) return MGBVH_OK;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    brute_kernel<<<(n_rays + 255) / 256, 256, 0, sm>>>(t->tris, t->n_tris,
+                                                        reinterpret_cast<const float4*>(d_rays), n_rays,
+                                                        d_hit_t, d_hit_prim);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    return trace_check(cudaStreamSynchronize(sm));
+}
+
+}  // extern "C"

@@ -196,3 +196,82 @@ def config1_mesh(seed: int = 1):
 def config2_mesh(seed: int = 2):
     """Noisy icosphere, level 8: 1,310,720 triangles, 655,362 shared vertices."""
     return noisy_icosphere(8, seed)
+
+
+def gaussian(seed: int, stream: int, idx) -> np.ndarray:
+    """Standard normal samples by the Box-Muller transform of two uniforms."""
+    u1 = uniform(seed, stream, idx)
+    u2 = uniform(seed, stream + 1, idx)
+    r = np.sqrt(-2.0 * np.log(1.0 - u1))
+    s, c = _sincos((2.0 * u2 - 1.0) * np.pi)
+    return r * c
+
+
+def mixed_scene(seed: int = 5, blobs: int = 64, n_blob: int = 8388608, grid=(2048, 1024),
+                n_thin: int = 4194304):
+    """The large mixed scene: n_blob small triangles in `blobs` Gaussian blobs
+    (sigma uniform in [0.5, 5]), a flat ground grid of grid[0] x grid[1] quads
+    split into two triangles each, and n_thin long thin triangles (aspect
+    1:200, random orientation). Vertices are unshared and stored compactly as
+    float32 [3N, 3] (12-byte stride); triangles are [3i, 3i+1, 3i+2]."""
+    parts = []
+    # blobs
+    b = np.arange(blobs, dtype=np.uint32)
+    centers = np.stack([uniform(seed, 1, b) * 160.0 - 80.0, uniform(seed, 2, b) * 60.0,
+                        uniform(seed, 3, b) * 160.0 - 80.0], axis=-1)
+    sigma = 0.5 + 4.5 * uniform(seed, 4, b)
+    i = np.arange(n_blob, dtype=np.uint32)
+    which = (i % blobs).astype(np.int64)
+    v0 = centers[which] + sigma[which, None] * np.stack(
+        [gaussian(seed, 10 + 2 * k, i) for k in range(3)], axis=-1)
+    e1 = unit_vectors(seed, 20, i) * (0.02 + 0.18 * uniform(seed, 22, i))[:, None]
+    e2 = unit_vectors(seed, 23, i) * (0.02 + 0.18 * uniform(seed, 25, i))[:, None]
+    parts.append(np.stack([v0, v0 + e1, v0 + e2], axis=1))
+    # ground grid on y = 0 over [-100, 100]^2
+    gx, gz = grid
+    xs = np.linspace(-100.0, 100.0, gx + 1)
+    zs = np.linspace(-100.0, 100.0, gz + 1)
+    qx, qz = np.meshgrid(np.arange(gx), np.arange(gz), indexing="ij")
+    qx = qx.ravel()
+    qz = qz.ravel()
+    p00 = np.stack([xs[qx], np.zeros(qx.size), zs[qz]], axis=-1)
+    p10 = np.stack([xs[qx + 1], np.zeros(qx.size), zs[qz]], axis=-1)
+    p01 = np.stack([xs[qx], np.zeros(qx.size), zs[qz + 1]], axis=-1)
+    p11 = np.stack([xs[qx + 1], np.zeros(qx.size), zs[qz + 1]], axis=-1)
+    t_a = np.stack([p00, p10, p11], axis=1)
+    t_b = np.stack([p00, p11, p01], axis=1)
+    parts.append(np.stack([t_a, t_b], axis=1).reshape(-1, 3, 3))
+    # long thin triangles: length U(2, 10), width length / 200
+    j = np.arange(n_thin, dtype=np.uint32)
+    c = np.stack([uniform(seed, 30, j) * 200.0 - 100.0, uniform(seed, 31, j) * 60.0,
+                  uniform(seed, 32, j) * 200.0 - 100.0], axis=-1)
+    u = unit_vectors(seed, 33, j)
+    w = unit_vectors(seed, 35, j)
+    w = w - (w * u).sum(axis=1, keepdims=True) * u
+    w = w / np.sqrt(np.maximum((w * w).sum(axis=1, keepdims=True), 1e-30))
+    length = 2.0 + 8.0 * uniform(seed, 37, j)
+    half = (0.5 * length)[:, None] * u
+    parts.append(np.stack([c - half, c + half, c + (length / 200.0)[:, None] * w], axis=1))
+    tri = np.concatenate(parts, axis=0)
+    n = tri.shape[0]
+    vertices = _f32(tri.reshape(3 * n, 3))
+    triangles = np.arange(3 * n, dtype=np.uint32).reshape(n, 3)
+    return vertices, triangles
+
+
+def rays_in_box(n: int, lo, hi, seed: int = 6, expand: float = 0.1):
+    """Rays with origins uniform in the box [lo, hi] grown by `expand` of its
+    extent on every side and directions uniform on the sphere: float32
+    [n, 8] = origin xyz, 0, direction xyz, 0."""
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    ext = hi - lo
+    lo2 = lo - expand * ext
+    ext2 = ext * (1.0 + 2.0 * expand)
+    i = np.arange(n, dtype=np.uint32)
+    o = lo2 + ext2 * np.stack([uniform(seed, 40 + k, i) for k in range(3)], axis=-1)
+    d = unit_vectors(seed, 43, i)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = _f32(o)
+    r[:, 4:7] = _f32(d)
+    return r

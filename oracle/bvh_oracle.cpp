@@ -633,4 +633,50 @@ int oracle_build(const float* verts, uint32_t vertex_stride_bytes, const uint32_
 
 uint32_t oracle_last_tie_events(void) { return g_tie_events; }
 
+// Closest hit of each ray against every triangle: the Moller-Trumbore test of
+// marigold/assets/shaders/slang/lib/scene.slang:19-89 (|det| < 1e-6 and
+// t < 1e-6 reject), every product and sum as written, lowest triangle index
+// on equal distances. rays: n_rays x 8 floats (origin xyz, -, dir xyz, -).
+void oracle_trace_bruteforce(const float* verts, uint32_t stride_floats, const uint32_t* tris,
+                             uint32_t n, const float* rays, uint32_t n_rays, float* out_t,
+                             uint32_t* out_prim) {
+    auto dot3 = [](float ax, float ay, float az, float bx, float by, float bz) {
+        float d = ax * bx;
+        d = d + ay * by;
+        d = d + az * bz;
+        return d;
+    };
+    for (uint32_t r = 0; r < n_rays; ++r) {
+        const float* R = rays + 8 * (size_t)r;
+        const float ox = R[0], oy = R[1], oz = R[2], dx = R[4], dy = R[5], dz = R[6];
+        float best = std::numeric_limits<float>::infinity();
+        uint32_t best_prim = 0xFFFFFFFFu;
+        for (uint32_t p = 0; p < n; ++p) {
+            const float* a = verts + (size_t)tris[3 * (size_t)p] * stride_floats;
+            const float* b = verts + (size_t)tris[3 * (size_t)p + 1] * stride_floats;
+            const float* c = verts + (size_t)tris[3 * (size_t)p + 2] * stride_floats;
+            const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+            const float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+            const float hx = dy * e2z - dz * e2y, hy = dz * e2x - dx * e2z, hz = dx * e2y - dy * e2x;
+            const float det = dot3(hx, hy, hz, e1x, e1y, e1z);
+            if (std::fabs(det) < 1e-6f) continue;
+            const float f = 1.0f / det;
+            const float sx = ox - a[0], sy = oy - a[1], sz = oz - a[2];
+            const float u = f * dot3(sx, sy, sz, hx, hy, hz);
+            if (u < 0.0f || u > 1.0f) continue;
+            const float qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+            const float v = f * dot3(dx, dy, dz, qx, qy, qz);
+            if (v < 0.0f || u + v > 1.0f) continue;
+            const float t = f * dot3(e2x, e2y, e2z, qx, qy, qz);
+            if (t < 1e-6f) continue;
+            if (t < best || (t == best && p < best_prim)) {
+                best = t;
+                best_prim = p;
+            }
+        }
+        out_t[r] = best_prim == 0xFFFFFFFFu ? -1.0f : best;
+        out_prim[r] = best_prim;
+    }
+}
+
 }  // extern "C"

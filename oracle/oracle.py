@@ -83,6 +83,8 @@ def lib():
                                        ctypes.POINTER(u32), ctypes.POINTER(Stats)]
             L.oracle_build.restype = ctypes.c_int
             L.oracle_last_tie_events.restype = u32
+            L.oracle_trace_bruteforce.argtypes = [P, u32, P, u32, P, u32, P, P]
+            L.oracle_trace_bruteforce.restype = None
             _lib = L
     return _lib
 
@@ -131,3 +133,16 @@ def build(vertices=None, triangles=None, aabbs=None, *, vertex_stride_bytes=32,
         "stats": st.as_dict(),
         "tie_events": L.oracle_last_tie_events(),
     }
+
+
+def trace_bruteforce(vertices, triangles, rays):
+    """Closest hit of each ray against every triangle (CPU); returns (t, prim)."""
+    L = lib()
+    v = np.ascontiguousarray(vertices, dtype=np.float32)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32)
+    r = np.ascontiguousarray(rays, dtype=np.float32)
+    out_t = np.zeros(r.shape[0], np.float32)
+    out_p = np.zeros(r.shape[0], np.uint32)
+    L.oracle_trace_bruteforce(_ptr(v), v.shape[1], _ptr(t), t.shape[0], _ptr(r), r.shape[0],
+                              _ptr(out_t), _ptr(out_p))
+    return out_t, out_p
