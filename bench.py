@@ -55,6 +55,8 @@ def parse_args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="icosphere", choices=["icosphere", "mixed"],
                    help="icosphere: the headline build; mixed: 16.8M-triangle scene + 8M rays")
+    p.add_argument("--mixed-scale", type=int, default=1,
+                   help="divide the mixed scene and its ray count by this factor")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-pointer (e2e) leg")
     p.add_argument("--profile-steps", type=int, default=None, help=argparse.SUPPRESS)
@@ -377,10 +379,16 @@ def run_mixed(args):
     from marigold_b200 import BvhSettings, _lib, build_device, synth
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
-    v, t = synth.mixed_scene()
+    sc = max(1, args.mixed_scale)
+
+    def log(msg):
+        print(f"[mixed {time.perf_counter() - t0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+    v, t = synth.mixed_scene(n_blob=8388608 // sc, grid=(2048, 1024 // sc), n_thin=4194304 // sc)
     n = t.shape[0]
-    rays = synth.rays_in_box(8388608, v.min(0), v.max(0))
+    rays = synth.rays_in_box(8388608 // sc, v.min(0), v.max(0))
     gen_s = time.perf_counter() - t0
+    log(f"generated {n} triangles, {rays.shape[0]} rays")
     ctx = _lib.Context(0)
     dv = torch.from_numpy(v).cuda()
     dt = torch.from_numpy(t.view(np.int32)).cuda()
@@ -402,6 +410,7 @@ def run_mixed(args):
         torch.cuda.synchronize()
         if k >= max(args.warmup, 1):
             build_ms.append(e0.elapsed_time(e1))
+        log(f"build {k}: {e0.elapsed_time(e1):.2f} ms, {count} nodes, height {st.get('height')}")
     tr = _lib.Tracer(0)
     L = tr.L
     sp = ctypes.c_void_p(stream.cuda_stream)
@@ -421,26 +430,30 @@ def run_mixed(args):
                                            ctypes.byref(secs), sp))
         if k >= max(args.warmup, 1):
             trace_ms.append(secs.value * 1e3)
+        log(f"trace {k}: {secs.value * 1e3:.2f} ms, counts {list(counts)}")
     # check: 65,536-ray subset against GPU brute force, 16 rays against the CPU
-    sub = 65536
+    sub = min(65536, m)
     bt = torch.empty(sub, dtype=torch.float32, device="cuda")
     bp = torch.empty(sub, dtype=torch.int32, device="cuda")
     tb = time.perf_counter()
     tr.check(L.mgbvh_trace_bruteforce_dev(tr.ptr, vp(dr), sub, vp(bt), vp(bp), sp))
     brute_s = time.perf_counter() - tb
+    log(f"brute force {sub} rays: {brute_s:.1f} s")
     gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
     btn, bpn = bt.cpu().numpy(), bp.cpu().numpy().view(np.uint32)
     mism = int(((gp != bpn) | (gt.view(np.uint32) != btn.view(np.uint32))).sum())
     from oracle import oracle as orc
     ct, cp = orc.trace_bruteforce(v, t, rays[:16])
     cpu_mism = int(((cp != bpn[:16]) | (ct.view(np.uint32) != btn[:16].view(np.uint32))).sum())
+    log("cpu brute force done")
     hits = int((hp.cpu().numpy().view(np.uint32) != 0xFFFFFFFF).sum())
     bms = float(np.mean(build_ms))
     tms = float(np.mean(trace_ms))
     out = {
         "metric": "BVH build Mtri/s; closest-hit Mrays/s", "workload": "mixed scene",
-        "config": {"triangles": n, "rays": m, "blobs": 64, "grid_quads": [2048, 1024],
-                   "thin": 4194304, "max_depth": 32, "leaf": 1, "profile": "reference"},
+        "config": {"triangles": n, "rays": m, "blobs": 64, "grid_quads": [2048, 1024 // sc],
+                   "thin": 4194304 // sc, "scale": sc, "max_depth": 32, "leaf": 1,
+                   "profile": "reference"},
         "build": {"value": round(n / (bms * 1e-3) / 1e6, 2), "unit": "Mtri/s",
                   "ms": round(bms, 3), "nodes": count, "height": st.get("height"),
                   "phase_ms": [round(x * 1e3, 3) for x in st.get("phase_seconds", [])]},

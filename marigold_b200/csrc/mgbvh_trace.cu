@@ -73,7 +73,8 @@ __device__ __forceinline__ float intersect_tri(float ox, float oy, float oz, flo
 }
 
 // Conservative slab test: the entry distance if the box can hold a hit at a
-// distance <= best, else +inf.
+// distance <= best, else NaN (which fails every comparison, also with an
+// infinite best).
 __device__ __forceinline__ float box_entry(float ox, float oy, float oz, float ix, float iy, float iz,
                                            const float4& lo, const float4& hi, float best) {
     const float tx0 = (lo.x - ox) * ix, tx1 = (hi.x - ox) * ix;
@@ -82,7 +83,7 @@ __device__ __forceinline__ float box_entry(float ox, float oy, float oz, float i
     const float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
     float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fmaxf(tz0, tz1));
     tf *= 1.0000003576278687f;  // 1 + 2 * gamma(3), gamma(n) = n*eps/(1 - n*eps)
-    return (tn <= tf && tn <= best) ? tn : __int_as_float(0x7F800000);
+    return (tn <= tf && tn <= best) ? tn : __int_as_float(0x7FFFFFFF);
 }
 
 struct Counts {
