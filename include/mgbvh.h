@@ -190,6 +190,45 @@ MGBVH_API int mgbvh_build_aabbs_dev(mgbvh_ctx* ctx, const float* d_aabbs, uint32
                           uint32_t* d_out_perm, mgbvh_stats* out_stats);
 
 /*
+ * Batched build: one BVH per mesh, every mesh in one pass of the pipeline.
+ * The BLAS loop of marigold/src/app/data/scene/model.rs:77-95 (one
+ * BoundingVolumeHierarchy::new per mesh, rayon across meshes) plus the TLAS
+ * of marigold/src/app/data/scene/geometry/mod.rs:175-199 become one call:
+ * give the TLAS as one more mesh whose objects are the instance AABBs.
+ *
+ * Each mesh's result is exactly what mgbvh_build_indexed / _aabbs returns for
+ * it alone: its nodes sit at d_out_nodes[out_node_offsets[m] ..
+ * out_node_offsets[m+1]) with child links relative to that range (as the
+ * crate's per-mesh node arrays), and its permutation at d_out_perm[first ..
+ * first + count) with first = the sum of the earlier meshes' counts.
+ * node_capacity >= sum over meshes of (2 count - 1) is always enough.
+ * All array pointers are device pointers; `meshes` and out_node_offsets
+ * (mesh_count + 1 entries) are host arrays. The settings' bounds field is
+ * ignored (each mesh carries its own).
+ */
+typedef struct mgbvh_mesh_desc {
+    const float* vertices;      /* device; NULL when the objects are AABBs */
+    uint32_t vertex_stride_bytes;
+    uint32_t vertex_count;
+    const uint32_t* triangles;  /* device, count x 3 (when vertices != NULL) */
+    const float* aabbs;         /* device, count x 6 (when vertices == NULL) */
+    uint32_t count;             /* objects of this mesh */
+    uint32_t has_bounds;        /* BvhSettings::bounds is Some(..) for this mesh */
+    float bounds[6];
+} mgbvh_mesh_desc;
+
+MGBVH_API int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes,
+                                    uint32_t mesh_count, const mgbvh_settings* settings,
+                                    mgbvh_node* d_out_nodes, uint32_t node_capacity,
+                                    uint32_t* d_out_lens, uint32_t* d_out_perm,
+                                    uint32_t* out_node_offsets, mgbvh_stats* out_stats);
+
+/* Speed knob of a context, no effect on the trees: nodes with more than
+   medium_max objects (33..1024, default 1024) go through the level passes,
+   smaller ones to the per-subtree kernels. */
+MGBVH_API int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max);
+
+/*
  * Allocation-free build over device-resident AABBs. This entry point has no
  * counterpart in the reference. It exists for callers that must not allocate
  * while they build: a render loop that rebuilds its TLAS every frame (as

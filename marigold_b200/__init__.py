@@ -10,6 +10,7 @@ from .bvh import (  # noqa: F401
     BoundingVolume,
     BoundingVolumeHierarchy,
     BvhSettings,
+    build_batch_device,
     build_device,
     encode_gpu_bytes,
     sah_cost,

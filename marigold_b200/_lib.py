@@ -32,6 +32,7 @@ EXPORTED = (
     "mgbvh_build_indexed_dev", "mgbvh_build_aabbs_dev", "mgbvh_encode_gpu_bytes",
     "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc", "mgbvh_tracer_create", "mgbvh_tracer_destroy",
     "mgbvh_tracer_set_blas_dev", "mgbvh_trace_closest_dev", "mgbvh_trace_bruteforce_dev",
+    "mgbvh_build_batch_dev", "mgbvh_set_tuning",
 )
 
 
@@ -80,6 +81,21 @@ class Stats(ctypes.Structure):
         d = {name: getattr(self, name) for name, _ in self._fields_}
         d["phase_seconds"] = list(self.phase_seconds)
         return d
+
+
+class MeshDesc(ctypes.Structure):
+    """mgbvh_mesh_desc: one mesh of a batched build (device pointers)."""
+
+    _fields_ = [
+        ("vertices", ctypes.c_void_p),
+        ("vertex_stride_bytes", ctypes.c_uint32),
+        ("vertex_count", ctypes.c_uint32),
+        ("triangles", ctypes.c_void_p),
+        ("aabbs", ctypes.c_void_p),
+        ("count", ctypes.c_uint32),
+        ("has_bounds", ctypes.c_uint32),
+        ("bounds", ctypes.c_float * 6),
+    ]
 
 
 class MgbvhError(RuntimeError):
@@ -145,6 +161,11 @@ def load():
         L.mgbvh_trace_closest_dev.restype = ctypes.c_int
         L.mgbvh_trace_bruteforce_dev.argtypes = [P, P, u32, P, P, P]
         L.mgbvh_trace_bruteforce_dev.restype = ctypes.c_int
+        L.mgbvh_build_batch_dev.argtypes = [P, ctypes.POINTER(MeshDesc), u32, ctypes.POINTER(Settings),
+                                            P, u32, P, P, pu32, ctypes.POINTER(Stats)]
+        L.mgbvh_build_batch_dev.restype = ctypes.c_int
+        L.mgbvh_set_tuning.argtypes = [P, u32]
+        L.mgbvh_set_tuning.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]
         L.mgbvh_sah_cost.restype = ctypes.c_double
         _lib = L

@@ -264,3 +264,49 @@ def build_device(ctx: Context, settings: BvhSettings, out_nodes, out_perm, *, ve
             ctypes.c_void_p(out_perm.data_ptr()), ctypes.byref(st))
     ctx.check(rc)
     return count.value, rc, st.as_dict()
+
+
+def build_batch_device(ctx: Context, settings: BvhSettings, meshes, out_nodes, out_perm, *,
+                       out_lens=None, min_leaf_objects: int = 1, max_leaf_objects: int = 1,
+                       stream=None):
+    """Batched build: one BVH per mesh (BLAS per mesh, the TLAS as one more
+    mesh of instance AABBs), all in one pass.
+
+    meshes: list of dicts, each either {"vertices": float32 [V, k] tensor,
+    "triangles": int32 [N, 3] tensor} or {"aabbs": float32 [N, 6] tensor},
+    plus optional "bounds" (6 floats; BvhSettings::bounds of that mesh).
+    Returns (node_offsets [len(meshes) + 1], status, stats): mesh m's nodes
+    are out_nodes rows node_offsets[m]..node_offsets[m+1] (child links local
+    to that range), its permutation is out_perm[first:first + N_m].
+    """
+    import torch
+
+    L = ctx.L
+    s = stream if stream is not None else torch.cuda.current_stream()
+    ctx.set_stream(s.cuda_stream)
+    cs = settings.to_c(min_leaf_objects, max_leaf_objects)
+    descs = (_lib.MeshDesc * max(len(meshes), 1))()
+    for i, m in enumerate(meshes):
+        d = descs[i]
+        if "aabbs" in m:
+            d.aabbs = m["aabbs"].data_ptr()
+            d.count = m["aabbs"].shape[0]
+        else:
+            d.vertices = m["vertices"].data_ptr()
+            d.vertex_stride_bytes = m["vertices"].shape[1] * 4
+            d.vertex_count = m["vertices"].shape[0]
+            d.triangles = m["triangles"].data_ptr()
+            d.count = m["triangles"].shape[0]
+        if m.get("bounds") is not None:
+            d.has_bounds = 1
+            for k in range(6):
+                d.bounds[k] = float(m["bounds"][k])
+    offs = (ctypes.c_uint32 * (len(meshes) + 1))()
+    st = _lib.Stats()
+    cap = out_nodes.numel() * out_nodes.element_size() // 32
+    rc = L.mgbvh_build_batch_dev(ctx.ptr, descs, len(meshes), ctypes.byref(cs),
+                                 ctypes.c_void_p(out_nodes.data_ptr()), cap,
+                                 ctypes.c_void_p(out_lens.data_ptr()) if out_lens is not None else None,
+                                 ctypes.c_void_p(out_perm.data_ptr()), offs, ctypes.byref(st))
+    ctx.check(rc)
+    return list(offs), rc, st.as_dict()

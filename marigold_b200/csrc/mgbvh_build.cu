@@ -60,7 +60,8 @@ struct Task {
     float hi[3];
     uint32_t len;
     uint32_t slot, pair, depth, buf;
-    uint32_t tile0, ntiles, pad0, pad1;
+    uint32_t tile0, ntiles;
+    uint32_t nbase, tbase;  // node-slot and record offsets of the object's mesh (batched builds)
 };
 
 // Split decision of one large node, read by its partition tiles.
@@ -223,7 +224,7 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
     t.buf = 0;
     t.tile0 = 0;
     t.ntiles = ntiles;
-    t.pad0 = t.pad1 = 0;
+    t.nbase = t.tbase = 0;
     if (cls == 0) {
         if (gtid == 0) {
             mgbvh_node nd;
@@ -405,7 +406,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         }
     }
     if (leaf) {
-        warp_store_node(O, t.slot, nb, t.start, t.len, 0u, lane);
+        warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, 0u, lane);
         if (lane == 0) {
             A.dec[w] = d;
             if (t.len > 1) {
@@ -442,7 +443,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         carry += __shfl_sync(kFull, inc, 31);
     }
     if (carry != d.n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
-    warp_store_node(O, t.slot, nb, t.start, t.len, t.pair, lane);
+    warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, t.pair, lane);
     if (lane == 0) atomicMax(&O.ctr->height, t.depth);
     const uint32_t n_gt = t.len - d.n_lt;
     for (int c = 0; c < 2; ++c) {
@@ -465,15 +466,16 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         ct.depth = depth;
         ct.buf = t.buf ^ 1u;
         ct.tile0 = ct.ntiles = 0;
-        ct.pad0 = ct.pad1 = 0;
+        ct.nbase = t.nbase;
+        ct.tbase = t.tbase;
         if (cleaf) {
-            warp_store_node(O, slot, cb, start, len, 0u, lane);
+            warp_store_node(O, t.nbase + slot, cb, start - t.tbase, len, 0u, lane);
             d.child_leaf[c] = 1;
             if (lane == 0 && len > 1) {
                 atomicAdd(&O.ctr->holes, 1u);
                 if (depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
             }
-        } else if (len > kMediumMax) {
+        } else if (len > P.medium_max) {
             const uint32_t nt = (len + kTile - 1) / kTile;
             uint32_t ti = 0, t0 = 0;
             if (lane == 0) {
@@ -697,9 +699,9 @@ __device__ __forceinline__ void medium_load_warp_records(const MediumSmem& S, ui
 // Warp: finish a leaf of the medium subtree (record + permutation).
 __device__ __forceinline__ void medium_leaf(const MediumSmem& S, uint32_t ib, uint32_t base,
                                             uint32_t s, uint32_t n, uint32_t slot, uint32_t depth,
-                                            const float* b, const Params& P, const Out& O,
-                                            uint32_t lane) {
-    warp_store_node(O, slot, b, base + s, n, 0u, lane);
+                                            const float* b, uint32_t nbase, uint32_t tbase,
+                                            const Params& P, const Out& O, uint32_t lane) {
+    warp_store_node(O, nbase + slot, b, base + s - tbase, n, 0u, lane);
     for (uint32_t p = lane; p < n; p += 32)
         O.perm[base + s + p] = __float_as_uint(S.rlo[S.idx[ib][s + p]].w);
     if (lane == 0 && n > 1) {
@@ -881,7 +883,7 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
                 }
             }
             if (leaf) {
-                medium_leaf(S, ib, base, s, n, nd.slot, depth, nd.b, P, O, lane);
+                medium_leaf(S, ib, base, s, n, nd.slot, depth, nd.b, t.nbase, t.tbase, P, O, lane);
                 continue;
             }
             uint32_t ck[12];
@@ -970,7 +972,7 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
             }
             if (__any_sync(kFull, bad) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
             warp_reduce_keys12(ck);
-            warp_store_node(O, nd.slot, nd.b, base + s, n, nd.pair, lane);
+            warp_store_node(O, t.nbase + nd.slot, nd.b, base + s - t.tbase, n, nd.pair, lane);
             any_split = true;
             hmax = max(hmax, depth);
             const uint32_t n_gt = n - n_lt;
@@ -985,7 +987,7 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
                 const bool cleaf =
                     len <= 1u || cdepth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
                 if (cleaf) {
-                    medium_leaf(S, ob, base, cs, len, slot, cdepth, cbx, P, O, lane);
+                    medium_leaf(S, ob, base, cs, len, slot, cdepth, cbx, t.nbase, t.tbase, P, O, lane);
                 } else if (len > kSmallMax) {
                     uint32_t li2 = 0;
                     if (lane == 0) li2 = atomicAdd(&S.list_n[cur ^ 1u], 1u);
@@ -1030,7 +1032,9 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
                         st.pair = pair;
                         st.depth = cdepth;
                         st.buf = t.buf;
-                        st.tile0 = st.ntiles = st.pad0 = st.pad1 = 0;
+                        st.tile0 = st.ntiles = 0;
+                        st.nbase = t.nbase;
+                        st.tbase = t.tbase;
                         small[si] = st;
                     }
                 }
@@ -1085,11 +1089,11 @@ __global__ void __launch_bounds__(256) small_kernel(const Task* __restrict__ tas
         }
         const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
         if constexpr (kLevels)
-            warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O,
-                                      xchg[wib]);
+            warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase,
+                                      t.tbase, b, P, O, xchg[wib]);
         else
-            warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, b, P, O,
-                               xchg[wib]);
+            warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase,
+                               b, P, O, xchg[wib]);
     }
 }
 
@@ -1113,6 +1117,189 @@ __global__ void compact_kernel(const mgbvh_node* __restrict__ src, const uint32_
     }
 }
 
+
+
+// ---------------------------------------------------------------- batched builds
+//
+// Many BVHs (the BLAS of every mesh and the TLAS over instances) in one
+// pipeline: the objects of all meshes are one record array, each mesh's root
+// is queued like a single build's root, and every node a kernel writes goes
+// to its mesh's own node range (slots offset by nbase, start indices
+// relative to the mesh's first record at tbase), so each mesh's nodes, child
+// links and permutation are exactly those of a build of that mesh alone.
+
+struct DevMesh {
+    const float* verts;  // NULL for an AABB list
+    const uint32_t* tris;
+    const float* aabbs;
+    uint32_t stride_floats, nverts;
+    uint32_t n, tbase, nbase;
+    uint32_t has_bounds;
+    float bounds[6];
+    uint32_t cls, list_index, tile0, ntiles;  // root plan (0 leaf, 1 small, 2 medium, 3 large, 4 empty)
+};
+
+__device__ __forceinline__ uint32_t mesh_of(const uint32_t* __restrict__ offs, uint32_t nm, uint32_t g) {
+    uint32_t lo = 0, hi = nm;  // offs[lo] <= g < offs[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (offs[mid] <= g)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Object records of every mesh (local object ids) and per-mesh root keys
+// (bounds lo/hi, centroid lo/hi; 12 per mesh).
+__global__ void __launch_bounds__(256) prep_batch_kernel(const DevMesh* __restrict__ meshes,
+                                                         const uint32_t* __restrict__ toffs,
+                                                         uint32_t nm, uint32_t total,
+                                                         Rec* __restrict__ out, uint32_t* mkeys,
+                                                         Counters* ctr) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // whole warps iterate together so that same-mesh warps can reduce first
+    for (uint32_t g0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u; g0 < total; g0 += stride) {
+        const uint32_t g = g0 + lane;
+        const bool valid = g < total;
+        uint32_t m = valid ? mesh_of(toffs, nm, g) : 0u;
+        float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+        if (valid) {
+            const DevMesh& M = meshes[m];
+            const uint32_t l = g - M.tbase;
+            if (M.verts) {
+                uint32_t t0 = M.tris[3 * (size_t)l], t1 = M.tris[3 * (size_t)l + 1],
+                         t2 = M.tris[3 * (size_t)l + 2];
+                if (t0 >= M.nverts || t1 >= M.nverts || t2 >= M.nverts) {
+                    set_error(ctr, MGBVH_ERR_INVALID_ARG, kSiteIndex);
+                    t0 = t1 = t2 = 0;
+                }
+                const float* p0 = M.verts + (size_t)t0 * M.stride_floats;
+                const float* p1 = M.verts + (size_t)t1 * M.stride_floats;
+                const float* p2 = M.verts + (size_t)t2 * M.stride_floats;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float x0 = __fadd_rn(__ldg(p0 + a), 0.0f), x1 = __fadd_rn(__ldg(p1 + a), 0.0f),
+                                x2 = __fadd_rn(__ldg(p2 + a), 0.0f);
+                    lo[a] = fminf(fminf(x0, x1), x2);
+                    hi[a] = fmaxf(fmaxf(x0, x1), x2);
+                }
+            } else {
+                const float* p = M.aabbs + 6 * (size_t)l;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = __fadd_rn(__ldg(p + a), 0.0f);
+                    hi[a] = __fadd_rn(__ldg(p + 3 + a), 0.0f);
+                }
+            }
+            Rec r;
+            r.lo = make_float4(lo[0], lo[1], lo[2], __uint_as_float(l));
+            r.hi = make_float4(hi[0], hi[1], hi[2], 0.0f);
+            out[g] = r;
+        }
+        uint32_t k[12];
+        init_key12(k);
+        if (valid) accum_keys(k, lo[0], lo[1], lo[2], hi[0], hi[1], hi[2]);
+        const uint32_t m0 = __shfl_sync(kFull, m, 0);
+        const bool uniform = __all_sync(kFull, !valid || m == m0);
+        if (uniform) {
+#pragma unroll
+            for (int q = 0; q < 12; ++q) {
+                const bool is_min = (q % 6) < 3;
+                const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+                if (lane == 0) {
+                    if (is_min)
+                        atomicMin(&mkeys[12 * m0 + q], v);
+                    else
+                        atomicMax(&mkeys[12 * m0 + q], v);
+                }
+            }
+        } else if (valid) {
+#pragma unroll
+            for (int q = 0; q < 12; ++q) {
+                if ((q % 6) < 3)
+                    atomicMin(&mkeys[12 * m + q], k[q]);
+                else
+                    atomicMax(&mkeys[12 * m + q], k[q]);
+            }
+        }
+    }
+}
+
+__global__ void init_mkeys_kernel(uint32_t* mkeys, uint32_t nm) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 12 * nm; i += gridDim.x * blockDim.x)
+        mkeys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+}
+
+// One warp per mesh: queue its root (or finish it when the root is a leaf).
+__global__ void init_roots_kernel(const DevMesh* __restrict__ meshes, uint32_t nm,
+                                  const uint32_t* __restrict__ mkeys, Task* large, uint32_t* bins,
+                                  uint32_t* cbkeys, uint32_t* tile_task, uint32_t* tile_begin,
+                                  Task* medium, Task* small, Out O, uint32_t max_depth) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; m < nm; m += nwarps) {
+        const DevMesh& M = meshes[m];
+        if (M.cls > 3) continue;  // empty mesh: nothing to build
+        float b[6];
+        for (int i = 0; i < 6; ++i) b[i] = M.has_bounds ? M.bounds[i] : funkey(mkeys[12 * m + i]);
+        Task t;
+        for (int a = 0; a < 3; ++a) {
+            t.lo[a] = b[a];
+            t.hi[a] = b[3 + a];
+        }
+        t.start = M.tbase;
+        t.len = M.n;
+        t.slot = 0;
+        t.pair = 1;
+        t.depth = 0;
+        t.buf = 0;
+        t.tile0 = M.tile0;
+        t.ntiles = M.ntiles;
+        t.nbase = M.nbase;
+        t.tbase = M.tbase;
+        if (M.cls == 0) {
+            warp_store_node(O, M.nbase, b, 0u, M.n, 0u, lane);
+            for (uint32_t i = lane; i < M.n; i += 32) O.perm[M.tbase + i] = i;
+            if (lane == 0 && M.n > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (max_depth == 0) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+        } else if (M.cls == 1) {
+            if (lane == 0) small[M.list_index] = t;
+        } else if (M.cls == 2) {
+            if (lane == 0) medium[M.list_index] = t;
+        } else {
+            if (lane == 0) large[M.list_index] = t;
+            init_task_bins(bins + (size_t)M.list_index * kBinWords, lane, 32);
+            if (lane < 6) cbkeys[6 * M.list_index + lane] = mkeys[12 * m + 6 + lane];
+            for (uint32_t i = lane; i < M.ntiles; i += 32) {
+                tile_task[M.tile0 + i] = M.list_index;
+                tile_begin[M.tile0 + i] = i * kTile;
+            }
+        }
+    }
+}
+
+// Compaction of a batch: slot s of mesh m moves to newidx[s] and its child
+// link (local) to newidx[nbase_m + child] - newidx[nbase_m].
+__global__ void compact_batch_kernel(const mgbvh_node* __restrict__ src, const uint32_t* __restrict__ lens,
+                                     const uint8_t* __restrict__ used, const uint32_t* __restrict__ newidx,
+                                     const uint32_t* __restrict__ noffs, uint32_t nm, uint32_t slots,
+                                     mgbvh_node* __restrict__ dst, uint32_t* dst_lens) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < slots; s += gridDim.x * blockDim.x) {
+        if (!used[s]) continue;
+        const uint32_t m = mesh_of(noffs, nm, s);
+        const uint32_t base_new = newidx[noffs[m]];
+        mgbvh_node nd = src[s];
+        if (nd.child_node) nd.child_node = newidx[noffs[m] + nd.child_node] - base_new;
+        const uint32_t d = newidx[s];
+        dst[d] = nd;
+        if (dst_lens) dst_lens[d] = lens[s];
+    }
+}
 
 // ---------------------------------------------------------------- allocation-free build
 //
@@ -1212,6 +1399,7 @@ struct mgbvh_ctx {
     int device = 0;
     int sm_count = 148;
     uint32_t levels_hint = 0;
+    uint32_t medium_max = kMediumMax;  // level-pass / subtree switch-over (speed only)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp[3] = {nullptr, nullptr, nullptr};
@@ -1219,6 +1407,7 @@ struct mgbvh_ctx {
     DevBuf rec[2], tasks[2], bins[2], cbkeys[2], tile_task[2], tile_begin[2];
     DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
     DevBuf in_a, in_b, out_nodes, out_lens;
+    DevBuf mesh_buf, toff_buf, noff_buf, mkeys;
     Counters* h_ctr = nullptr;
 };
 
@@ -1258,13 +1447,17 @@ struct Caps {
     uint32_t tasks, tiles, medium, small, nodes;
 };
 
-Caps caps_for(uint32_t n) {
+// List capacities for n objects over `meshes` roots. Nodes above medium_max
+// are disjoint at one level (<= n / (medium_max + 1) of them), and a binary
+// tree over n objects has fewer than 2n / medium_max nodes above medium_max,
+// each with two children at most.
+Caps caps_for(uint32_t n, uint32_t medium_max, uint32_t meshes, uint32_t node_slots) {
     Caps c;
-    c.tasks = n / (kMediumMax + 1) + 2;
+    c.tasks = n / (medium_max + 1) + 2;
     c.tiles = n / kTile + c.tasks + 2;
-    c.medium = 4 * (n / kMediumMax) + 8;
-    c.small = n / 2 + 8;
-    c.nodes = 2 * n - 1;
+    c.medium = 4 * (n / medium_max) + meshes + 8;
+    c.small = n / 2 + meshes + 8;
+    c.nodes = node_slots;
     return c;
 }
 
@@ -1308,95 +1501,19 @@ const char* site_text(uint32_t site) {
     }
 }
 
-// Runs a build whose inputs are device-resident. Outputs go to device memory:
-// d_nodes (capacity cap), d_lens (nullable), d_perm. Returns status.
-int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_node* d_nodes,
-              uint32_t cap, uint32_t* d_lens, uint32_t* d_perm, uint32_t* out_count,
-              mgbvh_stats* stats) {
-    const uint32_t n = in.n;
+// Level passes (nodes above medium_max), then the medium and small subtree
+// kernels, on the context's stream. Root tasks are already queued.
+int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, Rec* rec0, Rec* rec1,
+                 bool has_large, uint32_t& launches, uint32_t& levels) {
     const cudaStream_t sm = ctx->stream;
-    if (n > 0x7FFFFFFFu) return fail(ctx, MGBVH_ERR_UNSUPPORTED, "more than 2^31-1 objects");
-    const Caps C = caps_for(n);
-    int rc;
-#define ENS(buf, bytes) \
-    if ((rc = ensure(ctx, buf, (bytes))) != MGBVH_OK) return rc
-    ENS(ctx->rec[0], sizeof(Rec) * (size_t)n);
-    ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
-    for (int i = 0; i < 2; ++i) {
-        ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
-        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
-        ENS(ctx->cbkeys[i], 24ull * C.tasks);
-        ENS(ctx->tile_task[i], 4ull * C.tiles);
-        ENS(ctx->tile_begin[i], 4ull * C.tiles);
-    }
-    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);  // [axis][bin][tile]
-    ENS(ctx->tile_lt, 4ull * C.tiles);
-    ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
-    ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
-    ENS(ctx->small, sizeof(Task) * (size_t)C.small);
-    ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
-    ENS(ctx->lens, 4ull * C.nodes);
-    ENS(ctx->used, (size_t)C.nodes);
-    ENS(ctx->ctr, sizeof(Counters));
-#undef ENS
-    Params P;
-    P.min_leaf = st->min_leaf_objects;
-    P.max_leaf = st->max_leaf_objects;
-    P.max_depth = st->max_depth;
-    P.bins = st->bins;
-    P.adaptive_max_n = st->adaptive_max_n;
-    P.adaptive_steps = st->adaptive_steps;
-
-    Counters init;
-    std::memset(&init, 0, sizeof(init));
-    for (int i = 0; i < 12; ++i) init.root_keys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
-    Counters* d_ctr = P_<Counters>(ctx->ctr);
-    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
-    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
-
-    Out O;
-    O.nodes = P_<mgbvh_node>(ctx->nodes);
-    O.lens = P_<uint32_t>(ctx->lens);
-    O.used = P_<uint8_t>(ctx->used);
-    O.perm = d_perm;
-    O.ctr = d_ctr;
-    O.node_cap = C.nodes;
-    Rec* rec0 = P_<Rec>(ctx->rec[0]);
-    Rec* rec1 = P_<Rec>(ctx->rec[1]);
-
-    MG_CUDA(cudaEventRecord(ctx->ev0, sm));
-    const int prep_blocks = (int)std::min<uint32_t>((n + 255) / 256, 148u * 8u);
-    if (in.kind == kIndexed)
-        prep_indexed_kernel<<<prep_blocks, 256, 0, sm>>>(in.verts, in.stride_bytes / 4, in.nverts,
-                                                          in.tris, n, rec0, d_ctr);
-    else
-        prep_aabbs_kernel<<<prep_blocks, 256, 0, sm>>>(in.aabbs, n, rec0, d_ctr);
-
-    const bool root_leaf = n <= 1 || st->max_depth == 0 ||
-                           (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
-    const uint32_t cls = root_leaf ? 0u : (n <= kSmallMax ? 1u : (n <= kMediumMax ? 2u : 3u));
-    const uint32_t ntiles0 = (n + kTile - 1) / kTile;
-    const float* bb = st->bounds;
-    {
-        const int blocks = (int)std::min<uint32_t>((std::max(n, ntiles0) + 255) / 256 + 1, 1024u);
-        init_root_kernel<<<blocks, 256, 0, sm>>>(
-            n, cls, st->has_bounds, bb[0], bb[1], bb[2], bb[3], bb[4], bb[5], P_<Task>(ctx->tasks[0]),
-            P_<uint32_t>(ctx->bins[0]), P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]),
-            P_<uint32_t>(ctx->tile_begin[0]), P_<Task>(ctx->medium), P_<Task>(ctx->small), O, ntiles0,
-            st->max_depth);
-    }
-    MG_CUDA(cudaGetLastError());
-    MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
-    uint32_t launches = 2, levels = 0;
-    (void)ntiles0;
-
+    Counters* d_ctr = O.ctr;
     // Level passes over the large nodes. Kernels read their task and tile
     // counts on the device, so levels are launched in batches and the host
     // reads the next level's count only at the end of a batch.
     const int tile_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * 8u);
     const int eval_grid = (int)std::min<uint32_t>((C.tasks + 3) / 4, (uint32_t)ctx->sm_count * 4u);
     uint32_t level = 0;
-    bool more = cls == 3;
+    bool more = has_large;
     ctx->h_ctr->error = 0;
     bool first_batch = true;
     while (more) {
@@ -1441,8 +1558,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
         if (ctx->h_ctr->error) break;
         more = ctx->h_ctr->lvl[level & 1u][0] > 0;
     }
-    if (cls == 3) {
-        // levels that did work: the count of the last non-empty level
+    if (has_large) {
         ctx->levels_hint = level;
         levels = level;
     }
@@ -1464,6 +1580,94 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     } else {
         MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
     }
+    return MGBVH_OK;
+}
+
+// Runs a build whose inputs are device-resident. Outputs go to device memory:
+// d_nodes (capacity cap), d_lens (nullable), d_perm. Returns status.
+int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_node* d_nodes,
+              uint32_t cap, uint32_t* d_lens, uint32_t* d_perm, uint32_t* out_count,
+              mgbvh_stats* stats) {
+    const uint32_t n = in.n;
+    const cudaStream_t sm = ctx->stream;
+    if (n > 0x7FFFFFFFu) return fail(ctx, MGBVH_ERR_UNSUPPORTED, "more than 2^31-1 objects");
+    const Caps C = caps_for(n, ctx->medium_max, 1, 2 * n - 1);
+    int rc;
+#define ENS(buf, bytes) \
+    if ((rc = ensure(ctx, buf, (bytes))) != MGBVH_OK) return rc
+    ENS(ctx->rec[0], sizeof(Rec) * (size_t)n);
+    ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
+    for (int i = 0; i < 2; ++i) {
+        ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
+        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
+        ENS(ctx->cbkeys[i], 24ull * C.tasks);
+        ENS(ctx->tile_task[i], 4ull * C.tiles);
+        ENS(ctx->tile_begin[i], 4ull * C.tiles);
+    }
+    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);  // [axis][bin][tile]
+    ENS(ctx->tile_lt, 4ull * C.tiles);
+    ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
+    ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
+    ENS(ctx->small, sizeof(Task) * (size_t)C.small);
+    ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
+    ENS(ctx->lens, 4ull * C.nodes);
+    ENS(ctx->used, (size_t)C.nodes);
+    ENS(ctx->ctr, sizeof(Counters));
+#undef ENS
+    Params P;
+    P.min_leaf = st->min_leaf_objects;
+    P.max_leaf = st->max_leaf_objects;
+    P.max_depth = st->max_depth;
+    P.bins = st->bins;
+    P.adaptive_max_n = st->adaptive_max_n;
+    P.adaptive_steps = st->adaptive_steps;
+    P.medium_max = ctx->medium_max;
+
+    Counters init;
+    std::memset(&init, 0, sizeof(init));
+    for (int i = 0; i < 12; ++i) init.root_keys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    Counters* d_ctr = P_<Counters>(ctx->ctr);
+    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
+
+    Out O;
+    O.nodes = P_<mgbvh_node>(ctx->nodes);
+    O.lens = P_<uint32_t>(ctx->lens);
+    O.used = P_<uint8_t>(ctx->used);
+    O.perm = d_perm;
+    O.ctr = d_ctr;
+    O.node_cap = C.nodes;
+    Rec* rec0 = P_<Rec>(ctx->rec[0]);
+    Rec* rec1 = P_<Rec>(ctx->rec[1]);
+
+    MG_CUDA(cudaEventRecord(ctx->ev0, sm));
+    const int prep_blocks = (int)std::min<uint32_t>((n + 255) / 256, 148u * 8u);
+    if (in.kind == kIndexed)
+        prep_indexed_kernel<<<prep_blocks, 256, 0, sm>>>(in.verts, in.stride_bytes / 4, in.nverts,
+                                                          in.tris, n, rec0, d_ctr);
+    else
+        prep_aabbs_kernel<<<prep_blocks, 256, 0, sm>>>(in.aabbs, n, rec0, d_ctr);
+
+    const bool root_leaf = n <= 1 || st->max_depth == 0 ||
+                           (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
+    const uint32_t cls = root_leaf ? 0u : (n <= kSmallMax ? 1u : (n <= P.medium_max ? 2u : 3u));
+    const uint32_t ntiles0 = (n + kTile - 1) / kTile;
+    const float* bb = st->bounds;
+    {
+        const int blocks = (int)std::min<uint32_t>((std::max(n, ntiles0) + 255) / 256 + 1, 1024u);
+        init_root_kernel<<<blocks, 256, 0, sm>>>(
+            n, cls, st->has_bounds, bb[0], bb[1], bb[2], bb[3], bb[4], bb[5], P_<Task>(ctx->tasks[0]),
+            P_<uint32_t>(ctx->bins[0]), P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]),
+            P_<uint32_t>(ctx->tile_begin[0]), P_<Task>(ctx->medium), P_<Task>(ctx->small), O, ntiles0,
+            st->max_depth);
+    }
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+    uint32_t launches = 2, levels = 0;
+    (void)ntiles0;
+
+    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, cls == 3, launches, levels)) != MGBVH_OK)
+        return rc;
     MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
     MG_CUDA(cudaStreamSynchronize(sm));
@@ -1570,6 +1774,212 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     const uint32_t MIN = st->min_leaf_objects, MAX = st->max_leaf_objects;
     const bool feasible = (MIN == MAX) ? (n % MIN == 0) : (MAX >= 2 * MIN - 1);  // :710-714
     return feasible ? MGBVH_OK : MGBVH_WARN_INFEASIBLE;
+}
+
+
+// Batched build over several meshes (see include/mgbvh.h).
+int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const mgbvh_settings* st,
+              mgbvh_node* d_nodes, uint32_t cap, uint32_t* d_lens, uint32_t* d_perm,
+              uint32_t* out_offsets, mgbvh_stats* stats) {
+    const cudaStream_t sm = ctx->stream;
+    int rc;
+    // offsets and the root plan
+    std::vector<DevMesh> hm(nm);
+    std::vector<uint32_t> toffs(nm + 1), noffs(nm + 1);
+    uint64_t total = 0, slots = 0;
+    uint32_t n_large = 0, n_medium = 0, n_small = 0, tiles = 0;
+    for (uint32_t m = 0; m < nm; ++m) {
+        const mgbvh_mesh_desc& d = meshes[m];
+        DevMesh& M = hm[m];
+        std::memset(&M, 0, sizeof(M));
+        const bool tri = d.vertices != nullptr;
+        if (d.count && tri && (!d.triangles || d.vertex_stride_bytes < 12 || d.vertex_stride_bytes % 4))
+            return fail(ctx, MGBVH_ERR_INVALID_ARG, "mesh " + std::to_string(m) + ": bad vertex data");
+        if (d.count && !tri && !d.aabbs)
+            return fail(ctx, MGBVH_ERR_INVALID_ARG, "mesh " + std::to_string(m) + ": no objects");
+        M.verts = d.vertices;
+        M.tris = d.triangles;
+        M.aabbs = d.aabbs;
+        M.stride_floats = d.vertex_stride_bytes / 4;
+        M.nverts = d.vertex_count;
+        M.n = d.count;
+        M.tbase = (uint32_t)total;
+        M.nbase = (uint32_t)slots;
+        M.has_bounds = d.has_bounds;
+        for (int i = 0; i < 6; ++i) M.bounds[i] = d.bounds[i];
+        toffs[m] = (uint32_t)total;
+        noffs[m] = (uint32_t)slots;
+        total += d.count;
+        slots += d.count ? 2ull * d.count - 1 : 0;
+        if (total > 0x7FFFFFFFull || slots > 0xFFFFFFFEull)
+            return fail(ctx, MGBVH_ERR_UNSUPPORTED, "batch above 2^31-1 objects");
+        const uint32_t n = d.count;
+        if (n == 0) {
+            M.cls = 4;  // nothing to build
+            continue;
+        }
+        const bool leaf = n <= 1 || st->max_depth == 0 ||
+                          (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
+        if (leaf) {
+            M.cls = 0;
+        } else if (n <= kSmallMax) {
+            M.cls = 1;
+            M.list_index = n_small++;
+        } else if (n <= ctx->medium_max) {
+            M.cls = 2;
+            M.list_index = n_medium++;
+        } else {
+            M.cls = 3;
+            M.list_index = n_large++;
+            M.tile0 = tiles;
+            M.ntiles = (n + kTile - 1) / kTile;
+            tiles += M.ntiles;
+        }
+    }
+    toffs[nm] = (uint32_t)total;
+    noffs[nm] = (uint32_t)slots;
+    if (total == 0) {
+        for (uint32_t m = 0; m <= nm; ++m) out_offsets[m] = 0;
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return MGBVH_WARN_EMPTY;
+    }
+    const uint32_t n = (uint32_t)total;
+    const Caps C = caps_for(n, ctx->medium_max, nm, (uint32_t)slots);
+#define ENS(buf, bytes) \
+    if ((rc = ensure(ctx, buf, (bytes))) != MGBVH_OK) return rc
+    ENS(ctx->rec[0], sizeof(Rec) * (size_t)n);
+    ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
+    for (int i = 0; i < 2; ++i) {
+        ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
+        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
+        ENS(ctx->cbkeys[i], 24ull * C.tasks);
+        ENS(ctx->tile_task[i], 4ull * C.tiles);
+        ENS(ctx->tile_begin[i], 4ull * C.tiles);
+    }
+    ENS(ctx->tile_hist, 4ull * 96 * C.tiles);
+    ENS(ctx->tile_lt, 4ull * C.tiles);
+    ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
+    ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
+    ENS(ctx->small, sizeof(Task) * (size_t)C.small);
+    ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
+    ENS(ctx->lens, 4ull * C.nodes);
+    ENS(ctx->used, (size_t)C.nodes);
+    ENS(ctx->ctr, sizeof(Counters));
+    ENS(ctx->mesh_buf, sizeof(DevMesh) * (size_t)nm);
+    ENS(ctx->toff_buf, 4ull * (nm + 1));
+    ENS(ctx->noff_buf, 4ull * (nm + 1));
+    ENS(ctx->mkeys, 48ull * nm);
+#undef ENS
+    if (n_large > C.tasks || tiles > C.tiles || n_medium > C.medium || n_small > C.small)
+        return fail(ctx, MGBVH_ERR_CAPACITY, "batch root lists exceed their capacity");
+    Params P;
+    P.min_leaf = st->min_leaf_objects;
+    P.max_leaf = st->max_leaf_objects;
+    P.max_depth = st->max_depth;
+    P.bins = st->bins;
+    P.adaptive_max_n = st->adaptive_max_n;
+    P.adaptive_steps = st->adaptive_steps;
+    P.medium_max = ctx->medium_max;
+    Counters init;
+    std::memset(&init, 0, sizeof(init));
+    init.lvl[0][0] = n_large;
+    init.lvl[0][1] = tiles;
+    init.n_medium = n_medium;
+    init.n_small = n_small;
+    Counters* d_ctr = P_<Counters>(ctx->ctr);
+    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->mesh_buf.p, hm.data(), sizeof(DevMesh) * (size_t)nm,
+                            cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->toff_buf.p, toffs.data(), 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->noff_buf.p, noffs.data(), 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
+    Out O;
+    O.nodes = P_<mgbvh_node>(ctx->nodes);
+    O.lens = P_<uint32_t>(ctx->lens);
+    O.used = P_<uint8_t>(ctx->used);
+    O.perm = d_perm;
+    O.ctr = d_ctr;
+    O.node_cap = C.nodes;
+    Rec* rec0 = P_<Rec>(ctx->rec[0]);
+    Rec* rec1 = P_<Rec>(ctx->rec[1]);
+    const DevMesh* dmesh = P_<DevMesh>(ctx->mesh_buf);
+    MG_CUDA(cudaEventRecord(ctx->ev0, sm));
+    init_mkeys_kernel<<<std::max(1u, std::min((12 * nm + 255) / 256, 1024u)), 256, 0, sm>>>(
+        P_<uint32_t>(ctx->mkeys), nm);
+    prep_batch_kernel<<<(int)std::min<uint32_t>((n + 255) / 256, 148u * 8u), 256, 0, sm>>>(
+        dmesh, P_<uint32_t>(ctx->toff_buf), nm, n, rec0, P_<uint32_t>(ctx->mkeys), d_ctr);
+    init_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
+        dmesh, nm, P_<uint32_t>(ctx->mkeys), P_<Task>(ctx->tasks[0]), P_<uint32_t>(ctx->bins[0]),
+        P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]), P_<uint32_t>(ctx->tile_begin[0]),
+        P_<Task>(ctx->medium), P_<Task>(ctx->small), O, st->max_depth);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+    uint32_t launches = 4, levels = 0;
+    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, n_large > 0, launches, levels)) != MGBVH_OK)
+        return rc;
+    MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaStreamSynchronize(sm));
+    const Counters hc = *ctx->h_ctr;
+    if (hc.error) return fail(ctx, (int)hc.error, site_text(hc.error_site));
+    float ms = 0.0f;
+    MG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    uint32_t count = (uint32_t)slots;
+    if (hc.holes > 0) {
+        if ((rc = ensure(ctx, ctx->newidx, 4ull * C.nodes)) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->widened, 4ull * C.nodes)) != MGBVH_OK) return rc;
+        widen_used_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
+            P_<uint8_t>(ctx->used), C.nodes, P_<uint32_t>(ctx->widened));
+        size_t tmp = 0;
+        MG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp, P_<uint32_t>(ctx->widened),
+                                              P_<uint32_t>(ctx->newidx), C.nodes, sm));
+        if ((rc = ensure(ctx, ctx->cub_tmp, tmp)) != MGBVH_OK) return rc;
+        MG_CUDA(cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp, P_<uint32_t>(ctx->widened),
+                                              P_<uint32_t>(ctx->newidx), C.nodes, sm));
+        std::vector<uint32_t> nidx(C.nodes);
+        MG_CUDA(cudaMemcpyAsync(nidx.data(), ctx->newidx.p, 4ull * C.nodes, cudaMemcpyDeviceToHost, sm));
+        uint8_t last_used = 0;
+        MG_CUDA(cudaMemcpyAsync(&last_used, P_<uint8_t>(ctx->used) + (C.nodes - 1), 1,
+                                cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        count = nidx[C.nodes - 1] + last_used;
+        for (uint32_t m = 0; m < nm; ++m) out_offsets[m] = noffs[m] < C.nodes ? nidx[noffs[m]] : count;
+        out_offsets[nm] = count;
+        if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the trees");
+        compact_batch_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
+            P_<mgbvh_node>(ctx->nodes), P_<uint32_t>(ctx->lens), P_<uint8_t>(ctx->used),
+            P_<uint32_t>(ctx->newidx), P_<uint32_t>(ctx->noff_buf), nm, C.nodes, d_nodes, d_lens);
+        MG_CUDA(cudaGetLastError());
+    } else {
+        if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the trees");
+        for (uint32_t m = 0; m <= nm; ++m) out_offsets[m] = noffs[m];
+        MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
+                                cudaMemcpyDeviceToDevice, sm));
+        if (d_lens)
+            MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * count, cudaMemcpyDeviceToDevice, sm));
+    }
+    MG_CUDA(cudaStreamSynchronize(sm));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->construction_time = ms * 1e-3;
+        stats->node_count = count;
+        stats->total_object_count = n;
+        stats->height = hc.height;
+        stats->max_depth = st->max_depth;
+        stats->median_splits = hc.median_splits;
+        stats->depth_capped_leaves = hc.depth_capped;
+        stats->kernel_launches = launches;
+        stats->levels = levels;
+        const uint32_t MIN = st->min_leaf_objects, MAX = st->max_leaf_objects;
+        stats->feasible = MIN == MAX ? 1u : (MAX >= 2 * MIN - 1);
+        float pm[4] = {0.f, 0.f, 0.f, 0.f};
+        cudaEventElapsedTime(&pm[0], ctx->ev0, ctx->evp[0]);
+        cudaEventElapsedTime(&pm[1], ctx->evp[0], ctx->evp[1]);
+        cudaEventElapsedTime(&pm[2], ctx->evp[1], ctx->evp[2]);
+        cudaEventElapsedTime(&pm[3], ctx->evp[2], ctx->ev1);
+        for (int i = 0; i < 4; ++i) stats->phase_seconds[i] = pm[i] * 1e-3;
+    }
+    return MGBVH_OK;
 }
 
 int check_ctx(mgbvh_ctx* ctx) {
@@ -1726,7 +2136,8 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->tile_task[1], &ctx->tile_begin[0], &ctx->tile_begin[1], &ctx->tile_hist,
                      &ctx->tile_lt, &ctx->dec, &ctx->medium, &ctx->small, &ctx->nodes, &ctx->lens,
                      &ctx->used, &ctx->newidx, &ctx->widened, &ctx->perm, &ctx->ctr, &ctx->cub_tmp, &ctx->in_a,
-                     &ctx->in_b, &ctx->out_nodes, &ctx->out_lens};
+                     &ctx->in_b, &ctx->out_nodes, &ctx->out_lens, &ctx->mesh_buf,
+                     &ctx->toff_buf, &ctx->noff_buf, &ctx->mkeys};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
@@ -1815,6 +2226,28 @@ int mgbvh_build_aabbs_dev(mgbvh_ctx* ctx, const float* d_aabbs, uint32_t count,
     if (count && !d_aabbs) return fail(ctx, MGBVH_ERR_INVALID_ARG, "aabbs pointer is NULL");
     return build_common(ctx, make_aabbs(d_aabbs, count), settings, d_out_nodes, node_capacity,
                         out_node_count, d_out_lens, d_out_perm, out_stats);
+}
+
+int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t mesh_count,
+                          const mgbvh_settings* settings, mgbvh_node* d_out_nodes,
+                          uint32_t node_capacity, uint32_t* d_out_lens, uint32_t* d_out_perm,
+                          uint32_t* out_node_offsets, mgbvh_stats* out_stats) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if ((rc = validate_settings(ctx, settings)) != MGBVH_OK) return rc;
+    if ((mesh_count && !meshes) || !out_node_offsets)
+        return fail(ctx, MGBVH_ERR_INVALID_ARG, "meshes / out_node_offsets is NULL");
+    if (!d_out_nodes || !d_out_perm) return fail(ctx, MGBVH_ERR_INVALID_ARG, "output pointer is NULL");
+    return run_batch(ctx, meshes, mesh_count, settings, d_out_nodes, node_capacity, d_out_lens,
+                     d_out_perm, out_node_offsets, out_stats);
+}
+
+int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (medium_max < kSmallMax + 1 || medium_max > kMediumMax)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "medium_max must be 33..1024");
+    ctx->medium_max = medium_max;
+    return MGBVH_OK;
 }
 
 int mgbvh_encode_gpu_bytes(const mgbvh_node* nodes, const uint32_t* lens, uint32_t count,
@@ -1917,6 +2350,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
     P.bins = st->bins;
     P.adaptive_max_n = st->adaptive_max_n;
     P.adaptive_steps = st->adaptive_steps;
+    P.medium_max = kMediumMax;
     Out O;
     O.nodes = S->nodes;
     O.lens = S->lens;

@@ -28,6 +28,7 @@ struct Params {
     uint32_t bins;            // 0: len.clamp(16,32)
     uint32_t adaptive_max_n;  // adaptive sweep for len <= this (<= 32)
     uint32_t adaptive_steps;  // 0: len.clamp(8,32)
+    uint32_t medium_max;      // nodes above this go through the level passes (<= 1024)
 };
 
 // Device counters and flags of one build.
@@ -278,8 +279,9 @@ __device__ __forceinline__ void warp_stable_permute(bool in_seg, bool pred, uint
 // object i of the node's range (starting at global position `base`).
 // Writes every node of the subtree and the permutation entries of its range.
 __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32_t n0, uint32_t base,
-                                   uint32_t slot0, uint32_t pair0, uint32_t depth0,
-                                   const float* bounds0, const Params& P, const Out& O, XRec* xchg) {
+                                   uint32_t slot0, uint32_t pair0, uint32_t depth0, uint32_t nbase,
+                                   uint32_t tbase, const float* bounds0, const Params& P, const Out& O,
+                                   XRec* xchg) {
     const uint32_t lane = threadIdx.x & 31u;
     // Pending-node stack, entry k held by lane k.
     uint32_t st_sn = 0, st_slot = 0, st_pair = 0, st_depth = 0;
@@ -475,7 +477,7 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
         }
 
         if (leaf) {
-            warp_store_node(O, slot, nb, base + s, n, 0u, lane);
+            warp_store_node(O, nbase + slot, nb, base + s - tbase, n, 0u, lane);
             if (in_seg) O.perm[base + lane] = id;
             if (n > 1u) {
                 n_holes++;
@@ -502,7 +504,7 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
         // containment of centroids in child bounds (bvh/src/lib.rs:637-646)
         const bool ok = !in_seg || box_contains(pred ? win.lt : win.gt, c[0], c[1], c[2]);
         if (__ballot_sync(kFull, !ok)) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
-        warp_store_node(O, slot, nb, base + s, n, pair, lane);
+        warp_store_node(O, nbase + slot, nb, base + s - tbase, n, pair, lane);
         if (!median) warp_stable_permute(in_seg, pred, s, n_lt, lane, lo, hi, id, xchg);
 
         any_split = true;
@@ -615,8 +617,9 @@ __device__ __forceinline__ void warp_exchange(uint32_t dst, uint32_t lane, float
 // centroid per object below 8; bvh/src/lib.rs:417-437).
 __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id, uint32_t n0,
                                           uint32_t base, uint32_t slot0, uint32_t pair0,
-                                          uint32_t depth0, const float* bounds0, const Params& P,
-                                          const Out& O, XRec* xchg) {
+                                          uint32_t depth0, uint32_t nbase, uint32_t tbase,
+                                          const float* bounds0, const Params& P, const Out& O,
+                                          XRec* xchg) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t below = (1u << lane) - 1u;
     uint32_t s = 0, n = n0, slot = slot0, pair = pair0, depth = depth0;
@@ -787,7 +790,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         // leaves of this level
         if (live && leaf) {
             if (leader) {
-                lane_store_node(O, slot, nb, base + s, n, 0u);
+                lane_store_node(O, nbase + slot, nb, base + s - tbase, n, 0u);
                 if (n > 1u) {
                     n_holes++;
                     if (depth == P.max_depth) n_capped++;
@@ -807,7 +810,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         const bool ok = !split || box_contains(pred ? win.lt : win.gt, c[0], c[1], c[2]);
         if (__any_sync(kFull, !ok) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
         if (split && leader) {
-            lane_store_node(O, slot, nb, base + s, n, pair);
+            lane_store_node(O, nbase + slot, nb, base + s - tbase, n, pair);
             any_split = true;
             hmax = max(hmax, depth);
         }
@@ -846,18 +849,6 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         if (hol) atomicAdd(&O.ctr->holes, hol);
         if (cap) atomicAdd(&O.ctr->depth_capped, cap);
     }
-}
-
-// Subtree of <= 32 objects: the level-synchronous form when every node in it
-// is an adaptive node with one threshold per object, else depth first.
-__device__ __forceinline__ void warp_build(float lo[3], float hi[3], uint32_t id, uint32_t n0,
-                                           uint32_t base, uint32_t slot0, uint32_t pair0,
-                                           uint32_t depth0, const float* bounds0, const Params& P,
-                                           const Out& O, XRec* xchg) {
-    if (P.adaptive_steps == 0 && n0 <= P.adaptive_max_n)
-        warp_build_subtree_levels(lo, hi, id, n0, base, slot0, pair0, depth0, bounds0, P, O, xchg);
-    else
-        warp_build_subtree(lo, hi, id, n0, base, slot0, pair0, depth0, bounds0, P, O, xchg);
 }
 
 }  // namespace mgbvh

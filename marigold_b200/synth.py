@@ -6,7 +6,9 @@ same seed gives the same f32 data on every host. Only IEEE-exact float64
 operations are used (add, multiply, divide, sqrt, floor); sine and cosine are
 evaluated by a fixed Taylor polynomial, so no platform libm enters the data.
 Negative zeros are canonicalised to +0.0, as the builder's min/max semantics
-leave the sign of a zero unspecified.
+leave the sign of a zero unspecified. (The mixed scene's Gaussian blobs use
+numpy's log for the Box-Muller transform; its data is generated where it is
+used and never pinned by a committed hash.)
 
 Vertices use marigold's 32-byte MeshVertex layout (position xyz, uv_x,
 normal xyz, uv_y; mesh_interface/src/lib.rs:6-12) with zero normals and uvs.
@@ -275,3 +277,62 @@ def rays_in_box(n: int, lo, hi, seed: int = 6, expand: float = 0.1):
     r[:, 0:3] = _f32(o)
     r[:, 4:7] = _f32(d)
     return r
+
+
+def quaternion_matrix(q):
+    """3x3 rotation matrices of unit quaternions q [n, 4] (x, y, z, w)."""
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
+
+
+def instance_aabbs(mesh_bounds: np.ndarray, mesh_ids, rot, scale, trans) -> np.ndarray:
+    """World AABB of each instance: min/max over the 8 corners of its mesh's
+    bounds under x -> R (s x) + t (marigold/src/app/data/scene/model.rs:191-234)."""
+    b = mesh_bounds[mesh_ids]  # [n, 6]
+    corners = np.stack([np.stack([b[:, 3 * (i >> 2 & 1)], b[:, 1 + 3 * (i >> 1 & 1)],
+                                  b[:, 2 + 3 * (i & 1)]], -1) for i in range(8)], 1)  # [n, 8, 3]
+    w = np.einsum("nij,nkj->nki", rot, corners * scale[:, None, None]) + trans[:, None, :]
+    return _f32(np.concatenate([w.min(axis=1), w.max(axis=1)], axis=1))
+
+
+def batched_scene(seed: int = 3, n_meshes: int = 512, n_instances: int = 4096,
+                  lo: int = 64, hi: int = 262144):
+    """Many meshes plus instances: triangle counts log-uniform in [lo, hi];
+    each mesh is random small triangles or a noisy icosphere (coin flip; the
+    icosphere is subdivided to the first level with enough faces and trimmed);
+    instances pick a mesh uniformly, a random rotation (normalised 4-D
+    Gaussian quaternion), a uniform scale in [0.5, 2] and a translation uniform
+    in [-100, 100]^3. Returns (meshes, bounds [M, 6], instance AABBs [I, 6])
+    with meshes a list of (vertices float32 [V, 8], triangles uint32 [N, 3])."""
+    m = np.arange(n_meshes, dtype=np.uint32)
+    counts = np.rint(np.exp(np.log(lo) + (np.log(hi) - np.log(lo)) * uniform(seed, 1, m))).astype(np.int64)
+    kind = uniform(seed, 2, m) < 0.5
+    ico_cache = {}
+    meshes = []
+    for i in range(n_meshes):
+        n = int(counts[i])
+        if kind[i]:
+            v, t = random_triangles(n, seed=10000 + i)
+        else:
+            level = 0
+            while 20 * 4 ** level < n:
+                level += 1
+            if level not in ico_cache:
+                ico_cache[level] = icosphere(level)
+            p, f = ico_cache[level]
+            r = 1.0 + 0.05 * value_noise(p, 20000 + i)
+            v = pack_vertices(p * r[:, None])
+            t = f[:n].astype(np.uint32)
+        meshes.append((v, np.ascontiguousarray(t, dtype=np.uint32)))
+    bounds = np.stack([mesh_bounds(v) for v, _ in meshes])
+    j = np.arange(n_instances, dtype=np.uint32)
+    ids = np.minimum((uniform(seed, 3, j) * n_meshes).astype(np.int64), n_meshes - 1)
+    q = np.stack([gaussian(seed, 10 + 2 * k, j) for k in range(4)], -1)
+    q = q / np.sqrt((q * q).sum(axis=1, keepdims=True))
+    scale = 0.5 + 1.5 * uniform(seed, 20, j)
+    trans = np.stack([uniform(seed, 21 + k, j) * 200.0 - 100.0 for k in range(3)], -1)
+    inst = instance_aabbs(bounds.astype(np.float64), ids, quaternion_matrix(q), scale, trans)
+    return meshes, bounds, inst
