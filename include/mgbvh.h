@@ -122,10 +122,12 @@ typedef struct mgbvh_stats {
     uint32_t depth_capped_leaves; /* leaves made by depth == max_depth with len > 1 */
     uint32_t feasible;            /* the crate's feasibility flag */
     uint32_t kernel_launches;     /* builder kernels launched by this build */
-    uint32_t levels;              /* level-synchronous passes over nodes above 1024 objects */
+    uint32_t levels;              /* level-synchronous passes over the largest nodes */
     /* device seconds per phase: [0] object records + root, [1] level passes,
        [2] subtrees of 33..1024 objects, [3] subtrees of <= 32 objects */
     double phase_seconds[4];
+    uint32_t graph_replay;        /* 1: a batched build replayed its captured CUDA graph */
+    uint32_t reserved;
 } mgbvh_stats;
 
 typedef struct mgbvh_ctx mgbvh_ctx;
@@ -222,6 +224,12 @@ MGBVH_API int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshe
                                     mgbvh_node* d_out_nodes, uint32_t node_capacity,
                                     uint32_t* d_out_lens, uint32_t* d_out_perm,
                                     uint32_t* out_node_offsets, mgbvh_stats* out_stats);
+
+/* Batched builds on this context capture their launch sequence in a CUDA
+   graph and replay it when the same mesh set (pointers, counts, settings,
+   outputs, stream) is built again; a tree deeper than the captured one falls
+   back to a regular build. Off by default. */
+MGBVH_API int mgbvh_set_graph_capture(mgbvh_ctx* ctx, int enable);
 
 /* Speed knob of a context, no effect on the trees: nodes with more than
    medium_max objects (33..1024, default 1024) go through the level passes,

@@ -32,7 +32,7 @@ EXPORTED = (
     "mgbvh_build_indexed_dev", "mgbvh_build_aabbs_dev", "mgbvh_encode_gpu_bytes",
     "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc", "mgbvh_tracer_create", "mgbvh_tracer_destroy",
     "mgbvh_tracer_set_blas_dev", "mgbvh_trace_closest_dev", "mgbvh_trace_bruteforce_dev",
-    "mgbvh_build_batch_dev", "mgbvh_set_tuning",
+    "mgbvh_build_batch_dev", "mgbvh_set_tuning", "mgbvh_set_graph_capture",
 )
 
 
@@ -75,6 +75,8 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint32),
         ("levels", ctypes.c_uint32),
         ("phase_seconds", ctypes.c_double * 4),
+        ("graph_replay", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
     def as_dict(self):
@@ -164,6 +166,8 @@ def load():
         L.mgbvh_build_batch_dev.argtypes = [P, ctypes.POINTER(MeshDesc), u32, ctypes.POINTER(Settings),
                                             P, u32, P, P, pu32, ctypes.POINTER(Stats)]
         L.mgbvh_build_batch_dev.restype = ctypes.c_int
+        L.mgbvh_set_graph_capture.argtypes = [P, ctypes.c_int]
+        L.mgbvh_set_graph_capture.restype = ctypes.c_int
         L.mgbvh_set_tuning.argtypes = [P, u32]
         L.mgbvh_set_tuning.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]

@@ -1408,6 +1408,12 @@ struct mgbvh_ctx {
     DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
     DevBuf in_a, in_b, out_nodes, out_lens;
     DevBuf mesh_buf, toff_buf, noff_buf, mkeys;
+    void* pin = nullptr;  // pinned staging of a batch plan
+    size_t pin_bytes = 0;
+    bool graph_mode = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<unsigned char> graph_sig;
+    uint32_t graph_levels = 0, graph_launches = 0;
     Counters* h_ctr = nullptr;
 };
 
@@ -1503,8 +1509,11 @@ const char* site_text(uint32_t site) {
 
 // Level passes (nodes above medium_max), then the medium and small subtree
 // kernels, on the context's stream. Root tasks are already queued.
+// fixed_levels > 0: launch exactly that many level passes and never read
+// back (the form a CUDA graph captures); 0: read the next level's count at
+// the end of each batch of levels.
 int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, Rec* rec0, Rec* rec1,
-                 bool has_large, uint32_t& launches, uint32_t& levels) {
+                 bool has_large, uint32_t fixed_levels, uint32_t& launches, uint32_t& levels) {
     const cudaStream_t sm = ctx->stream;
     Counters* d_ctr = O.ctr;
     // Level passes over the large nodes. Kernels read their task and tile
@@ -1514,10 +1523,11 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     const int eval_grid = (int)std::min<uint32_t>((C.tasks + 3) / 4, (uint32_t)ctx->sm_count * 4u);
     uint32_t level = 0;
     bool more = has_large;
-    ctx->h_ctr->error = 0;
+    if (!fixed_levels) ctx->h_ctr->error = 0;
     bool first_batch = true;
     while (more) {
-        const uint32_t batch = first_batch ? std::max(ctx->levels_hint, 4u) : 2u;
+        const uint32_t batch =
+            fixed_levels ? fixed_levels : (first_batch ? std::max(ctx->levels_hint, 4u) : 2u);
         first_batch = false;
         for (uint32_t bl = 0; bl < batch; ++bl, ++level) {
             const uint32_t lv = level & 1u, nx = lv ^ 1u;
@@ -1553,23 +1563,24 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
         }
         MG_CUDA(cudaGetLastError());
+        if (fixed_levels) break;
         MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
         MG_CUDA(cudaStreamSynchronize(sm));
         if (ctx->h_ctr->error) break;
         more = ctx->h_ctr->lvl[level & 1u][0] > 0;
     }
     if (has_large) {
-        ctx->levels_hint = level;
+        if (!fixed_levels) ctx->levels_hint = level;
         levels = level;
     }
-    MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
-    if (!ctx->h_ctr->error) {
+    if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
+    if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
         const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
         medium_kernel<<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
             P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O);
         launches++;
-        MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
+        if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
         // small subtrees: count read on the device; grid sized for full occupancy
         if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
             small_kernel<true><<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
@@ -1666,7 +1677,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     uint32_t launches = 2, levels = 0;
     (void)ntiles0;
 
-    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, cls == 3, launches, levels)) != MGBVH_OK)
+    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, cls == 3, 0, launches, levels)) != MGBVH_OK)
         return rc;
     MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
@@ -1778,19 +1789,32 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
 
 
 // Batched build over several meshes (see include/mgbvh.h).
-int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const mgbvh_settings* st,
-              mgbvh_node* d_nodes, uint32_t cap, uint32_t* d_lens, uint32_t* d_perm,
-              uint32_t* out_offsets, mgbvh_stats* stats) {
-    const cudaStream_t sm = ctx->stream;
-    int rc;
-    // offsets and the root plan
-    std::vector<DevMesh> hm(nm);
-    std::vector<uint32_t> toffs(nm + 1), noffs(nm + 1);
+//
+// Plan (host): object and node offsets of every mesh, each root's list and
+// tiles. Device work (enqueue_batch): inputs of the plan copied from pinned
+// staging, record prep, roots, the pipeline, and either a read-back per
+// batch of levels (eager) or a fixed number of levels and the copy of the
+// results to the caller (graph capture). With graph capture on, the first
+// build of a mesh set runs eagerly and learns its level count; later builds
+// of the same set (same pointers, counts and settings) replay one CUDA graph
+// of the whole batch with one spare level, and fall back to the eager path
+// if the spare level turns out to have work (a deeper tree).
+struct BatchPlan {
+    uint32_t nm = 0, n = 0, slots = 0, n_large = 0, n_medium = 0, n_small = 0, tiles = 0;
+    std::vector<DevMesh> hm;
+    std::vector<uint32_t> toffs, noffs;
+};
+
+int plan_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const mgbvh_settings* st,
+               BatchPlan& B) {
+    B.nm = nm;
+    B.hm.assign(nm, DevMesh());
+    B.toffs.assign(nm + 1, 0);
+    B.noffs.assign(nm + 1, 0);
     uint64_t total = 0, slots = 0;
-    uint32_t n_large = 0, n_medium = 0, n_small = 0, tiles = 0;
     for (uint32_t m = 0; m < nm; ++m) {
         const mgbvh_mesh_desc& d = meshes[m];
-        DevMesh& M = hm[m];
+        DevMesh& M = B.hm[m];
         std::memset(&M, 0, sizeof(M));
         const bool tri = d.vertices != nullptr;
         if (d.count && tri && (!d.triangles || d.vertex_stride_bytes < 12 || d.vertex_stride_bytes % 4))
@@ -1807,15 +1831,15 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         M.nbase = (uint32_t)slots;
         M.has_bounds = d.has_bounds;
         for (int i = 0; i < 6; ++i) M.bounds[i] = d.bounds[i];
-        toffs[m] = (uint32_t)total;
-        noffs[m] = (uint32_t)slots;
+        B.toffs[m] = (uint32_t)total;
+        B.noffs[m] = (uint32_t)slots;
         total += d.count;
         slots += d.count ? 2ull * d.count - 1 : 0;
         if (total > 0x7FFFFFFFull || slots > 0xFFFFFFFEull)
             return fail(ctx, MGBVH_ERR_UNSUPPORTED, "batch above 2^31-1 objects");
         const uint32_t n = d.count;
         if (n == 0) {
-            M.cls = 4;  // nothing to build
+            M.cls = 4;
             continue;
         }
         const bool leaf = n <= 1 || st->max_depth == 0 ||
@@ -1824,27 +1848,114 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
             M.cls = 0;
         } else if (n <= kSmallMax) {
             M.cls = 1;
-            M.list_index = n_small++;
+            M.list_index = B.n_small++;
         } else if (n <= ctx->medium_max) {
             M.cls = 2;
-            M.list_index = n_medium++;
+            M.list_index = B.n_medium++;
         } else {
             M.cls = 3;
-            M.list_index = n_large++;
-            M.tile0 = tiles;
+            M.list_index = B.n_large++;
+            M.tile0 = B.tiles;
             M.ntiles = (n + kTile - 1) / kTile;
-            tiles += M.ntiles;
+            B.tiles += M.ntiles;
         }
     }
-    toffs[nm] = (uint32_t)total;
-    noffs[nm] = (uint32_t)slots;
-    if (total == 0) {
+    B.toffs[nm] = (uint32_t)total;
+    B.noffs[nm] = (uint32_t)slots;
+    B.n = (uint32_t)total;
+    B.slots = (uint32_t)slots;
+    return MGBVH_OK;
+}
+
+Params params_of(const mgbvh_ctx* ctx, const mgbvh_settings* st) {
+    Params P;
+    P.min_leaf = st->min_leaf_objects;
+    P.max_leaf = st->max_leaf_objects;
+    P.max_depth = st->max_depth;
+    P.bins = st->bins;
+    P.adaptive_max_n = st->adaptive_max_n;
+    P.adaptive_steps = st->adaptive_steps;
+    P.medium_max = ctx->medium_max;
+    return P;
+}
+
+// Device work of a batch on the context's stream. fixed_levels == 0: eager
+// (reads level counts back); > 0: capture form, which also copies the slot
+// array to the caller's outputs and the counters to pinned host memory.
+int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh_settings* st,
+                  uint32_t fixed_levels, mgbvh_node* d_nodes, uint32_t* d_lens, uint32_t* d_perm,
+                  uint32_t& launches, uint32_t& levels) {
+    const cudaStream_t sm = ctx->stream;
+    const uint32_t nm = B.nm, n = B.n;
+    const Params P = params_of(ctx, st);
+    // pinned staging: counters, mesh records, object offsets, node offsets
+    unsigned char* pin = static_cast<unsigned char*>(ctx->pin);
+    Counters* h_init = reinterpret_cast<Counters*>(pin);
+    DevMesh* h_mesh = reinterpret_cast<DevMesh*>(pin + sizeof(Counters));
+    uint32_t* h_toffs = reinterpret_cast<uint32_t*>(h_mesh + nm);
+    uint32_t* h_noffs = h_toffs + (nm + 1);
+    Counters* d_ctr = P_<Counters>(ctx->ctr);
+    MG_CUDA(cudaMemcpyAsync(d_ctr, h_init, sizeof(Counters), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->mesh_buf.p, h_mesh, sizeof(DevMesh) * (size_t)nm,
+                            cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->toff_buf.p, h_toffs, 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemcpyAsync(ctx->noff_buf.p, h_noffs, 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
+    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
+    Out O;
+    O.nodes = P_<mgbvh_node>(ctx->nodes);
+    O.lens = P_<uint32_t>(ctx->lens);
+    O.used = P_<uint8_t>(ctx->used);
+    O.perm = d_perm;
+    O.ctr = d_ctr;
+    O.node_cap = C.nodes;
+    Rec* rec0 = P_<Rec>(ctx->rec[0]);
+    Rec* rec1 = P_<Rec>(ctx->rec[1]);
+    const DevMesh* dmesh = P_<DevMesh>(ctx->mesh_buf);
+    // timing events are recorded outside a captured graph (around its launch)
+    if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->ev0, sm));
+    init_mkeys_kernel<<<std::max(1u, std::min((12 * nm + 255) / 256, 1024u)), 256, 0, sm>>>(
+        P_<uint32_t>(ctx->mkeys), nm);
+    prep_batch_kernel<<<(int)std::min<uint32_t>((n + 255) / 256, 148u * 8u), 256, 0, sm>>>(
+        dmesh, P_<uint32_t>(ctx->toff_buf), nm, n, rec0, P_<uint32_t>(ctx->mkeys), d_ctr);
+    init_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
+        dmesh, nm, P_<uint32_t>(ctx->mkeys), P_<Task>(ctx->tasks[0]), P_<uint32_t>(ctx->bins[0]),
+        P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]), P_<uint32_t>(ctx->tile_begin[0]),
+        P_<Task>(ctx->medium), P_<Task>(ctx->small), O, st->max_depth);
+    MG_CUDA(cudaGetLastError());
+    if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+    launches = 3;
+    levels = 0;
+    int rc = run_pipeline(ctx, C, P, O, rec0, rec1, B.n_large > 0, fixed_levels, launches, levels);
+    if (rc != MGBVH_OK) return rc;
+    if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+    if (fixed_levels) {
+        MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)B.slots,
+                                cudaMemcpyDeviceToDevice, sm));
+        if (d_lens)
+            MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * B.slots, cudaMemcpyDeviceToDevice, sm));
+    }
+    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+    return MGBVH_OK;
+}
+
+bool same_signature(const mgbvh_ctx* ctx, const std::vector<unsigned char>& sig) {
+    return ctx->graph_exec && ctx->graph_sig == sig;
+}
+
+int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const mgbvh_settings* st,
+              mgbvh_node* d_nodes, uint32_t cap, uint32_t* d_lens, uint32_t* d_perm,
+              uint32_t* out_offsets, mgbvh_stats* stats) {
+    const cudaStream_t sm = ctx->stream;
+    int rc;
+    BatchPlan B;
+    if ((rc = plan_batch(ctx, meshes, nm, st, B)) != MGBVH_OK) return rc;
+    if (B.n == 0) {
         for (uint32_t m = 0; m <= nm; ++m) out_offsets[m] = 0;
         if (stats) std::memset(stats, 0, sizeof(*stats));
         return MGBVH_WARN_EMPTY;
     }
-    const uint32_t n = (uint32_t)total;
-    const Caps C = caps_for(n, ctx->medium_max, nm, (uint32_t)slots);
+    const uint32_t n = B.n;
+    const Caps C = caps_for(n, ctx->medium_max, nm, B.slots);
 #define ENS(buf, bytes) \
     if ((rc = ensure(ctx, buf, (bytes))) != MGBVH_OK) return rc
     ENS(ctx->rec[0], sizeof(Rec) * (size_t)n);
@@ -1870,61 +1981,84 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     ENS(ctx->noff_buf, 4ull * (nm + 1));
     ENS(ctx->mkeys, 48ull * nm);
 #undef ENS
-    if (n_large > C.tasks || tiles > C.tiles || n_medium > C.medium || n_small > C.small)
+    if (B.n_large > C.tasks || B.tiles > C.tiles || B.n_medium > C.medium || B.n_small > C.small)
         return fail(ctx, MGBVH_ERR_CAPACITY, "batch root lists exceed their capacity");
-    Params P;
-    P.min_leaf = st->min_leaf_objects;
-    P.max_leaf = st->max_leaf_objects;
-    P.max_depth = st->max_depth;
-    P.bins = st->bins;
-    P.adaptive_max_n = st->adaptive_max_n;
-    P.adaptive_steps = st->adaptive_steps;
-    P.medium_max = ctx->medium_max;
-    Counters init;
-    std::memset(&init, 0, sizeof(init));
-    init.lvl[0][0] = n_large;
-    init.lvl[0][1] = tiles;
-    init.n_medium = n_medium;
-    init.n_small = n_small;
-    Counters* d_ctr = P_<Counters>(ctx->ctr);
-    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
-    MG_CUDA(cudaMemcpyAsync(ctx->mesh_buf.p, hm.data(), sizeof(DevMesh) * (size_t)nm,
-                            cudaMemcpyHostToDevice, sm));
-    MG_CUDA(cudaMemcpyAsync(ctx->toff_buf.p, toffs.data(), 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
-    MG_CUDA(cudaMemcpyAsync(ctx->noff_buf.p, noffs.data(), 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
-    MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
-    Out O;
-    O.nodes = P_<mgbvh_node>(ctx->nodes);
-    O.lens = P_<uint32_t>(ctx->lens);
-    O.used = P_<uint8_t>(ctx->used);
-    O.perm = d_perm;
-    O.ctr = d_ctr;
-    O.node_cap = C.nodes;
-    Rec* rec0 = P_<Rec>(ctx->rec[0]);
-    Rec* rec1 = P_<Rec>(ctx->rec[1]);
-    const DevMesh* dmesh = P_<DevMesh>(ctx->mesh_buf);
-    MG_CUDA(cudaEventRecord(ctx->ev0, sm));
-    init_mkeys_kernel<<<std::max(1u, std::min((12 * nm + 255) / 256, 1024u)), 256, 0, sm>>>(
-        P_<uint32_t>(ctx->mkeys), nm);
-    prep_batch_kernel<<<(int)std::min<uint32_t>((n + 255) / 256, 148u * 8u), 256, 0, sm>>>(
-        dmesh, P_<uint32_t>(ctx->toff_buf), nm, n, rec0, P_<uint32_t>(ctx->mkeys), d_ctr);
-    init_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
-        dmesh, nm, P_<uint32_t>(ctx->mkeys), P_<Task>(ctx->tasks[0]), P_<uint32_t>(ctx->bins[0]),
-        P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]), P_<uint32_t>(ctx->tile_begin[0]),
-        P_<Task>(ctx->medium), P_<Task>(ctx->small), O, st->max_depth);
-    MG_CUDA(cudaGetLastError());
-    MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
-    uint32_t launches = 4, levels = 0;
-    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, n_large > 0, launches, levels)) != MGBVH_OK)
-        return rc;
-    MG_CUDA(cudaEventRecord(ctx->ev1, sm));
-    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
-    MG_CUDA(cudaStreamSynchronize(sm));
+    // pinned staging of the plan
+    const size_t pin_bytes = sizeof(Counters) + sizeof(DevMesh) * (size_t)nm + 8ull * (nm + 1);
+    if (ctx->pin_bytes < pin_bytes) {
+        // a graph captured against the old staging must not be replayed
+        if (ctx->graph_exec) {
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+            ctx->graph_sig.clear();
+        }
+        if (ctx->pin) cudaFreeHost(ctx->pin);
+        ctx->pin = nullptr;
+        ctx->pin_bytes = 0;
+        MG_CUDA(cudaMallocHost(&ctx->pin, pin_bytes));
+        ctx->pin_bytes = pin_bytes;
+    }
+    {
+        unsigned char* pin = static_cast<unsigned char*>(ctx->pin);
+        Counters init;
+        std::memset(&init, 0, sizeof(init));
+        init.lvl[0][0] = B.n_large;
+        init.lvl[0][1] = B.tiles;
+        init.n_medium = B.n_medium;
+        init.n_small = B.n_small;
+        std::memcpy(pin, &init, sizeof(init));
+        std::memcpy(pin + sizeof(Counters), B.hm.data(), sizeof(DevMesh) * (size_t)nm);
+        uint32_t* t = reinterpret_cast<uint32_t*>(pin + sizeof(Counters) + sizeof(DevMesh) * (size_t)nm);
+        std::memcpy(t, B.toffs.data(), 4ull * (nm + 1));
+        std::memcpy(t + nm + 1, B.noffs.data(), 4ull * (nm + 1));
+    }
+    // signature of everything a captured graph bakes in
+    std::vector<unsigned char> sig;
+    if (ctx->graph_mode) {
+        auto put = [&](const void* p, size_t k) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            sig.insert(sig.end(), c, c + k);
+        };
+        put(meshes, sizeof(mgbvh_mesh_desc) * (size_t)nm);
+        put(st, sizeof(*st));
+        put(&ctx->medium_max, 4);
+        put(&d_nodes, sizeof(d_nodes));
+        put(&d_lens, sizeof(d_lens));
+        put(&d_perm, sizeof(d_perm));
+        put(&cap, 4);
+        put(&ctx->stream, sizeof(ctx->stream));
+    }
+    uint32_t launches = 0, levels = 0;
+    bool done = false;
+    bool from_graph = false;
+    if (ctx->graph_mode && same_signature(ctx, sig)) {
+        MG_CUDA(cudaEventRecord(ctx->ev0, sm));
+        MG_CUDA(cudaGraphLaunch(ctx->graph_exec, sm));
+        MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        const Counters& hc = *ctx->h_ctr;
+        // the spare level must have found nothing to do
+        if (!hc.error && hc.lvl[ctx->graph_levels & 1u][0] == 0) {
+            done = true;
+            from_graph = true;
+            launches = ctx->graph_launches;
+            levels = ctx->graph_levels;
+        }
+    }
+    if (!done) {
+        if ((rc = enqueue_batch(ctx, B, C, st, 0, d_nodes, d_lens, d_perm, launches, levels)) != MGBVH_OK)
+            return rc;
+        MG_CUDA(cudaStreamSynchronize(sm));
+    }
     const Counters hc = *ctx->h_ctr;
     if (hc.error) return fail(ctx, (int)hc.error, site_text(hc.error_site));
     float ms = 0.0f;
-    MG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-    uint32_t count = (uint32_t)slots;
+    if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) {
+        ms = 0.0f;
+        cudaGetLastError();
+    }
+    const std::vector<uint32_t>& noffs = B.noffs;
+    uint32_t count = B.slots;
     if (hc.holes > 0) {
         if ((rc = ensure(ctx, ctx->newidx, 4ull * C.nodes)) != MGBVH_OK) return rc;
         if ((rc = ensure(ctx, ctx->widened, 4ull * C.nodes)) != MGBVH_OK) return rc;
@@ -1953,12 +2087,43 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     } else {
         if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the trees");
         for (uint32_t m = 0; m <= nm; ++m) out_offsets[m] = noffs[m];
-        MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
-                                cudaMemcpyDeviceToDevice, sm));
-        if (d_lens)
-            MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * count, cudaMemcpyDeviceToDevice, sm));
+        if (!from_graph) {
+            MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
+                                    cudaMemcpyDeviceToDevice, sm));
+            if (d_lens)
+                MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * count, cudaMemcpyDeviceToDevice, sm));
+        }
     }
     MG_CUDA(cudaStreamSynchronize(sm));
+    // capture a graph for the next build of this mesh set
+    if (ctx->graph_mode && !from_graph && hc.holes == 0 && cap >= B.slots) {
+        if (ctx->graph_exec) {
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+        }
+        ctx->graph_sig.clear();
+        cudaGraph_t g = nullptr;
+        uint32_t gl = 0, glev = 0;
+        const uint32_t fixed = (B.n_large > 0 ? levels : 0) + 1;
+        // (capture is not possible on the legacy default stream: then no graph)
+        if (cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            cudaGetLastError();
+        } else {
+        const int erc = enqueue_batch(ctx, B, C, st, fixed, d_nodes, d_lens, d_perm, gl, glev);
+        const cudaError_t ce = cudaStreamEndCapture(sm, &g);
+        if (erc == MGBVH_OK && ce == cudaSuccess && g) {
+            if (cudaGraphInstantiate(&ctx->graph_exec, g, 0) == cudaSuccess) {
+                ctx->graph_sig = sig;
+                ctx->graph_levels = fixed;
+                ctx->graph_launches = gl;
+            } else {
+                ctx->graph_exec = nullptr;
+            }
+        }
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        }
+    }
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
         stats->construction_time = ms * 1e-3;
@@ -1973,11 +2138,15 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         const uint32_t MIN = st->min_leaf_objects, MAX = st->max_leaf_objects;
         stats->feasible = MIN == MAX ? 1u : (MAX >= 2 * MIN - 1);
         float pm[4] = {0.f, 0.f, 0.f, 0.f};
-        cudaEventElapsedTime(&pm[0], ctx->ev0, ctx->evp[0]);
-        cudaEventElapsedTime(&pm[1], ctx->evp[0], ctx->evp[1]);
-        cudaEventElapsedTime(&pm[2], ctx->evp[1], ctx->evp[2]);
-        cudaEventElapsedTime(&pm[3], ctx->evp[2], ctx->ev1);
+        if (!from_graph) {  // phases are not timed inside a graph
+            cudaEventElapsedTime(&pm[0], ctx->ev0, ctx->evp[0]);
+            cudaEventElapsedTime(&pm[1], ctx->evp[0], ctx->evp[1]);
+            cudaEventElapsedTime(&pm[2], ctx->evp[1], ctx->evp[2]);
+            cudaEventElapsedTime(&pm[3], ctx->evp[2], ctx->ev1);
+            cudaGetLastError();
+        }
         for (int i = 0; i < 4; ++i) stats->phase_seconds[i] = pm[i] * 1e-3;
+        stats->graph_replay = from_graph ? 1u : 0u;
     }
     return MGBVH_OK;
 }
@@ -2141,6 +2310,8 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+    if (ctx->pin) cudaFreeHost(ctx->pin);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (cudaEvent_t e : ctx->evp)
@@ -2240,6 +2411,18 @@ int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_
     if (!d_out_nodes || !d_out_perm) return fail(ctx, MGBVH_ERR_INVALID_ARG, "output pointer is NULL");
     return run_batch(ctx, meshes, mesh_count, settings, d_out_nodes, node_capacity, d_out_lens,
                      d_out_perm, out_node_offsets, out_stats);
+}
+
+int mgbvh_set_graph_capture(mgbvh_ctx* ctx, int enable) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    ctx->graph_mode = enable != 0;
+    if (!ctx->graph_mode && ctx->graph_exec) {
+        cudaSetDevice(ctx->device);
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_sig.clear();
+    }
+    return MGBVH_OK;
 }
 
 int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max) {

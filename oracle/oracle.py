@@ -43,6 +43,8 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint32),
         ("levels", ctypes.c_uint32),
         ("phase_seconds", ctypes.c_double * 4),
+        ("graph_replay", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
     def as_dict(self):

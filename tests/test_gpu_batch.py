@@ -117,3 +117,36 @@ def test_batch_meshes_match_oracle():
     msg = compare_exact(nodes[offs[k]:offs[k + 1]], lens[offs[k]:offs[k + 1]],
                         perm[first:first + inst.shape[0]], o["nodes"], o["lens"], o["perm"])
     assert msg is None, f"tlas: {msg}"
+
+
+def test_graph_replay_equals_eager_build():
+    import torch
+    meshes, bounds, inst = scene(n_meshes=24, n_inst=200, hi=60000, seed=12)
+    ctx = _lib.Context(0)
+    ctx.check(ctx.L.mgbvh_set_graph_capture(ctx.ptr, 1))
+    stream = torch.cuda.Stream()  # capture needs a stream other than the legacy default
+    descs = [{"vertices": torch.from_numpy(v).cuda(), "triangles": torch.from_numpy(t.view(np.int32)).cuda(),
+              "bounds": b if t.shape[0] else None} for (v, t), b in zip(meshes, bounds)]
+    descs.append({"aabbs": torch.from_numpy(inst).cuda()})
+    total = sum(t.shape[0] for _, t in meshes) + inst.shape[0]
+    slots = sum(2 * t.shape[0] - 1 for _, t in meshes if t.shape[0]) + 2 * inst.shape[0] - 1
+    nodes = torch.zeros(slots * 8, dtype=torch.int32, device="cuda")
+    lens = torch.zeros(slots, dtype=torch.int32, device="cuda")
+    perm = torch.zeros(total, dtype=torch.int32, device="cuda")
+    results = []
+    for k in range(3):
+        nodes.zero_()
+        perm.zero_()
+        torch.cuda.synchronize()
+        offs, rc, st = build_batch_device(ctx, BvhSettings(), descs, nodes, perm, out_lens=lens,
+                                          stream=stream)
+        stream.synchronize()
+        results.append((offs, st["graph_replay"], nodes.cpu().numpy().copy(),
+                        lens.cpu().numpy().copy(), perm.cpu().numpy().copy()))
+    assert results[0][1] == 0 and results[1][1] == 1 and results[2][1] == 1
+    for r in results[1:]:
+        assert r[0] == results[0][0]
+        msg = compare_exact(r[2].view(np.uint32).reshape(-1, 8), r[3], r[4],
+                            results[0][2].view(np.uint32).reshape(-1, 8), results[0][3], results[0][4])
+        assert msg is None, msg
+    ctx.close()
