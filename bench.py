@@ -53,7 +53,7 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="icosphere", choices=["icosphere", "mixed"],
+    p.add_argument("--workload", default="icosphere", choices=["icosphere", "mixed", "batched"],
                    help="icosphere: the headline build; mixed: 16.8M-triangle scene + 8M rays")
     p.add_argument("--mixed-scale", type=int, default=1,
                    help="divide the mixed scene and its ray count by this factor")
@@ -190,6 +190,9 @@ def run_ours(args):
     n = t.shape[0]
     settings = BvhSettings(name="bench", bounds=bounds, max_depth=32)
     ctx = _lib.Context(local)
+    from marigold_b200 import autotune
+    medium_max = autotune.choice("icosphere_l8", "medium_max", 1024)  # speed only; same tree
+    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
     dv = torch.from_numpy(v).cuda()
     dt = torch.from_numpy(t.view(np.int32)).cuda()
     cap = 2 * n - 1
@@ -470,9 +473,76 @@ def run_mixed(args):
     print(json.dumps(out), flush=True)
 
 
+def run_batched(args):
+    """The batched scene: 512 meshes with triangle counts log-uniform in
+    [64, 262144] (random small triangles or a trimmed noisy icosphere, coin
+    flip) plus the TLAS over 4,096 instances (random rotation, scale in
+    [0.5, 2], translation in [-100, 100]^3; instance AABBs from the 8 corners
+    of the mesh bounds), all 513 trees in one batched build. The first build
+    runs eagerly and captures a CUDA graph; timed builds replay the graph."""
+    import torch
+    from marigold_b200 import BvhSettings, _lib, autotune, build_batch_device, synth
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    meshes, bounds, inst = synth.batched_scene()
+    gen_s = time.perf_counter() - t0
+    medium_max = autotune.choice("batched_scene", "medium_max", 1024)
+    bins = autotune.choice("batched_scene", "bins", 0)
+    ctx = _lib.Context(0)
+    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
+    ctx.check(ctx.L.mgbvh_set_graph_capture(ctx.ptr, 1))
+    descs = [{"vertices": torch.from_numpy(v).cuda(), "triangles": torch.from_numpy(t.view(np.int32)).cuda(),
+              "bounds": b} for (v, t), b in zip(meshes, bounds)]
+    descs.append({"aabbs": torch.from_numpy(inst).cuda()})
+    n_tris = sum(t.shape[0] for _, t in meshes)
+    total = n_tris + inst.shape[0]
+    slots = sum(2 * t.shape[0] - 1 for _, t in meshes) + 2 * inst.shape[0] - 1
+    nodes = torch.empty(slots * 8, dtype=torch.int32, device="cuda")
+    lens = torch.empty(slots, dtype=torch.int32, device="cuda")
+    perm = torch.empty(total, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    settings = BvhSettings(bins=bins)
+    times, replays, eager_ms = [], 0, None
+    offs = None
+    for k in range(max(args.warmup, 2) + args.steps):
+        flush.fill_(k & 0xFF)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        offs, rc, st = build_batch_device(ctx, settings, descs, nodes, perm, out_lens=lens,
+                                          stream=stream)
+        e1.record(stream)
+        stream.synchronize()
+        if k == 0:
+            eager_ms = e0.elapsed_time(e1)
+        if k >= max(args.warmup, 2):
+            times.append(e0.elapsed_time(e1))
+            replays += st["graph_replay"]
+    from marigold_b200.bvh import NODE_DTYPE, sah_cost
+    nh = nodes.cpu().numpy().view(NODE_DTYPE)
+    lh = lens.cpu().numpy().view(np.uint32)
+    sah_blas = sum(sah_cost(nh[offs[i]:offs[i + 1]], lh[offs[i]:offs[i + 1]]) for i in range(len(meshes)))
+    sah_tlas = sah_cost(nh[offs[-2]:offs[-1]], lh[offs[-2]:offs[-1]])
+    ms = float(np.mean(times))
+    out = {
+        "metric": "BVH build Mtri/s (batched: 512 BLAS + TLAS)", "workload": "batched scene",
+        "value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms_per_step": round(ms, 3),
+        "eager_first_build_ms": round(eager_ms, 3), "graph_replays": replays, "steps": args.steps,
+        "config": {"meshes": len(meshes), "triangles": n_tris, "instances": int(inst.shape[0]),
+                   "trees": len(meshes) + 1, "nodes": int(offs[-1]), "medium_max": medium_max,
+                   "bins": bins or "reference (32)", "tuning": "marigold_b200/tuning.json"},
+        "sah": {"blas_sum": round(sah_blas, 3), "tlas": round(sah_tlas, 3)},
+        "generation_s": round(gen_s, 1), "l2": "flushed before every build",
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse_args()
-    if args.workload == "mixed":
+    if args.workload == "batched":
+        run_batched(args)
+    elif args.workload == "mixed":
         run_mixed(args)
     elif args.impl == "reference":
         run_reference(args)

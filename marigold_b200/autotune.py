@@ -1,0 +1,154 @@
+"""Autotuner of the builder's per-workload choices; writes tuning.json.
+
+Two knobs are tuned per workload:
+  * medium_max — the size at which nodes leave the level passes for the
+    per-subtree kernels (33..1024). Every phase computes the same split
+    decisions, so this knob changes speed only, never the tree: the fastest
+    value is always taken.
+  * bins — the binned-sweep bin count. The reference profile (bins = 0,
+    32 bins) is what the crate builds; other counts change the tree. A
+    non-reference count is chosen only for workloads that allow it, and only
+    when its total SAH cost is within 1% of the reference profile's.
+
+Each candidate is timed as the median of several builds (CUDA events on the
+build stream, inputs resident on the device, L2 flushed before each build).
+Run on a GPU:  python -m marigold_b200.autotune [--workloads ...]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "tuning.json")
+
+MEDIUM_MAX = (64, 128, 256, 512, 1024)
+BINS = (0, 8, 16, 24)
+
+
+def load_table() -> dict:
+    try:
+        with open(TABLE) as f:
+            return json.load(f)
+    except FileNotFoundError:
+        return {}
+
+
+def choice(workload: str, key: str, default):
+    return load_table().get(workload, {}).get("choice", {}).get(key, default)
+
+
+def _workloads():
+    from . import synth
+
+    def icosphere():
+        v, t = synth.config2_mesh()
+        return [{"v": v, "t": t, "bounds": synth.mesh_bounds(v)}], False
+
+    def batched():
+        meshes, bounds, inst = synth.batched_scene()
+        ms = [{"v": v, "t": t, "bounds": b} for (v, t), b in zip(meshes, bounds)]
+        ms.append({"aabbs": inst})
+        return ms, True
+
+    def mixed():
+        v, t = synth.mixed_scene()
+        return [{"v": v, "t": t, "bounds": None}], False
+
+    return {"icosphere_l8": icosphere, "batched_scene": batched, "mixed_scene": mixed}
+
+
+def _measure(ctx, meshes, medium_max, bins, reps=5):
+    import torch
+    from . import BvhSettings, build_batch_device
+    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
+    descs = []
+    for m in meshes:
+        if "aabbs" in m:
+            descs.append({"aabbs": m["dev_aabbs"]})
+        else:
+            descs.append({"vertices": m["dev_v"], "triangles": m["dev_t"], "bounds": m["bounds"]})
+    total = sum(m["n"] for m in meshes)
+    slots = sum(2 * m["n"] - 1 for m in meshes if m["n"])
+    nodes = torch.empty(slots * 8, dtype=torch.int32, device="cuda")
+    lens = torch.empty(slots, dtype=torch.int32, device="cuda")
+    perm = torch.empty(total, dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    times = []
+    offs = None
+    for k in range(reps + 1):
+        flush.fill_(k & 0xFF)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        offs, rc, st = build_batch_device(ctx, BvhSettings(bins=bins), descs, nodes, perm,
+                                          out_lens=lens, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k:
+            times.append(e0.elapsed_time(e1))
+    from .bvh import NODE_DTYPE, sah_cost
+    nh = nodes.cpu().numpy().view(NODE_DTYPE)
+    lh = lens.cpu().numpy().view(np.uint32)
+    sah = sum(sah_cost(nh[offs[i]:offs[i + 1]], lh[offs[i]:offs[i + 1]])
+              for i in range(len(meshes)) if offs[i + 1] > offs[i])
+    return float(np.median(times)), sah
+
+
+def tune(names):
+    import torch
+    from . import _lib
+    table = load_table()
+    ctx = _lib.Context(0)
+    for name in names:
+        meshes, bins_free = _workloads()[name]()
+        for m in meshes:
+            if "aabbs" in m:
+                m["dev_aabbs"] = torch.from_numpy(m["aabbs"]).cuda()
+                m["n"] = m["aabbs"].shape[0]
+            else:
+                m["dev_v"] = torch.from_numpy(m["v"]).cuda()
+                m["dev_t"] = torch.from_numpy(m["t"].view(np.int32)).cuda()
+                m["n"] = m["t"].shape[0]
+        rows = []
+        for mm in MEDIUM_MAX:
+            ms, sah = _measure(ctx, meshes, mm, 0)
+            rows.append({"medium_max": mm, "bins": 0, "ms": round(ms, 4), "sah": sah})
+            print(name, rows[-1], file=sys.stderr, flush=True)
+        best_ref = min((r for r in rows if r["bins"] == 0), key=lambda r: r["ms"])
+        ref_sah = best_ref["sah"]
+        chosen = dict(best_ref)
+        if bins_free:
+            for b in BINS[1:]:
+                ms, sah = _measure(ctx, meshes, best_ref["medium_max"], b)
+                rows.append({"medium_max": best_ref["medium_max"], "bins": b, "ms": round(ms, 4),
+                             "sah": sah})
+                print(name, rows[-1], file=sys.stderr, flush=True)
+                if sah <= 1.01 * ref_sah and ms < chosen["ms"]:
+                    chosen = dict(rows[-1])
+        table[name] = {
+            "choice": {"medium_max": chosen["medium_max"], "bins": chosen["bins"]},
+            "reference_profile_sah": ref_sah,
+            "candidates": rows,
+            "rule": ("fastest medium_max (tree unchanged); bins other than the reference "
+                     "profile only where allowed and within 1% of its SAH")
+                    + ("" if bins_free else "; bins fixed to the reference profile"),
+            "measured": time.strftime("%Y-%m-%d"),
+        }
+        with open(TABLE, "w") as f:
+            json.dump(table, f, indent=1)
+    ctx.close()
+    return table
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workloads", nargs="*", default=["icosphere_l8", "batched_scene"])
+    a = ap.parse_args()
+    tune(a.workloads)
+    print(json.dumps(load_table(), indent=1))
