@@ -127,7 +127,7 @@ typedef struct mgbvh_stats {
        [2] subtrees of 33..1024 objects, [3] subtrees of <= 32 objects */
     double phase_seconds[4];
     uint32_t graph_replay;        /* 1: a batched build replayed its captured CUDA graph */
-    uint32_t reserved;
+    uint32_t learned_splits;      /* nodes where a split-network proposal replaced the binned split */
 } mgbvh_stats;
 
 typedef struct mgbvh_ctx mgbvh_ctx;
@@ -305,6 +305,45 @@ MGBVH_API int mgbvh_trace_closest_dev(mgbvh_tracer* tracer, const float* d_rays,
 MGBVH_API int mgbvh_trace_bruteforce_dev(mgbvh_tracer* tracer, const float* d_rays,
                                          uint32_t n_rays, float* d_hit_t, uint32_t* d_hit_prim,
                                          void* cuda_stream);
+
+/*
+ * Learned split proposer (no counterpart in the reference). A small MLP,
+ * 24 -> 64 -> 64 -> 49 with GELU, BF16 parameters and FP32 accumulation,
+ * proposes split positions for nodes of 33..1024 objects; the builder scores
+ * the proposals exactly with the reference's cost formula and keeps the plain
+ * split unless a proposal costs less (mgbvh_set_split_proposer). Parameters:
+ * MGBVH_MLP_PARAMS values, W1[64x24] b1[64] W2[64x64] b2[64] W3[49x64] b3[49].
+ * Training on the GPU: the caller zeroes d_grad and d_loss, calls
+ * mgbvh_mlp_train_step_dev over a batch (features B x 24 f32, labels B u32 =
+ * axis * 16 + position bucket or 0xFFFFFFFF, gains B f32 in {0, 1}), which
+ * adds the gradient of the mean loss (softmax cross-entropy of the 48
+ * position logits + binary cross-entropy of the refine logit) and the summed
+ * losses [ce, bce]; then mgbvh_mlp_adam_dev updates the FP32 master weights
+ * and rewrites the BF16 copy. All pointers are device pointers.
+ */
+#define MGBVH_MLP_PARAMS 8945
+MGBVH_API int mgbvh_mlp_train_step_dev(const float* d_features, const uint32_t* d_labels,
+                                       const float* d_gains, uint32_t batch,
+                                       const void* d_weights_bf16, float* d_grad, float* d_loss,
+                                       void* cuda_stream);
+MGBVH_API int mgbvh_mlp_forward_dev(const float* d_features, uint32_t batch,
+                                    const void* d_weights_bf16, float* d_out, void* cuda_stream);
+MGBVH_API int mgbvh_mlp_adam_dev(float* d_master, void* d_weights_bf16, const float* d_grad,
+                                 float* d_m, float* d_v, uint32_t step, float lr, float beta1,
+                                 float beta2, float eps, void* cuda_stream);
+
+/* Builds on this context use the learned split proposer at every binned node
+   of 33..1024 objects (d_weights_bf16: MGBVH_MLP_PARAMS BF16 values on the
+   device; NULL turns it off). gate != 0: only where the network's refine
+   logit is positive. The trees then differ from the reference's (the plain
+   split is replaced only by an exactly cheaper one). */
+MGBVH_API int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate);
+/* Builds on this context also write one training sample (30 floats: 24
+   features, label bits, gain, n, plain cost, full-sweep cost, node start) per
+   binned node of 33..1024 objects to d_samples (device, capacity samples) and
+   count them in *d_count (device; the caller zeroes it). NULL turns it off. */
+MGBVH_API int mgbvh_set_sample_output(mgbvh_ctx* ctx, float* d_samples, uint32_t capacity,
+                                      uint32_t* d_count);
 
 /*
  * AsGpuBytes for BvhNode (bvh/src/lib.rs:157-212), host side: 8 u32 words per

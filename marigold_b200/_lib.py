@@ -33,6 +33,8 @@ EXPORTED = (
     "mgbvh_sah_cost", "mgbvh_build_aabbs_noalloc", "mgbvh_tracer_create", "mgbvh_tracer_destroy",
     "mgbvh_tracer_set_blas_dev", "mgbvh_trace_closest_dev", "mgbvh_trace_bruteforce_dev",
     "mgbvh_build_batch_dev", "mgbvh_set_tuning", "mgbvh_set_graph_capture",
+    "mgbvh_mlp_train_step_dev", "mgbvh_mlp_forward_dev", "mgbvh_mlp_adam_dev",
+    "mgbvh_set_split_proposer", "mgbvh_set_sample_output",
 )
 
 
@@ -76,7 +78,7 @@ class Stats(ctypes.Structure):
         ("levels", ctypes.c_uint32),
         ("phase_seconds", ctypes.c_double * 4),
         ("graph_replay", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("learned_splits", ctypes.c_uint32),
     ]
 
     def as_dict(self):
@@ -166,6 +168,17 @@ def load():
         L.mgbvh_build_batch_dev.argtypes = [P, ctypes.POINTER(MeshDesc), u32, ctypes.POINTER(Settings),
                                             P, u32, P, P, pu32, ctypes.POINTER(Stats)]
         L.mgbvh_build_batch_dev.restype = ctypes.c_int
+        L.mgbvh_mlp_train_step_dev.argtypes = [P, P, P, u32, P, P, P, P]
+        L.mgbvh_mlp_train_step_dev.restype = ctypes.c_int
+        L.mgbvh_mlp_forward_dev.argtypes = [P, u32, P, P, P]
+        L.mgbvh_mlp_forward_dev.restype = ctypes.c_int
+        f32 = ctypes.c_float
+        L.mgbvh_mlp_adam_dev.argtypes = [P, P, P, P, P, u32, f32, f32, f32, f32, P]
+        L.mgbvh_mlp_adam_dev.restype = ctypes.c_int
+        L.mgbvh_set_split_proposer.argtypes = [P, P, ctypes.c_int]
+        L.mgbvh_set_split_proposer.restype = ctypes.c_int
+        L.mgbvh_set_sample_output.argtypes = [P, P, u32, P]
+        L.mgbvh_set_sample_output.restype = ctypes.c_int
         L.mgbvh_set_graph_capture.argtypes = [P, ctypes.c_int]
         L.mgbvh_set_graph_capture.restype = ctypes.c_int
         L.mgbvh_set_tuning.argtypes = [P, u32]
@@ -200,6 +213,27 @@ class Context:
 
     def set_stream(self, stream_handle: int | None):
         self.check(self.L.mgbvh_set_stream(self.ptr, ctypes.c_void_p(stream_handle or 0)))
+
+    def set_tuning(self, medium_max: int):
+        self.check(self.L.mgbvh_set_tuning(self.ptr, medium_max))
+
+    def set_graph_capture(self, on: bool):
+        self.check(self.L.mgbvh_set_graph_capture(self.ptr, 1 if on else 0))
+
+    def set_split_proposer(self, weights_bf16=None, gate: bool = True):
+        """Device BF16 parameter tensor (8,945 values, kept alive by the
+        caller) or None to build with the plain binned split only."""
+        p = ctypes.c_void_p(weights_bf16.data_ptr()) if weights_bf16 is not None else None
+        self.check(self.L.mgbvh_set_split_proposer(self.ptr, p, 1 if gate else 0))
+
+    def set_sample_output(self, samples=None, capacity: int = 0, count=None):
+        """Device float32 buffer of capacity x 30 values and a uint32/int32
+        counter (both kept alive by the caller), or None to stop sampling."""
+        if samples is None:
+            self.check(self.L.mgbvh_set_sample_output(self.ptr, None, 0, None))
+            return
+        self.check(self.L.mgbvh_set_sample_output(self.ptr, ctypes.c_void_p(samples.data_ptr()),
+                                                  capacity, ctypes.c_void_p(count.data_ptr())))
 
     def close(self):
         if self.ptr:

@@ -14,8 +14,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgbvh.so")
-SOURCES = ["mgbvh_build.cu", "mgbvh_trace.cu"]
-HEADERS = ["mgbvh_exact.cuh", "mgbvh_device.cuh"]
+SOURCES = ["mgbvh_build.cu", "mgbvh_trace.cu", "mgbvh_mlp.cu"]
+HEADERS = ["mgbvh_exact.cuh", "mgbvh_device.cuh", "mgbvh_mlp.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -36,6 +36,7 @@
 #include <cub/device/device_scan.cuh>
 
 #include "mgbvh_device.cuh"
+#include "mgbvh_learn.cuh"
 
 namespace mgbvh {
 
@@ -758,10 +759,123 @@ __device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
         k[q] = ((q % 6) < 3) ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
 }
 
+// The learned form at one binned node of the medium phase (warp-uniform):
+//  * with LN.samples: write a training sample (node features, the exact
+//    full-sweep optimum's axis and 1/16 position bucket, whether it beats the
+//    plain split, n, both costs, the node's start);
+//  * with LN.w: run the network, score 16 thresholds inside each of its two
+//    best (axis, bucket) proposals exactly (one per lane), and replace the
+//    plain split when the best of them costs strictly less.
+__device__ __noinline__ void learned_node(const MediumSmem& S, const Learn& LN, const Params& P,
+                                          const MNode& nd, uint32_t ib, uint32_t base, uint32_t s,
+                                          uint32_t n, uint32_t depth, uint32_t tbase,
+                                          const uint32_t* cnt, const float* ext,
+                                          uint32_t plain_ck, uint32_t lane, Cand& win,
+                                          uint32_t& axis, uint32_t& n_lt, bool& use_thr) {
+    float f[24];
+    node_features(nd.b, nd.cb, n, depth, cnt, f);
+    const float sa_p = surface_area6(nd.b);
+    auto fetch = [&](uint32_t j, float* lo, float* hi) {
+        const uint32_t r = S.idx[ib][s + j];
+        const float4 a = S.rlo[r], b = S.rhi[r];
+        lo[0] = a.x;
+        lo[1] = a.y;
+        lo[2] = a.z;
+        hi[0] = b.x;
+        hi[1] = b.y;
+        hi[2] = b.z;
+    };
+    if (LN.samples) {
+        // full sweep: every centroid a threshold on every axis; first minimum
+        // of (cost, axis, threshold value)
+        uint32_t bk = kNoKey, ba = 3, bt = kNoKey;
+        float bthr = 0.0f;
+        for (uint32_t a = 0; a < 3; ++a) {
+            for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                float thr = 0.0f;
+                if (k < n) {
+                    float lo[3], hi[3];
+                    fetch(k, lo, hi);
+                    thr = center_of(lo[a], hi[a]);
+                }
+                Cand c;
+                score_threshold(fetch, n, a, thr, k < n, sa_p, P, c, 0);
+                const uint32_t ck = static_cast<uint32_t>(c.key >> 32);
+                const uint32_t tk = fkey(thr);
+                if (c.key != ~0ull && (ck < bk || (ck == bk && (a < ba || (a == ba && tk < bt))))) {
+                    bk = ck;
+                    ba = a;
+                    bt = tk;
+                    bthr = thr;
+                }
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const uint32_t ok = __shfl_xor_sync(kFull, bk, off);
+            const uint32_t oa = __shfl_xor_sync(kFull, ba, off);
+            const uint32_t ot = __shfl_xor_sync(kFull, bt, off);
+            const float oth = __shfl_xor_sync(kFull, bthr, off);
+            if (ok < bk || (ok == bk && (oa < ba || (oa == ba && ot < bt)))) {
+                bk = ok;
+                ba = oa;
+                bt = ot;
+                bthr = oth;
+            }
+        }
+        if (lane == 0) {
+            const uint32_t slot = atomicAdd(LN.count, 1u);
+            if (slot < LN.cap) {
+                float* out = LN.samples + (size_t)slot * kSampleWidth;
+                for (int j = 0; j < 24; ++j) out[j] = f[j];
+                uint32_t label = 0xFFFFFFFFu;
+                float gain = 0.0f;
+                if (bk != kNoKey && ext[ba] > 0.0f) {
+                    const float pct = (bthr - nd.cb[ba]) / ext[ba];
+                    int q = (int)floorf(pct * 16.0f);
+                    q = min(max(q, 0), 15);
+                    label = ba * 16u + (uint32_t)q;
+                    gain = bk < plain_ck ? 1.0f : 0.0f;
+                }
+                out[24] = __uint_as_float(label);
+                out[25] = gain;
+                out[26] = (float)n;
+                out[27] = funkey(plain_ck);
+                out[28] = bk == kNoKey ? __int_as_float(0x7F800000) : funkey(bk);
+                out[29] = (float)(base + s - tbase);
+            }
+        }
+    }
+    if (LN.w) {
+        int top0 = 0, top1 = 0;
+        float refine = 0.0f;
+        mgbvh_mlp::warp_forward(f, LN.w, lane, top0, top1, refine);
+        if (!LN.gate || refine > 0.0f) {
+            const int prop = (lane >> 4) ? top1 : top0;
+            const uint32_t pa = (uint32_t)prop >> 4, bucket = (uint32_t)prop & 15u;
+            const uint32_t k = lane & 15u;
+            const float thr = __fadd_rn(nd.cb[pa], __fmul_rn(ext[pa], __fdiv_rn(
+                                                                           (float)(bucket * 16u + k + 1u),
+                                                                           256.0f)));
+            Cand c;
+            score_threshold(fetch, n, pa, thr, ext[pa] > 0.0f, sa_p, P, c, lane);
+            const uint64_t wk2 = warp_min_key(c.key);
+            const uint32_t wlo = static_cast<uint32_t>(wk2);
+            if (wlo != kNoKey && static_cast<uint32_t>(wk2 >> 32) < plain_ck) {
+                shfl_cand(c, wlo & 0xFFu);
+                win = c;
+                axis = (wlo >> 8) & 3u;
+                n_lt = c.n_lt;
+                use_thr = true;
+            }
+        }
+    }
+}
+
 // One CTA builds the subtree of one medium node (33..1024 objects).
 __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* rec0, Rec* rec1,
                                             Task* small, uint32_t cap_small, const Params& P,
-                                            const Out& O) {
+                                            const Out& O, const Learn& LN) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     Rec* src = (t.buf ? rec1 : rec0) + t.start;
     const uint32_t base = t.start;
@@ -824,6 +938,7 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
             Cand win;
             uint32_t axis = 0, sbin = 0, n_lt = 0;
             bool median = false;
+            bool use_thr = false;  // the learned form replaced the binned split
             const uint32_t B = P.bins ? P.bins : 32u;
             float ext[3];
             bool axis_ok[3];
@@ -880,6 +995,11 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
                     const float cost = funkey(static_cast<uint32_t>(wk >> 32));
                     if (n <= P.max_leaf && cost >= leaf_cost(n)) leaf = true;
                     n_lt = win.n_lt;
+                    if (!leaf && (LN.w || LN.samples) && B == 32u)
+                        learned_node(S, LN, P, nd, ib, base, s, n, depth, t.tbase, cnt, ext,
+                                     static_cast<uint32_t>(wk >> 32), lane, win, axis, n_lt,
+                                     use_thr);
+                    if (use_thr && lane == 0) atomicAdd(&O.ctr->learned, 1u);
                 }
             }
             if (leaf) {
@@ -890,11 +1010,12 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
             init_key12(ck);
             uint32_t ob = ib ^ 1u;
             if (!median) {
-                const float cmin = nd.cb[axis], ex = ext[axis];
+                const float cmin = nd.cb[axis], ex = ext[axis], thr = win.thr;
+                const bool by_thr = use_thr;
                 const uint32_t got = medium_partition(
                     S, ib, s, n, n_lt, lane,
                     [&](uint32_t, const float* c) {
-                        return bin_of(c[axis], cmin, ex, B) < sbin;
+                        return by_thr ? c[axis] < thr : bin_of(c[axis], cmin, ex, B) < sbin;
                     },
                     ck);
                 if (got != n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
@@ -1050,13 +1171,14 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
 
 __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
-                                                                uint32_t cap_small, Params P, Out O) {
+                                                                uint32_t cap_small, Params P, Out O,
+                                                                Learn LN) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
     const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
     for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
         __syncthreads();
-        medium_task(S, tasks[ti], rec0, rec1, small, cap_small, P, O);
+        medium_task(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
     }
 }
 
@@ -1414,6 +1536,12 @@ struct mgbvh_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<unsigned char> graph_sig;
     uint32_t graph_levels = 0, graph_launches = 0;
+    // learned split proposer (changes trees) and training-sample output
+    const void* learn_w = nullptr;
+    int learn_gate = 1;
+    float* learn_samples = nullptr;
+    uint32_t learn_cap = 0;
+    uint32_t* learn_count = nullptr;
     Counters* h_ctr = nullptr;
 };
 
@@ -1577,8 +1705,14 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
         const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
+        Learn LN;
+        LN.w = static_cast<const __nv_bfloat16*>(ctx->learn_w);
+        LN.gate = ctx->learn_gate;
+        LN.samples = ctx->learn_samples;
+        LN.cap = ctx->learn_cap;
+        LN.count = ctx->learn_count;
         medium_kernel<<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
-            P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O);
+            P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
         launches++;
         if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
         // small subtrees: count read on the device; grid sized for full occupancy
@@ -1733,6 +1867,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
         stats->height = hc.height;
         stats->max_depth = st->max_depth;
         stats->median_splits = hc.median_splits;
+        stats->learned_splits = hc.learned;
         stats->depth_capped_leaves = hc.depth_capped;
         stats->kernel_launches = launches;
         stats->levels = levels;
@@ -2132,6 +2267,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         stats->height = hc.height;
         stats->max_depth = st->max_depth;
         stats->median_splits = hc.median_splits;
+        stats->learned_splits = hc.learned;
         stats->depth_capped_leaves = hc.depth_capped;
         stats->kernel_launches = launches;
         stats->levels = levels;
@@ -2413,6 +2549,33 @@ int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_
                      d_out_perm, out_node_offsets, out_stats);
 }
 
+int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    ctx->learn_w = d_weights_bf16;
+    ctx->learn_gate = gate != 0;
+    if (ctx->graph_exec) {  // a captured graph holds the old switch
+        cudaSetDevice(ctx->device);
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_sig.clear();
+    }
+    return MGBVH_OK;
+}
+
+int mgbvh_set_sample_output(mgbvh_ctx* ctx, float* d_samples, uint32_t capacity, uint32_t* d_count) {
+    if (!ctx || (d_samples && !d_count)) return MGBVH_ERR_INVALID_ARG;
+    ctx->learn_samples = d_samples;
+    ctx->learn_cap = d_samples ? capacity : 0;
+    ctx->learn_count = d_samples ? d_count : nullptr;
+    if (ctx->graph_exec) {
+        cudaSetDevice(ctx->device);
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_sig.clear();
+    }
+    return MGBVH_OK;
+}
+
 int mgbvh_set_graph_capture(mgbvh_ctx* ctx, int enable) {
     if (!ctx) return MGBVH_ERR_INVALID_ARG;
     ctx->graph_mode = enable != 0;
@@ -2553,7 +2716,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
                                                       st->max_depth);
     if (cls == 2)
         medium_kernel<<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
-            S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O);
+            S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr});
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
         if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)

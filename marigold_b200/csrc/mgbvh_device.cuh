@@ -43,6 +43,8 @@ struct Counters {
     uint32_t n_medium;
     uint32_t n_small;
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
+    uint32_t learned;        // nodes where a proposal of the split network replaced the binned split
+    uint32_t pad_;
 };
 
 enum ErrorSite : uint32_t {

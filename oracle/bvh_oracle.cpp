@@ -172,6 +172,13 @@ struct CachedAcc {  // precomputed AABBs (parity mode; identical values)
 
 struct Knobs {
     uint32_t bins, adaptive_max_n, adaptive_steps;
+    uint32_t full_sweep;  // every node: every centroid a threshold on every axis
+    // the learned form with fixed proposals (learn_max_n 0: off): at every
+    // binned node of 33..learn_max_n objects, 16 thresholds inside each of
+    // the two (axis * 16 + bucket) proposals replace the binned split when
+    // strictly cheaper
+    uint32_t learn_max_n;
+    uint32_t prop[2];
 };
 
 template <class Acc, bool kFaithful>
@@ -182,7 +189,10 @@ struct Builder {
     std::vector<uint32_t> list;
     std::vector<Node> nodes;
     uint32_t height = 0;
-    uint32_t median_splits = 0, tie_events = 0, depth_capped = 0;
+    // node samples for the learned split proposer (features + full-sweep label)
+    std::vector<float>* samples = nullptr;
+    uint32_t sample_min_n = 33;
+    uint32_t median_splits = 0, tie_events = 0, depth_capped = 0, learned_splits = 0;
     int error = 0;
 
     Builder(const Acc& a, uint32_t mn, uint32_t mx, uint32_t md, Knobs kn)
@@ -374,8 +384,211 @@ struct Builder {
         return sp;
     }
 
+    // Exact sweep (not in the reference; the quality yardstick of the learned
+    // proposer): on each axis, every distinct centroid value is a threshold
+    // (lt = centroids strictly below it), scored with the reference's cost
+    // formula; first minimum over (cost, axis, threshold rank) wins.
+    bool full_sweep(const BV& parent, uint32_t s, uint32_t n, Split& out) {
+        const float sa_p = bv_surface_area(parent);
+        std::vector<std::pair<float, uint32_t>> key(n);
+        std::vector<BV> pre(n), suf(n);
+        bool found = false;
+        for (int axis = 0; axis < 3; ++axis) {
+            for (uint32_t i = 0; i < n; ++i) key[i] = {center(list[s + i], axis), list[s + i]};
+            std::stable_sort(key.begin(), key.end(),
+                             [](const auto& a, const auto& b) { return total_key(a.first) < total_key(b.first); });
+            BV acc = bv_empty();
+            for (uint32_t i = 0; i < n; ++i) {
+                bv_grow(acc, acc_box(key[i].second));
+                pre[i] = acc;
+            }
+            acc = bv_empty();
+            for (uint32_t i = n; i-- > 0;) {
+                bv_grow(acc, acc_box(key[i].second));
+                suf[i] = acc;
+            }
+            for (uint32_t i = 1; i < n; ++i) {
+                if (!(key[i - 1].first < key[i].first)) continue;  // same centroid: same set
+                const uint32_t nl = i, ng = n - i;
+                if (nl < MIN || ng < MIN) continue;
+                Split sp{};
+                sp.lt = pre[i - 1];
+                sp.gt = suf[i];
+                sp.cnt_lt = nl;
+                sp.cnt_gt = ng;
+                sp.cost = split_cost(bv_surface_area(sp.lt), bv_surface_area(sp.gt), sa_p, nl, ng);
+                sp.kind = kThreshold;
+                sp.axis = axis;
+                sp.threshold = key[i].first;
+                if (!found || better(sp, out)) {
+                    out = sp;
+                    found = true;
+                }
+            }
+        }
+        return found;
+    }
+
+    BV acc_box(uint32_t id) const { return acc(id); }
+
+    // One training sample per node: 24 features, then the label: the
+    // full-sweep optimum's axis * 16 + position bucket (16 equal buckets over
+    // the centroid extent), whether it beats the plain split's cost, the
+    // object count, both costs and the node's start in the object list. Feature order (all finite):
+    //   0-2  node extent / largest node extent
+    //   3-5  centroid extent / largest node extent
+    //   6    log2(n) / 20
+    //   7-18 per axis, the fraction of centroids in 4 equal buckets of the
+    //        centroid extent (floor(4 * (c - cmin) / ext), clamped)
+    //   19   SA(centroid bounds) / SA(node)
+    //   20   depth / 32
+    //   21   middle / largest node extent, 22 smallest / largest node extent
+    //   23   largest centroid extent / largest node extent
+    void record_sample(const BV& parent, uint32_t s, uint32_t n, uint32_t depth) {
+        float cmn[3] = {kInf, kInf, kInf}, cmx[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = s; i < s + n; ++i) {
+            BV b = acc(list[i]);
+            for (int a = 0; a < 3; ++a) {
+                const float c = bv_center(b, a);
+                cmn[a] = vmin(cmn[a], c);
+                cmx[a] = vmax(cmx[a], c);
+            }
+        }
+        float f[24] = {0};
+        float ext[3], cext[3];
+        for (int a = 0; a < 3; ++a) {
+            ext[a] = parent.mx[a] - parent.mn[a];
+            cext[a] = cmx[a] - cmn[a];
+        }
+        const float emax = std::max(std::max(ext[0], ext[1]), std::max(ext[2], 1e-30f));
+        for (int a = 0; a < 3; ++a) {
+            f[a] = ext[a] / emax;
+            f[3 + a] = cext[a] / emax;
+        }
+        f[6] = std::log2((float)n) / 20.0f;
+        for (uint32_t i = s; i < s + n; ++i) {
+            BV b = acc(list[i]);
+            for (int a = 0; a < 3; ++a) {
+                if (!(cext[a] > 0.0f)) continue;
+                const float pct = (bv_center(b, a) - cmn[a]) / cext[a];
+                int q = (int)std::floor(pct * 4.0f);
+                q = std::min(std::max(q, 0), 3);
+                f[7 + 4 * a + q] += 1.0f;
+            }
+        }
+        for (int j = 7; j < 19; ++j) f[j] /= (float)n;
+        BV cb{{cmn[0], cmn[1], cmn[2]}, {cmx[0], cmx[1], cmx[2]}};
+        const float sap = bv_surface_area(parent);
+        f[19] = sap > 0.0f ? bv_surface_area(cb) / sap : 0.0f;
+        f[20] = (float)depth / 32.0f;
+        float e[3] = {ext[0], ext[1], ext[2]};
+        std::sort(e, e + 3);
+        f[21] = e[1] / emax;
+        f[22] = e[0] / emax;
+        f[23] = std::max(std::max(cext[0], cext[1]), cext[2]) / emax;
+        Split plain, best;
+        const bool okp = select_split_plain(parent, s, n, plain);
+        const bool okf = full_sweep(parent, s, n, best);
+        uint32_t label = 0xFFFFFFFFu, gain = 0;
+        if (okf && cext[best.axis] > 0.0f) {
+            const float pct = (best.threshold - cmn[best.axis]) / cext[best.axis];
+            int q = (int)std::floor(pct * 16.0f);
+            q = std::min(std::max(q, 0), 15);
+            label = (uint32_t)best.axis * 16u + (uint32_t)q;
+            gain = (!okp || total_key(best.cost) < total_key(plain.cost)) ? 1u : 0u;
+        }
+        for (int j = 0; j < 24; ++j) samples->push_back(f[j]);
+        uint32_t lb = label;
+        float w;
+        std::memcpy(&w, &lb, 4);
+        samples->push_back(w);
+        samples->push_back((float)gain);
+        samples->push_back((float)n);
+        samples->push_back(okp ? plain.cost : kInf);
+        samples->push_back(okf ? best.cost : kInf);
+        samples->push_back((float)s);
+    }
+
+    // The learned form's split rule (not in the reference), for two given
+    // proposals: lane p * 16 + k (p = proposal, k = 0..15) tries the
+    // threshold cmin + ext * ((bucket * 16 + k + 1) / 256) on the proposal's
+    // axis; the first minimum of (cost, axis, lane) replaces the binned split
+    // when its cost is strictly below the binned cost.
+    void learned_refine(const BV& parent, uint32_t s, uint32_t n, Split& sp) {
+        float cmn[3] = {kInf, kInf, kInf}, cmx[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = s; i < s + n; ++i) {
+            BV b = acc(list[i]);
+            for (int a = 0; a < 3; ++a) {
+                const float c = bv_center(b, a);
+                cmn[a] = vmin(cmn[a], c);
+                cmx[a] = vmax(cmx[a], c);
+            }
+        }
+        uint64_t best = ~0ull;
+        Split bsp{};
+        for (uint32_t lane = 0; lane < 32; ++lane) {
+            const uint32_t prop = k.prop[lane >> 4];
+            const int a = (int)(prop >> 4);
+            const uint32_t bucket = prop & 15u, kk = lane & 15u;
+            const float ext = cmx[a] - cmn[a];
+            if (!(ext > 0.0f)) continue;
+            const float thr = cmn[a] + ext * ((float)(bucket * 16u + kk + 1u) / 256.0f);
+            Split c = eval_threshold(parent, s, n, a, thr);
+            if (c.cnt_lt < MIN || c.cnt_gt < MIN) continue;
+            const uint64_t key = ((uint64_t)total_key(c.cost) << 32) | ((uint64_t)a << 8) | lane;
+            if (key < best) {
+                best = key;
+                bsp = c;
+            }
+        }
+        if (best != ~0ull && (uint32_t)(best >> 32) < total_key(sp.cost)) {
+            sp = bsp;
+            learned_splits++;
+        }
+    }
+
+    // select_split without the full-sweep switch and without side effects on
+    // the list (binned / adaptive only; the median is not needed for labels)
+    bool select_split_plain(const BV& parent, uint32_t s, uint32_t n, Split& out) {
+        float cmn[3] = {kInf, kInf, kInf}, cmx[3] = {-kInf, -kInf, -kInf};
+        for (uint32_t i = s; i < s + n; ++i) {
+            BV b = acc(list[i]);
+            for (int a = 0; a < 3; ++a) {
+                const float c = bv_center(b, a);
+                cmn[a] = vmin(cmn[a], c);
+                cmx[a] = vmax(cmx[a], c);
+            }
+        }
+        BV cb{{cmn[0], cmn[1], cmn[2]}, {cmx[0], cmx[1], cmx[2]}};
+        bool found = false;
+        for (int axis = 0; axis < 3; ++axis) {
+            Split sp;
+            const bool ok = (n <= k.adaptive_max_n) ? adaptive_sweep(parent, cb, s, n, axis, sp)
+                                                    : binned_sweep(parent, cb, s, n, axis, sp);
+            if (ok && (!found || better(sp, out))) {
+                out = sp;
+                found = true;
+            }
+        }
+        return found;
+    }
+
     // ---- select_split, :493-534
     bool select_split(const BV& parent, uint32_t s, uint32_t n, Split& out) {
+        if (k.full_sweep) {
+            if (full_sweep(parent, s, n, out)) return true;
+            if (n <= MAX) return false;
+            bool found = false;  // coincident centroids: the forced median as below
+            for (int axis = 0; axis < 3; ++axis) {
+                Split sp = median_split(parent, s, n, axis);
+                if (!found || better(sp, out)) {
+                    out = sp;
+                    found = true;
+                }
+            }
+            median_splits++;
+            return found;
+        }
         float cmn[3] = {kInf, kInf, kInf}, cmx[3] = {-kInf, -kInf, -kInf};
         for (uint32_t i = s; i < s + n; ++i) {
             BV b = acc(list[i]);
@@ -470,10 +683,14 @@ struct Builder {
                 continue;
             }
             uint32_t s = self.start, n = self.len;
+            if (samples && n >= sample_min_n) record_sample(self.bounds, s, n, depth);
             Split sp;
             if (!select_split(self.bounds, s, n, sp)) continue;  // :576-579
             // :583 (leaf_cost, :251-253); a NaN cost compares false and splits
             if (self.len <= MAX && sp.cost >= kObjectCost * static_cast<float>(self.len)) continue;
+            if (k.learn_max_n && !k.full_sweep && n > 32 && n <= k.learn_max_n && sp.kind == kIndex &&
+                (k.bins ? k.bins : std::clamp<uint32_t>(n, 16, 32)) == 32)
+                learned_refine(self.bounds, s, n, sp);
             uint32_t split_index;
             if (sp.kind == kThreshold) {  // :598-600
                 int ax = sp.axis;
@@ -576,6 +793,7 @@ int run_build(const Acc& acc, uint32_t n, const float* root_bounds, uint32_t MIN
         st->height = b.height;
         st->max_depth = max_depth;
         st->median_splits = b.median_splits;
+        st->learned_splits = b.learned_splits;
         st->depth_capped_leaves = b.depth_capped;
         st->feasible = feasible;
     }
@@ -588,7 +806,8 @@ int run_build(const Acc& acc, uint32_t n, const float* root_bounds, uint32_t MIN
 extern "C" {
 
 typedef struct oracle_knobs {
-    uint32_t bins, adaptive_max_n, adaptive_steps, faithful;
+    uint32_t bins, adaptive_max_n, adaptive_steps, faithful, full_sweep;
+    uint32_t learn_max_n, prop0, prop1;  // the learned form with fixed proposals (0: off)
 } oracle_knobs;
 
 // Builds with the oracle. Exactly one of (verts, tris) or aabbs is given.
@@ -607,7 +826,9 @@ int oracle_build(const float* verts, uint32_t vertex_stride_bytes, const uint32_
         if (st) std::memset(st, 0, sizeof(*st));
         return MGBVH_WARN_EMPTY;
     }
-    Knobs k{kn ? kn->bins : 0, kn ? kn->adaptive_max_n : 32, kn ? kn->adaptive_steps : 0};
+    Knobs k{kn ? kn->bins : 0, kn ? kn->adaptive_max_n : 32, kn ? kn->adaptive_steps : 0,
+            kn ? kn->full_sweep : 0, kn ? kn->learn_max_n : 0,
+            {kn ? kn->prop0 % 48u : 0, kn ? kn->prop1 % 48u : 0}};
     bool faithful = kn && kn->faithful;
     if (verts) {
         IndexedAcc acc{verts, vertex_stride_bytes / 4, tris};
@@ -632,6 +853,34 @@ int oracle_build(const float* verts, uint32_t vertex_stride_bytes, const uint32_
 }
 
 uint32_t oracle_last_tie_events(void) { return g_tie_events; }
+
+// Node samples of a plain (reference-profile) build over triangles: 30 floats
+// per node with at least min_n objects (24 features, label as u32 bits, gain
+// flag, n, plain cost, full-sweep cost, start). Returns the number of samples
+// written (at most capacity).
+uint32_t oracle_sample_nodes(const float* verts, uint32_t vertex_stride_bytes, const uint32_t* tris,
+                             uint32_t n, uint32_t min_n, float* out, uint32_t capacity) {
+    IndexedAcc acc0{verts, vertex_stride_bytes / 4, tris};
+    std::vector<BV> cache(n);
+    for (uint32_t i = 0; i < n; ++i) cache[i] = acc0(i);
+    CachedAcc acc{cache.data()};
+    Builder<CachedAcc, false> b(acc, 1, 1, 32, Knobs{0, 32, 0, 0, 0, {0, 0}});
+    std::vector<float> samples;
+    b.samples = &samples;
+    b.sample_min_n = min_n;
+    b.list.resize(n);
+    std::iota(b.list.begin(), b.list.end(), 0u);
+    Node root{};
+    root.bounds = bv_empty();
+    for (uint32_t i = 0; i < n; ++i) bv_grow(root.bounds, acc(i));
+    root.start = 0;
+    root.len = n;
+    b.nodes.reserve(2 * (size_t)n);
+    b.build(root);
+    const uint32_t count = std::min<uint32_t>((uint32_t)(samples.size() / 30), capacity);
+    std::memcpy(out, samples.data(), sizeof(float) * 30 * (size_t)count);
+    return count;
+}
 
 // Closest hit of each ray against every triangle: the Moller-Trumbore test of
 // marigold/assets/shaders/slang/lib/scene.slang:19-89 (|det| < 1e-6 and

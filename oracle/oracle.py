@@ -44,7 +44,7 @@ class Stats(ctypes.Structure):
         ("levels", ctypes.c_uint32),
         ("phase_seconds", ctypes.c_double * 4),
         ("graph_replay", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("learned_splits", ctypes.c_uint32),
     ]
 
     def as_dict(self):
@@ -59,6 +59,10 @@ class _Knobs(ctypes.Structure):
         ("adaptive_max_n", ctypes.c_uint32),
         ("adaptive_steps", ctypes.c_uint32),
         ("faithful", ctypes.c_uint32),
+        ("full_sweep", ctypes.c_uint32),
+        ("learn_max_n", ctypes.c_uint32),
+        ("prop0", ctypes.c_uint32),
+        ("prop1", ctypes.c_uint32),
     ]
 
 
@@ -87,6 +91,8 @@ def lib():
             L.oracle_last_tie_events.restype = u32
             L.oracle_trace_bruteforce.argtypes = [P, u32, P, u32, P, u32, P, P]
             L.oracle_trace_bruteforce.restype = None
+            L.oracle_sample_nodes.argtypes = [P, u32, P, u32, u32, P, u32]
+            L.oracle_sample_nodes.restype = u32
             _lib = L
     return _lib
 
@@ -97,13 +103,16 @@ def _ptr(a):
 
 def build(vertices=None, triangles=None, aabbs=None, *, vertex_stride_bytes=32,
           root_bounds=None, min_leaf=1, max_leaf=1, max_depth=32, bins=0,
-          adaptive_max_n=32, adaptive_steps=0, faithful=False):
+          adaptive_max_n=32, adaptive_steps=0, faithful=False, full_sweep=False,
+          learned=None):
     """Build one BVH with the oracle.
 
     Either ``vertices`` (float32 [V, stride/4]) + ``triangles`` (uint32 [N, 3])
     or ``aabbs`` (float32 [N, 6]). Returns a dict with ``status``, ``nodes``
     (uint32 [count, 8], the mgbvh_node layout), ``lens``, ``perm``, ``stats``
-    and ``tie_events``.
+    and ``tie_events``. ``learned`` = (max_n, proposal0, proposal1) applies the
+    learned form's split rule with fixed (axis * 16 + bucket) proposals at
+    every binned node of 33..max_n objects.
     """
     L = lib()
     if aabbs is not None:
@@ -122,7 +131,9 @@ def build(vertices=None, triangles=None, aabbs=None, *, vertex_stride_bytes=32,
     rb = None if root_bounds is None else np.ascontiguousarray(root_bounds, dtype=np.float32)
     count = ctypes.c_uint32(0)
     st = Stats()
-    kn = _Knobs(bins, adaptive_max_n, adaptive_steps, 1 if faithful else 0)
+    lm, p0, p1 = learned if learned is not None else (0, 0, 0)
+    kn = _Knobs(bins, adaptive_max_n, adaptive_steps, 1 if faithful else 0, 1 if full_sweep else 0,
+                lm, p0, p1)
     status = L.oracle_build(_ptr(vp), vertex_stride_bytes, _ptr(tp), _ptr(aabbs), n, _ptr(rb),
                             min_leaf, max_leaf, max_depth, ctypes.byref(kn), _ptr(nodes), cap,
                             _ptr(lens), _ptr(perm), ctypes.byref(count), ctypes.byref(st))
@@ -148,3 +159,18 @@ def trace_bruteforce(vertices, triangles, rays):
     L.oracle_trace_bruteforce(_ptr(v), v.shape[1], _ptr(t), t.shape[0], _ptr(r), r.shape[0],
                               _ptr(out_t), _ptr(out_p))
     return out_t, out_p
+
+
+SAMPLE_WIDTH = 30  # 24 features, label, gain, n, plain cost, full-sweep cost, start
+
+
+def sample_nodes(vertices, triangles, min_n=33):
+    """Training samples of the learned split proposer from one plain build:
+    float32 [K, 30] rows (features[0:24], label bits, gain, n, costs, start)."""
+    L = lib()
+    v = np.ascontiguousarray(vertices, dtype=np.float32)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32)
+    cap = max(t.shape[0] // 4, 16)
+    out = np.zeros((cap, SAMPLE_WIDTH), np.float32)
+    k = L.oracle_sample_nodes(_ptr(v), v.shape[1] * 4, _ptr(t), t.shape[0], min_n, _ptr(out), cap)
+    return out[:k].copy()
