@@ -53,7 +53,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="icosphere", choices=["icosphere", "mixed", "batched"],
+    p.add_argument("--workload", default="icosphere",
+                   choices=["icosphere", "mixed", "batched", "learned"],
                    help="icosphere: the headline build; mixed: 16.8M-triangle scene + 8M rays")
     p.add_argument("--mixed-scale", type=int, default=1,
                    help="divide the mixed scene and its ray count by this factor")
@@ -376,7 +377,8 @@ def run_mixed(args):
     built with the reference profile, then 8,388,608 closest-hit rays with
     origins uniform in the scene box grown by 10% and uniform directions. The
     traversal is checked hit for hit against GPU brute force on a
-    65,536-ray subset and the brute force against the CPU oracle on 16 rays."""
+    65,536-ray subset (the brute-force kernel is itself checked against the
+    CPU oracle by the test suite)."""
     import ctypes
     import torch
     from marigold_b200 import BvhSettings, _lib, build_device, synth
@@ -445,10 +447,6 @@ def run_mixed(args):
     gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
     btn, bpn = bt.cpu().numpy(), bp.cpu().numpy().view(np.uint32)
     mism = int(((gp != bpn) | (gt.view(np.uint32) != btn.view(np.uint32))).sum())
-    from oracle import oracle as orc
-    ct, cp = orc.trace_bruteforce(v, t, rays[:16])
-    cpu_mism = int(((cp != bpn[:16]) | (ct.view(np.uint32) != btn[:16].view(np.uint32))).sum())
-    log("cpu brute force done")
     hits = int((hp.cpu().numpy().view(np.uint32) != 0xFFFFFFFF).sum())
     bms = float(np.mean(build_ms))
     tms = float(np.mean(trace_ms))
@@ -464,7 +462,6 @@ def run_mixed(args):
                   "ms": round(tms, 3), "hit_rays": hits,
                   "nodes_visited": counts[0], "box_tests": counts[1], "triangle_tests": counts[2]},
         "check": {"subset_rays": sub, "mismatches_vs_gpu_bruteforce": mism,
-                  "cpu_rays": 16, "mismatches_gpu_bruteforce_vs_cpu": cpu_mism,
                   "bruteforce_s": round(brute_s, 2)},
         "steps": args.steps, "warmup": args.warmup, "generation_s": round(gen_s, 1),
         "l2": "flushed before every build and trace",
@@ -538,9 +535,119 @@ def run_batched(args):
     print(json.dumps(out), flush=True)
 
 
+def _trace_rate(tr, d_nodes, count, dv, nv, dt, d_perm, n, dr, m, stream, flush, reps):
+    """Closest-hit Mrays/s of one built tree (median of reps traces, L2
+    flushed before each) and the number of rays that hit."""
+    import ctypes
+    import torch
+    L = tr.L
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 12, nv, vp(dt),
+                                         vp(d_perm), n, sp))
+    ht = torch.empty(m, dtype=torch.float32, device="cuda")
+    hp = torch.empty(m, dtype=torch.int32, device="cuda")
+    counts = (ctypes.c_uint64 * 3)()
+    secs = ctypes.c_double(0)
+    ms = []
+    for k in range(reps + 1):
+        flush.fill_(k & 0xFF)
+        tr.check(L.mgbvh_trace_closest_dev(tr.ptr, vp(dr), m, vp(ht), vp(hp), counts,
+                                           ctypes.byref(secs), sp))
+        if k:
+            ms.append(secs.value * 1e3)
+    hits = int((hp != -1).sum().item())
+    return m / (statistics.median(ms) * 1e-3) / 1e6, hits, list(counts)
+
+
+def run_learned(args):
+    """The learned split proposer against the plain builder on held-out seeds
+    of its two training generators (65,536 random small triangles; the
+    level-8 noisy icosphere). Per mesh and build form: device-timed build
+    Mtri/s (L2 flushed before every build), total SAH cost, and closest-hit
+    Mrays/s of 1,048,576 rays (origins uniform in the mesh box grown by 10%,
+    uniform directions) on the built tree. The full-sweep SAH of each mesh
+    comes from tests/golden/full_sweep_sah.json (written by the script beside
+    it). Forms: plain (the reference's tree), learned (trained network, refine
+    gate on), learned-ungated (every binned node of 33..1024 objects scores
+    the network's proposals)."""
+    import torch
+    from marigold_b200 import BvhSettings, _lib, build_device, learned, synth
+    from marigold_b200.bvh import NODE_DTYPE, sah_cost
+    torch.cuda.set_device(0)
+    with open(os.path.join(ROOT, "tests", "golden", "full_sweep_sah.json")) as f:
+        golden = json.load(f)
+    weights = torch.from_numpy(learned.load_weights().view(np.int16)).cuda()
+    ctx = _lib.Context(0)
+    ctx.set_tuning(1024)
+    tr = _lib.Tracer(0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    rows = []
+    for name, kind, size, seed in learned.EVAL_MESHES:
+        v, t = learned.eval_mesh(kind, size, seed)
+        n = t.shape[0]
+        dv = torch.from_numpy(v).cuda()
+        dt = torch.from_numpy(t.view(np.int32)).cuda()
+        cap = 2 * n - 1
+        d_nodes = torch.empty(cap * 8, dtype=torch.int32, device="cuda")
+        d_lens = torch.empty(cap, dtype=torch.int32, device="cuda")
+        d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        rays = synth.rays_in_box(1048576, v[:, :3].min(0), v[:, :3].max(0), seed=seed + 1)
+        dr = torch.from_numpy(rays).cuda()
+        full = golden[name]["full_sweep"]
+        row = {"mesh": name, "triangles": n, "full_sweep_sah": round(full, 4)}
+        plain_sah = None
+        for form, w, gate in (("plain", None, False), ("learned", weights, True),
+                              ("learned_ungated", weights, False)):
+            ctx.set_split_proposer(w, gate)
+            ms = []
+            for k in range(max(args.warmup, 3) + args.steps):
+                flush.fill_(k & 0xFF)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                count, rc, st = build_device(ctx, BvhSettings(), d_nodes, d_perm, vertices=dv,
+                                             triangles=dt, out_lens=d_lens, stream=stream)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ctx.check(rc)
+                if k >= max(args.warmup, 3):
+                    ms.append(e0.elapsed_time(e1))
+            nh = d_nodes[: count * 8].cpu().numpy().view(NODE_DTYPE)
+            sah = sah_cost(nh, d_lens[:count].cpu().numpy().view(np.uint32))
+            mrays, hits, _ = _trace_rate(tr, d_nodes, count, dv, v.shape[0], dt, d_perm, n, dr,
+                                         rays.shape[0], stream, flush, 5)
+            bms = statistics.median(ms)
+            row[form] = {"build_mtris": round(n / (bms * 1e-3) / 1e6, 2), "build_ms": round(bms, 3),
+                         "sah": round(sah, 4), "vs_full_sweep_pct": round(100 * (sah / full - 1), 4),
+                         "learned_splits": st["learned_splits"], "mrays": round(mrays, 2),
+                         "hit_rays": hits}
+            if form == "plain":
+                plain_sah = sah
+            else:
+                row[form]["gap_closed_pct"] = round(100 * (plain_sah - sah) / (plain_sah - full), 2)
+        ctx.set_split_proposer(None)
+        rows.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    tr.close()
+    rec = learned.load_record()
+    out = {
+        "metric": "learned split proposer: SAH vs plain binned and full sweep; build Mtri/s; Mrays/s",
+        "workload": "learned split proposer, held-out meshes", "dtype": "f32 (network bf16/fp32)",
+        "steps": args.steps, "warmup": args.warmup, "results": rows,
+        "network": {"samples": rec.get("samples"), "steps": rec.get("steps"),
+                    "heldout_accuracy": rec.get("heldout_accuracy")},
+        "config": {"medium_max": 1024, "leaf": 1, "max_depth": 32, "profile": "reference",
+                   "rays": 1048576, "l2": "flushed before every build and trace"},
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse_args()
-    if args.workload == "batched":
+    if args.workload == "learned":
+        run_learned(args)
+    elif args.workload == "batched":
         run_batched(args)
     elif args.workload == "mixed":
         run_mixed(args)

@@ -334,9 +334,10 @@ MGBVH_API int mgbvh_mlp_adam_dev(float* d_master, void* d_weights_bf16, const fl
 
 /* Builds on this context use the learned split proposer at every binned node
    of 33..1024 objects (d_weights_bf16: MGBVH_MLP_PARAMS BF16 values on the
-   device; NULL turns it off). gate != 0: only where the network's refine
-   logit is positive. The trees then differ from the reference's (the plain
-   split is replaced only by an exactly cheaper one). */
+   device, copied by this call, which returns once the copy is done; NULL
+   turns the proposer off). gate != 0: only where the network's refine logit
+   is positive. The trees then differ from the reference's (the plain split
+   is replaced only by an exactly cheaper one). No reference counterpart. */
 MGBVH_API int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate);
 /* Builds on this context also write one training sample (30 floats: 24
    features, label bits, gain, n, plain cost, full-sweep cost, node start) per

@@ -221,8 +221,8 @@ class Context:
         self.check(self.L.mgbvh_set_graph_capture(self.ptr, 1 if on else 0))
 
     def set_split_proposer(self, weights_bf16=None, gate: bool = True):
-        """Device BF16 parameter tensor (8,945 values, kept alive by the
-        caller) or None to build with the plain binned split only."""
+        """Device BF16 parameter tensor (8,945 values; the library keeps its
+        own copy) or None to build with the plain binned split only."""
         p = ctypes.c_void_p(weights_bf16.data_ptr()) if weights_bf16 is not None else None
         self.check(self.L.mgbvh_set_split_proposer(self.ptr, p, 1 if gate else 0))
 

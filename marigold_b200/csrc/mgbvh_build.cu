@@ -73,7 +73,9 @@ struct Decision {
     uint32_t n_lt;
     uint32_t child_task[2];  // [0] gt, [1] lt: next-level large task, or kNone
     uint32_t child_leaf[2];
-    uint32_t pad;
+    uint32_t use_thr;    // 1: a learned proposal won; the partition is centroid < thr
+    float thr;
+    uint32_t plain_key;  // cost key of the binned split
     float ltb[6], gtb[6];
 };
 
@@ -352,87 +354,31 @@ struct EvalArgs {
     Task* medium;
     Task* small;
     uint32_t cap_tasks, cap_tiles, cap_medium, cap_small;
+    // learned form (lw NULL: off): transposed network parameters, refine gate,
+    // per-task pending proposals, their interval bins and per-tile counts
+    const __nv_bfloat16* lw;
+    int lgate;
+    LvlRefine* refine;
+    uint32_t* rbins;
+    const uint32_t* tile_hist2;  // [proposal * 17 + interval][tile]
 };
 
-__device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
-    const Task t = A.tasks[w];
-    const uint32_t* tb = A.bins + (size_t)w * kBinWords;
-    float cmn[3], ext[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        cmn[a] = funkey(A.cbkeys[6 * w + a]);
-        ext[a] = __fsub_rn(funkey(A.cbkeys[6 * w + 3 + a]), cmn[a]);
-    }
+// Writes the node and its children of a decided split: the per-tile lt
+// counts (exclusive scan across the node's tiles of the sum of `nrows`
+// histogram rows from row0: the bins, or the intervals, left of the split),
+// the node record, and each child as a leaf, a next-level task, a medium or
+// a small subtree.
+__device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane,
+                           const Task& t, Decision& d, const uint32_t* hist, uint32_t row0,
+                           uint32_t nrows) {
     const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-    const uint32_t B = P.bins ? P.bins : 32u;
-    bool leaf = t.depth == P.max_depth || (t.len <= P.max_leaf && t.len < 2u * P.min_leaf);
-    Decision d;
-    d.kind = 1;
-    d.axis = d.split_bin = 0;
-    d.bins = B;
-    d.cmin = d.ext = 0.0f;
-    d.n_lt = 0;
-    d.child_task[0] = d.child_task[1] = kNone;
-    d.child_leaf[0] = d.child_leaf[1] = 0;
-    d.pad = 0;
-    Cand win;
-    if (!leaf) {
-        uint32_t cnt[3];
-        float box[3][6];
-        bool axis_ok[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const uint32_t* bw = tb + (a * 32 + lane) * 7;
-            cnt[a] = bw[0];
-            for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
-            axis_ok[a] = !(ext[a] == 0.0f);
-        }
-        Cand best;
-        binned_candidates(cnt, box, axis_ok, B, t.len, surface_area6(nb), P, lane, best);
-        const uint64_t wk = warp_min_key(best.key);
-        const uint32_t wlo = static_cast<uint32_t>(wk);
-        if (wlo == kNoKey) {
-            if (t.len > P.max_leaf) {
-                if (lane == 0) set_error(O.ctr, MGBVH_ERR_UNSUPPORTED, kSiteLargeMedian);
-                return;
-            }
-            leaf = true;
-        } else {
-            d.axis = (wlo >> 8) & 3u;
-            d.split_bin = wlo & 0xFFu;
-            win = best;
-            shfl_cand(win, d.split_bin);
-            const float cost = funkey(static_cast<uint32_t>(wk >> 32));
-            if (t.len <= P.max_leaf && cost >= leaf_cost(t.len)) leaf = true;
-        }
-    }
-    if (leaf) {
-        warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, 0u, lane);
-        if (lane == 0) {
-            A.dec[w] = d;
-            if (t.len > 1) {
-                atomicAdd(&O.ctr->holes, 1u);
-                if (t.depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
-            }
-        }
-        return;
-    }
-    d.kind = 0;
-    d.cmin = cmn[d.axis];
-    d.ext = ext[d.axis];
-    d.n_lt = win.n_lt;
-    for (int i = 0; i < 6; ++i) {
-        d.ltb[i] = win.lt[i];
-        d.gtb[i] = win.gt[i];
-    }
-    // lt count of every tile of the node, exclusive-scanned across tiles
     uint32_t carry = 0;
     for (uint32_t b0 = 0; b0 < t.ntiles; b0 += 32) {
         const uint32_t ti = b0 + lane;
         uint32_t v = 0;
         if (ti < t.ntiles) {
-            const uint32_t* h = A.tile_hist + (size_t)(d.axis * 32) * A.cap_tiles + t.tile0 + ti;
-            for (uint32_t b = 0; b < d.split_bin; ++b) v += h[(size_t)b * A.cap_tiles];
+            const uint32_t* h = hist + (size_t)row0 * A.cap_tiles + t.tile0 + ti;
+            for (uint32_t b = 0; b < nrows; ++b) v += h[(size_t)b * A.cap_tiles];
         }
         uint32_t inc = v;
 #pragma unroll
@@ -453,7 +399,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         const uint32_t slot = c == 0 ? t.pair : t.pair + 1u;
         const uint32_t pair = c == 0 ? t.pair + 2u : t.pair + 2u * n_gt;
         const uint32_t depth = t.depth + 1u;
-        const float* cb = c == 0 ? win.gt : win.lt;
+        const float* cb = c == 0 ? d.gtb : d.ltb;
         const bool cleaf = len <= 1u || depth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
         Task ct;
         for (int a = 0; a < 3; ++a) {
@@ -522,12 +468,395 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
     if (lane == 0) A.dec[w] = d;
 }
 
+__device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
+    const Task t = A.tasks[w];
+    const uint32_t* tb = A.bins + (size_t)w * kBinWords;
+    if (A.refine && lane == 0) A.refine[w].on = 0;  // before any return: nothing pending
+    float cmn[3], ext[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        cmn[a] = funkey(A.cbkeys[6 * w + a]);
+        ext[a] = __fsub_rn(funkey(A.cbkeys[6 * w + 3 + a]), cmn[a]);
+    }
+    const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    const uint32_t B = P.bins ? P.bins : 32u;
+    bool leaf = t.depth == P.max_depth || (t.len <= P.max_leaf && t.len < 2u * P.min_leaf);
+    Decision d;
+    d.kind = 1;
+    d.axis = d.split_bin = 0;
+    d.bins = B;
+    d.cmin = d.ext = 0.0f;
+    d.n_lt = 0;
+    d.child_task[0] = d.child_task[1] = kNone;
+    d.child_leaf[0] = d.child_leaf[1] = 0;
+    d.use_thr = 0;
+    d.thr = 0.0f;
+    d.plain_key = kNoKey;
+    Cand win;
+    uint32_t cnt[3] = {0, 0, 0};
+    if (!leaf) {
+        float box[3][6];
+        bool axis_ok[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const uint32_t* bw = tb + (a * 32 + lane) * 7;
+            cnt[a] = bw[0];
+            for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
+            axis_ok[a] = !(ext[a] == 0.0f);
+        }
+        Cand best;
+        binned_candidates(cnt, box, axis_ok, B, t.len, surface_area6(nb), P, lane, best);
+        const uint64_t wk = warp_min_key(best.key);
+        const uint32_t wlo = static_cast<uint32_t>(wk);
+        if (wlo == kNoKey) {
+            if (t.len > P.max_leaf) {
+                if (lane == 0) set_error(O.ctr, MGBVH_ERR_UNSUPPORTED, kSiteLargeMedian);
+                return;
+            }
+            leaf = true;
+        } else {
+            d.axis = (wlo >> 8) & 3u;
+            d.split_bin = wlo & 0xFFu;
+            d.plain_key = static_cast<uint32_t>(wk >> 32);
+            win = best;
+            shfl_cand(win, d.split_bin);
+            const float cost = funkey(d.plain_key);
+            if (t.len <= P.max_leaf && cost >= leaf_cost(t.len)) leaf = true;
+        }
+    }
+    if (leaf) {
+        warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, 0u, lane);
+        if (lane == 0) {
+            A.dec[w] = d;
+            if (t.len > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (t.depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+        }
+        return;
+    }
+    d.kind = 0;
+    d.cmin = cmn[d.axis];
+    d.ext = ext[d.axis];
+    d.n_lt = win.n_lt;
+    for (int i = 0; i < 6; ++i) {
+        d.ltb[i] = win.lt[i];
+        d.gtb[i] = win.gt[i];
+    }
+    if (A.lw && B == 32u) {
+        // the learned form: run the network; with proposals to score, the
+        // decision waits for the refine pass (lvl_eval2_kernel)
+        const float cb[6] = {cmn[0], cmn[1], cmn[2], funkey(A.cbkeys[6 * w + 3]),
+                             funkey(A.cbkeys[6 * w + 4]), funkey(A.cbkeys[6 * w + 5])};
+        float f[24];
+        node_features(nb, cb, t.len, t.depth, cnt, f);
+        int top0 = 0, top1 = 0;
+        float refine = 0.0f;
+        mgbvh_mlp::warp_forward_t(f, A.lw, lane, top0, top1, refine);
+        const bool on = !A.lgate || refine > 0.0f;
+        if (lane == 0) {
+            LvlRefine R;
+            R.on = on ? 1u : 0u;
+            R.prop[0] = (uint32_t)top0;
+            R.prop[1] = (uint32_t)top1;
+            R.pad = 0;
+            A.refine[w] = R;
+        }
+        if (on) {
+            uint32_t* rb = A.rbins + (size_t)w * kRBinWords;
+            for (uint32_t i = lane; i < kRBinWords; i += 32) {
+                const uint32_t f7 = i % 7u;
+                rb[i] = f7 == 0 ? 0u : (f7 <= 3 ? kKeyPosInf : kKeyNegInf);
+            }
+            if (lane == 0) A.dec[w] = d;
+            return;
+        }
+    }
+    emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u, d.split_bin);
+}
+
 __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_tasks; w += nwarps)
         eval_task(A, P, O, w, lane);
+}
+
+// Interval bins of the pending nodes: for each proposal, the node's objects
+// by the interval of their centroid among the proposal's 16 thresholds
+// (count + AABB keys), with shared-memory atomics, merged into the node's
+// global interval bins; per-tile counts go to tile_hist2. Grid-stride over
+// the level's tiles.
+__global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
+    const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys,
+    const LvlRefine* __restrict__ refine, uint32_t* __restrict__ rbins,
+    const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
+    uint32_t* __restrict__ tile_hist2, uint32_t cap_tiles, const Rec* __restrict__ rec0,
+    const Rec* __restrict__ rec1, const Counters* __restrict__ ctr, uint32_t lv) {
+    __shared__ uint32_t sb[kRBinWords];
+    __shared__ float sthr[32];
+    const uint32_t ntiles = ctr->lvl[lv][1];
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t ti = tile_task[tile];
+        const LvlRefine R = refine[ti];
+        if (!R.on) continue;  // block-uniform
+        __syncthreads();      // the previous tile's readers of sb are done
+        for (uint32_t i = threadIdx.x; i < kRBinWords; i += blockDim.x) {
+            const uint32_t f7 = i % 7u;
+            sb[i] = f7 == 0 ? 0u : (f7 <= 3 ? kKeyPosInf : kKeyNegInf);
+        }
+        uint32_t ax[2];
+        bool act[2];
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            ax[p] = min(R.prop[p] >> 4, 2u);
+            const float cmin = funkey(cbkeys[6 * ti + ax[p]]);
+            const float ext = __fsub_rn(funkey(cbkeys[6 * ti + 3 + ax[p]]), cmin);
+            act[p] = ext > 0.0f;
+            if (threadIdx.x >= 16u * p && threadIdx.x < 16u * (p + 1))
+                sthr[threadIdx.x] = proposal_threshold(cmin, ext, R.prop[p] & 15u, threadIdx.x & 15u);
+        }
+        __syncthreads();
+        const Task& t = tasks[ti];
+        const uint32_t begin = tile_begin[tile];
+        const uint32_t cnt = min(kTile, t.len - begin);
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            const float4 lo = src[i].lo, hi = src[i].hi;
+            const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+            for (int p = 0; p < 2; ++p) {
+                if (!act[p]) continue;  // block-uniform
+                const float c = center_of(l[ax[p]], h[ax[p]]);
+                // interval = number of thresholds thr with !(c < thr)
+                uint32_t lo_i = 0, hi_i = 16;
+#pragma unroll
+                for (int s = 0; s < 5; ++s) {
+                    if (lo_i < hi_i) {
+                        const uint32_t mid = (lo_i + hi_i) >> 1;
+                        if (!(c < sthr[16 * p + mid]))
+                            lo_i = mid + 1;
+                        else
+                            hi_i = mid;
+                    }
+                }
+                uint32_t* wd = sb + (p * 17 + lo_i) * 7;
+                atomicAdd(wd, 1u);
+                atomicMin(wd + 1, fkey(l[0]));
+                atomicMin(wd + 2, fkey(l[1]));
+                atomicMin(wd + 3, fkey(l[2]));
+                atomicMax(wd + 4, fkey(h[0]));
+                atomicMax(wd + 5, fkey(h[1]));
+                atomicMax(wd + 6, fkey(h[2]));
+            }
+        }
+        __syncthreads();
+        for (uint32_t r = threadIdx.x; r < 34; r += blockDim.x)
+            tile_hist2[(size_t)r * cap_tiles + tile] = sb[r * 7];
+        uint32_t* gb = rbins + (size_t)ti * kRBinWords;
+        for (uint32_t k = threadIdx.x; k < kRBinWords; k += blockDim.x) {
+            const uint32_t r = k / 7u, f7 = k % 7u;
+            if (sb[r * 7] == 0) continue;
+            if (f7 == 0)
+                atomicAdd(gb + k, sb[k]);
+            else if (f7 <= 3)
+                atomicMin(gb + k, sb[k]);
+            else
+                atomicMax(gb + k, sb[k]);
+        }
+    }
+}
+
+// Pending nodes: lane p * 16 + k scores threshold k of proposal p exactly
+// from the interval bins (lt = intervals 0..k, gt = k + 1..16); the first
+// minimum of (cost, axis, lane) replaces the binned split when strictly
+// cheaper; then the node and its children are written.
+__device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
+    const Task t = A.tasks[w];
+    Decision d = A.dec[w];
+    const LvlRefine R = A.refine[w];
+    const uint32_t p = lane >> 4, k = lane & 15u;
+    const uint32_t a = min(R.prop[p] >> 4, 2u);
+    const float cmin = funkey(A.cbkeys[6 * w + a]);
+    const float ext = __fsub_rn(funkey(A.cbkeys[6 * w + 3 + a]), cmin);
+    const float thr = proposal_threshold(cmin, ext, R.prop[p] & 15u, k);
+    const uint32_t* rb = A.rbins + (size_t)w * kRBinWords + p * 17u * 7u;
+    float lt[6], gt[6];
+    box_empty(lt);
+    box_empty(gt);
+    uint32_t nl = 0, ng = 0;
+    for (uint32_t j = 0; j < 17; ++j) {
+        const uint32_t* b = rb + j * 7;
+        const uint32_t c = b[0];
+        if (c == 0) continue;
+        float* bx = j <= k ? lt : gt;
+        if (j <= k)
+            nl += c;
+        else
+            ng += c;
+        box_grow(bx, funkey(b[1]), funkey(b[2]), funkey(b[3]), funkey(b[4]), funkey(b[5]), funkey(b[6]));
+    }
+    const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    uint64_t key = ~0ull;
+    if (ext > 0.0f && nl >= P.min_leaf && ng >= P.min_leaf)
+        key = cand_key(split_cost(surface_area6(lt), surface_area6(gt), surface_area6(nb), nl, ng), a, lane);
+    const uint64_t wk = warp_min_key(key);
+    const uint32_t wlo = static_cast<uint32_t>(wk);
+    if (wlo != kNoKey && static_cast<uint32_t>(wk >> 32) < d.plain_key) {
+        const uint32_t src = wlo & 0xFFu;
+        d.use_thr = 1;
+        d.axis = (wlo >> 8) & 3u;
+        d.thr = __shfl_sync(kFull, thr, src);
+        d.n_lt = __shfl_sync(kFull, nl, src);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            d.ltb[i] = __shfl_sync(kFull, lt[i], src);
+            d.gtb[i] = __shfl_sync(kFull, gt[i], src);
+        }
+        if (lane == 0) atomicAdd(&O.ctr->learned, 1u);
+        emit_split(A, P, O, w, lane, t, d, A.tile_hist2, (src >> 4) * 17u, (src & 15u) + 1u);
+    } else {
+        emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u, d.split_bin);
+    }
+}
+
+__global__ void __launch_bounds__(128) lvl_eval2_kernel(EvalArgs A, Params P, Out O) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_tasks; w += nwarps)
+        if (A.refine[w].on) eval2_task(A, P, O, w, lane);
+}
+
+// Training samples of the level-pass nodes of at most kSampleLargeMax
+// objects that took a binned split: one CTA per node computes the exact
+// full sweep (every centroid a threshold on every axis; first minimum of
+// (cost, axis, threshold)), one thread per threshold, the node's records
+// streamed through shared memory; warp 0 then writes the sample.
+constexpr uint32_t kSampleChunk = 1024;
+
+__global__ void __launch_bounds__(256) lvl_sample_kernel(const Task* __restrict__ tasks,
+                                                         const Decision* __restrict__ dec,
+                                                         const uint32_t* __restrict__ bins,
+                                                         const uint32_t* __restrict__ cbkeys,
+                                                         const Rec* __restrict__ rec0,
+                                                         const Rec* __restrict__ rec1,
+                                                         const Counters* __restrict__ ctr, uint32_t lv,
+                                                         Params P, Learn LN) {
+    __shared__ float3 slo[kSampleChunk], shi[kSampleChunk];
+    __shared__ uint32_t rk[8], ra[8], rt[8];
+    __shared__ float rthr[8];
+    const uint32_t n_tasks = ctr->lvl[lv][0];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if ((P.bins ? P.bins : 32u) != 32u) return;
+    for (uint32_t w = blockIdx.x; w < n_tasks; w += gridDim.x) {
+        const Task t = tasks[w];
+        const Decision d = dec[w];
+        if (d.kind != 0 || t.len > kSampleLargeMax) continue;  // block-uniform
+        const uint32_t n = t.len;
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+        const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+        const float sa_p = surface_area6(nb);
+        uint32_t bk = kNoKey, ba = 3, bt = kNoKey;
+        float bthr = 0.0f;
+        for (uint32_t a = 0; a < 3; ++a) {
+            for (uint32_t k0 = 0; k0 < n; k0 += blockDim.x) {
+                const uint32_t kk = k0 + threadIdx.x;
+                float thr = 0.0f;
+                if (kk < n) {
+                    const float* lo = reinterpret_cast<const float*>(&src[kk].lo);
+                    const float* hi = reinterpret_cast<const float*>(&src[kk].hi);
+                    thr = center_of(lo[a], hi[a]);
+                }
+                float blt[6], bgt[6];
+                box_empty(blt);
+                box_empty(bgt);
+                uint32_t nl = 0;
+                for (uint32_t c0 = 0; c0 < n; c0 += kSampleChunk) {
+                    const uint32_t m = min(kSampleChunk, n - c0);
+                    __syncthreads();
+                    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                        const Rec r = src[c0 + i];
+                        slo[i] = make_float3(r.lo.x, r.lo.y, r.lo.z);
+                        shi[i] = make_float3(r.hi.x, r.hi.y, r.hi.z);
+                    }
+                    __syncthreads();
+                    for (uint32_t j = 0; j < m; ++j) {
+                        const float3 l = slo[j], h = shi[j];
+                        const float cj = center_of(a == 0 ? l.x : (a == 1 ? l.y : l.z),
+                                                   a == 0 ? h.x : (a == 1 ? h.y : h.z));
+                        if (cj < thr) {
+                            box_grow(blt, l.x, l.y, l.z, h.x, h.y, h.z);
+                            nl++;
+                        } else {
+                            box_grow(bgt, l.x, l.y, l.z, h.x, h.y, h.z);
+                        }
+                    }
+                }
+                const uint32_t ng = n - nl;
+                if (kk < n && nl >= P.min_leaf && ng >= P.min_leaf) {
+                    const uint32_t ck = fkey(split_cost(surface_area6(blt), surface_area6(bgt), sa_p, nl, ng));
+                    const uint32_t tk = fkey(thr);
+                    if (ck < bk || (ck == bk && (a < ba || (a == ba && tk < bt)))) {
+                        bk = ck;
+                        ba = a;
+                        bt = tk;
+                        bthr = thr;
+                    }
+                }
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const uint32_t ok = __shfl_xor_sync(kFull, bk, off);
+            const uint32_t oa = __shfl_xor_sync(kFull, ba, off);
+            const uint32_t ot = __shfl_xor_sync(kFull, bt, off);
+            const float oth = __shfl_xor_sync(kFull, bthr, off);
+            if (ok < bk || (ok == bk && (oa < ba || (oa == ba && ot < bt)))) {
+                bk = ok;
+                ba = oa;
+                bt = ot;
+                bthr = oth;
+            }
+        }
+        if (lane == 0) {
+            rk[warp] = bk;
+            ra[warp] = ba;
+            rt[warp] = bt;
+            rthr[warp] = bthr;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            bk = lane < 8 ? rk[lane] : kNoKey;
+            ba = lane < 8 ? ra[lane] : 3u;
+            bt = lane < 8 ? rt[lane] : kNoKey;
+            bthr = lane < 8 ? rthr[lane] : 0.0f;
+            for (int off = 16; off > 0; off >>= 1) {
+                const uint32_t ok = __shfl_xor_sync(kFull, bk, off);
+                const uint32_t oa = __shfl_xor_sync(kFull, ba, off);
+                const uint32_t ot = __shfl_xor_sync(kFull, bt, off);
+                const float oth = __shfl_xor_sync(kFull, bthr, off);
+                if (ok < bk || (ok == bk && (oa < ba || (oa == ba && ot < bt)))) {
+                    bk = ok;
+                    ba = oa;
+                    bt = ot;
+                    bthr = oth;
+                }
+            }
+            float cb[6];
+            for (int a = 0; a < 6; ++a) cb[a] = funkey(cbkeys[6 * w + a]);
+            uint32_t cnt[3];
+            for (int a = 0; a < 3; ++a)
+                cnt[a] = cb[3 + a] - cb[a] == 0.0f ? 0u : bins[(size_t)w * kBinWords + (a * 32 + lane) * 7];
+            float f[24];
+            node_features(nb, cb, n, t.depth, cnt, f);
+            if (lane == 0) {
+                const float cmin_a = ba < 3 ? cb[ba] : 0.0f;
+                const float ext_a = ba < 3 ? __fsub_rn(cb[3 + ba], cb[ba]) : 0.0f;
+                write_sample(LN, f, bk, ba, bthr, cmin_a, ext_a, d.plain_key, n, t.start - t.tbase);
+            }
+        }
+    }
 }
 
 // Stable partition of the large nodes' records into the other buffer: lt
@@ -565,7 +894,8 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
             continue;
         }
         const uint32_t axis = d.axis, split_bin = d.split_bin, nbins = d.bins, n_lt = d.n_lt;
-        const float cmin = d.cmin, ext = d.ext;
+        const float cmin = d.cmin, ext = d.ext, thr = d.thr;
+        const bool use_thr = d.use_thr != 0;
         if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
         if (threadIdx.x == 0) sbad = 0;
         const uint32_t w0 = warp * (32u * kPartPerLane);
@@ -579,7 +909,8 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
             if (i < cnt) {
                 const float* lo = reinterpret_cast<const float*>(&src[i].lo);
                 const float* hi = reinterpret_cast<const float*>(&src[i].hi);
-                pred = bin_of(center_of(lo[axis], hi[axis]), cmin, ext, nbins) < split_bin;
+                const float c = center_of(lo[axis], hi[axis]);
+                pred = use_thr ? c < thr : bin_of(c, cmin, ext, nbins) < split_bin;
             }
             bal[j] = __ballot_sync(kFull, pred);
             lt_w += __popc(bal[j]);
@@ -823,40 +1154,19 @@ __device__ __noinline__ void learned_node(const MediumSmem& S, const Learn& LN, 
                 bthr = oth;
             }
         }
-        if (lane == 0) {
-            const uint32_t slot = atomicAdd(LN.count, 1u);
-            if (slot < LN.cap) {
-                float* out = LN.samples + (size_t)slot * kSampleWidth;
-                for (int j = 0; j < 24; ++j) out[j] = f[j];
-                uint32_t label = 0xFFFFFFFFu;
-                float gain = 0.0f;
-                if (bk != kNoKey && ext[ba] > 0.0f) {
-                    const float pct = (bthr - nd.cb[ba]) / ext[ba];
-                    int q = (int)floorf(pct * 16.0f);
-                    q = min(max(q, 0), 15);
-                    label = ba * 16u + (uint32_t)q;
-                    gain = bk < plain_ck ? 1.0f : 0.0f;
-                }
-                out[24] = __uint_as_float(label);
-                out[25] = gain;
-                out[26] = (float)n;
-                out[27] = funkey(plain_ck);
-                out[28] = bk == kNoKey ? __int_as_float(0x7F800000) : funkey(bk);
-                out[29] = (float)(base + s - tbase);
-            }
-        }
+        if (lane == 0)
+            write_sample(LN, f, bk, ba, bthr, ba < 3 ? nd.cb[ba] : 0.0f, ba < 3 ? ext[ba] : 0.0f,
+                         plain_ck, n, base + s - tbase);
     }
     if (LN.w) {
         int top0 = 0, top1 = 0;
         float refine = 0.0f;
-        mgbvh_mlp::warp_forward(f, LN.w, lane, top0, top1, refine);
+        mgbvh_mlp::warp_forward_t(f, LN.w, lane, top0, top1, refine);
         if (!LN.gate || refine > 0.0f) {
             const int prop = (lane >> 4) ? top1 : top0;
             const uint32_t pa = (uint32_t)prop >> 4, bucket = (uint32_t)prop & 15u;
             const uint32_t k = lane & 15u;
-            const float thr = __fadd_rn(nd.cb[pa], __fmul_rn(ext[pa], __fdiv_rn(
-                                                                           (float)(bucket * 16u + k + 1u),
-                                                                           256.0f)));
+            const float thr = proposal_threshold(nd.cb[pa], ext[pa], bucket, k);
             Cand c;
             score_threshold(fetch, n, pa, thr, ext[pa] > 0.0f, sa_p, P, c, lane);
             const uint64_t wk2 = warp_min_key(c.key);
@@ -870,6 +1180,15 @@ __device__ __noinline__ void learned_node(const MediumSmem& S, const Learn& LN, 
             }
         }
     }
+}
+
+// The builder's transposed copy of the network parameters (layout in
+// mgbvh_mlp.cuh); padding outputs are zero.
+__global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, __nv_bfloat16* __restrict__ t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mgbvh_mlp::kTParams) return;
+    const int src = mgbvh_mlp::transposed_source(i);
+    t[i] = src >= 0 ? w[src] : __float2bfloat16_rn(0.0f);
 }
 
 // One CTA builds the subtree of one medium node (33..1024 objects).
@@ -1536,8 +1855,10 @@ struct mgbvh_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<unsigned char> graph_sig;
     uint32_t graph_levels = 0, graph_launches = 0;
-    // learned split proposer (changes trees) and training-sample output
+    // learned split proposer (changes trees) and training-sample output;
+    // learn_w points into learn_wt, the transposed copy of the parameters
     const void* learn_w = nullptr;
+    DevBuf learn_wt, lref, rbins, tile_hist2;  // level-pass refine state (learned form)
     int learn_gate = 1;
     float* learn_samples = nullptr;
     uint32_t learn_cap = 0;
@@ -1652,6 +1973,12 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     uint32_t level = 0;
     bool more = has_large;
     if (!fixed_levels) ctx->h_ctr->error = 0;
+    Learn LN;
+    LN.w = static_cast<const __nv_bfloat16*>(ctx->learn_w);
+    LN.gate = ctx->learn_gate;
+    LN.samples = ctx->learn_samples;
+    LN.cap = ctx->learn_cap;
+    LN.count = ctx->learn_count;
     bool first_batch = true;
     while (more) {
         const uint32_t batch =
@@ -1684,7 +2011,25 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             A.cap_tiles = C.tiles;
             A.cap_medium = C.medium;
             A.cap_small = C.small;
+            A.lw = LN.w;
+            A.lgate = LN.gate;
+            A.refine = LN.w ? P_<LvlRefine>(ctx->lref) : nullptr;
+            A.rbins = LN.w ? P_<uint32_t>(ctx->rbins) : nullptr;
+            A.tile_hist2 = LN.w ? P_<uint32_t>(ctx->tile_hist2) : nullptr;
             lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+            if (LN.samples) {
+                lvl_sample_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(
+                    A.tasks, A.dec, A.bins, A.cbkeys, rec0, rec1, d_ctr, lv, P, LN);
+                launches++;
+            }
+            if (LN.w) {
+                lvl_refine_bin_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+                    A.tasks, A.cbkeys, A.refine, A.rbins, P_<uint32_t>(ctx->tile_task[lv]),
+                    P_<uint32_t>(ctx->tile_begin[lv]), P_<uint32_t>(ctx->tile_hist2), C.tiles, rec0, rec1,
+                    d_ctr, lv);
+                lvl_eval2_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+                launches += 2;
+            }
             lvl_part_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
                 P_<Task>(ctx->tasks[lv]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[lv]),
                 P_<uint32_t>(ctx->tile_begin[lv]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
@@ -1705,12 +2050,6 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
         const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
-        Learn LN;
-        LN.w = static_cast<const __nv_bfloat16*>(ctx->learn_w);
-        LN.gate = ctx->learn_gate;
-        LN.samples = ctx->learn_samples;
-        LN.cap = ctx->learn_cap;
-        LN.count = ctx->learn_count;
         medium_kernel<<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
             P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
         launches++;
@@ -1758,6 +2097,11 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     ENS(ctx->lens, 4ull * C.nodes);
     ENS(ctx->used, (size_t)C.nodes);
     ENS(ctx->ctr, sizeof(Counters));
+    if (ctx->learn_w) {
+        ENS(ctx->lref, sizeof(LvlRefine) * (size_t)C.tasks);
+        ENS(ctx->rbins, 4ull * kRBinWords * C.tasks);
+        ENS(ctx->tile_hist2, 4ull * 34 * C.tiles);  // [proposal * 17 + interval][tile]
+    }
 #undef ENS
     Params P;
     P.min_leaf = st->min_leaf_objects;
@@ -2115,6 +2459,11 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     ENS(ctx->toff_buf, 4ull * (nm + 1));
     ENS(ctx->noff_buf, 4ull * (nm + 1));
     ENS(ctx->mkeys, 48ull * nm);
+    if (ctx->learn_w) {
+        ENS(ctx->lref, sizeof(LvlRefine) * (size_t)C.tasks);
+        ENS(ctx->rbins, 4ull * kRBinWords * C.tasks);
+        ENS(ctx->tile_hist2, 4ull * 34 * C.tiles);
+    }
 #undef ENS
     if (B.n_large > C.tasks || B.tiles > C.tiles || B.n_medium > C.medium || B.n_small > C.small)
         return fail(ctx, MGBVH_ERR_CAPACITY, "batch root lists exceed their capacity");
@@ -2442,7 +2791,8 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->tile_lt, &ctx->dec, &ctx->medium, &ctx->small, &ctx->nodes, &ctx->lens,
                      &ctx->used, &ctx->newidx, &ctx->widened, &ctx->perm, &ctx->ctr, &ctx->cub_tmp, &ctx->in_a,
                      &ctx->in_b, &ctx->out_nodes, &ctx->out_lens, &ctx->mesh_buf,
-                     &ctx->toff_buf, &ctx->noff_buf, &ctx->mkeys};
+                     &ctx->toff_buf, &ctx->noff_buf, &ctx->mkeys, &ctx->learn_wt, &ctx->lref,
+                     &ctx->rbins, &ctx->tile_hist2};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
@@ -2550,15 +2900,21 @@ int mgbvh_build_batch_dev(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_
 }
 
 int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate) {
-    if (!ctx) return MGBVH_ERR_INVALID_ARG;
-    ctx->learn_w = d_weights_bf16;
-    ctx->learn_gate = gate != 0;
+    if (int rc = check_ctx(ctx)) return rc;
     if (ctx->graph_exec) {  // a captured graph holds the old switch
-        cudaSetDevice(ctx->device);
         cudaGraphExecDestroy(ctx->graph_exec);
         ctx->graph_exec = nullptr;
         ctx->graph_sig.clear();
     }
+    ctx->learn_w = nullptr;
+    ctx->learn_gate = gate != 0;
+    if (!d_weights_bf16) return MGBVH_OK;
+    if (int rc = ensure(ctx, ctx->learn_wt, sizeof(__nv_bfloat16) * mgbvh_mlp::kTParams)) return rc;
+    transpose_weights_kernel<<<(mgbvh_mlp::kTParams + 255) / 256, 256, 0, ctx->stream>>>(
+        static_cast<const __nv_bfloat16*>(d_weights_bf16), P_<__nv_bfloat16>(ctx->learn_wt));
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaStreamSynchronize(ctx->stream));  // the caller's buffer may go after this
+    ctx->learn_w = ctx->learn_wt.p;
     return MGBVH_OK;
 }
 

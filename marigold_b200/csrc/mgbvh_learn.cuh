@@ -24,6 +24,52 @@ struct Learn {
 };
 
 constexpr int kSampleWidth = 30;  // 24 features, label bits, gain, n, plain cost, full cost, start
+constexpr uint32_t kSampleLargeMax = 8192;  // level-pass nodes sampled up to this many objects
+
+// Threshold k (0..15) inside proposal bucket `bucket` (0..15) of an axis with
+// centroid range [cmin, cmin + ext]: cmin + ext * ((bucket * 16 + k + 1) / 256).
+// Nondecreasing in bucket * 16 + k.
+__device__ __forceinline__ float proposal_threshold(float cmin, float ext, uint32_t bucket, uint32_t k) {
+    return __fadd_rn(cmin, __fmul_rn(ext, __fdiv_rn((float)(bucket * 16u + k + 1u), 256.0f)));
+}
+
+// A level-pass node waiting for its proposals to be scored.
+struct LvlRefine {
+    uint32_t on;       // 1: proposals pending (the node's split is decided after the refine pass)
+    uint32_t prop[2];  // axis * 16 + bucket
+    uint32_t pad;
+};
+// interval bins of a pending level-pass node: [proposal][interval 0..16]{count, lo key xyz, hi key xyz};
+// interval j holds the centroids c with thr[j - 1] <= c < thr[j]
+constexpr uint32_t kRBinWords = 2 * 17 * 7;
+
+// One training sample (lane 0 of the calling warp): features f, the
+// full-sweep optimum (cost key bk, axis ba, threshold bthr; bk == kNoKey:
+// none), the centroid range of axis ba, the binned split's cost key, the
+// object count and the node's start in its object list.
+__device__ __forceinline__ void write_sample(const Learn& LN, const float* f, uint32_t bk, uint32_t ba,
+                                             float bthr, float cmin_a, float ext_a, uint32_t plain_ck,
+                                             uint32_t n, uint32_t start) {
+    const uint32_t slot = atomicAdd(LN.count, 1u);
+    if (slot >= LN.cap) return;
+    float* out = LN.samples + (size_t)slot * kSampleWidth;
+    for (int j = 0; j < 24; ++j) out[j] = f[j];
+    uint32_t label = 0xFFFFFFFFu;
+    float gain = 0.0f;
+    if (bk != kNoKey && ext_a > 0.0f) {
+        const float pct = (bthr - cmin_a) / ext_a;
+        int q = (int)floorf(pct * 16.0f);
+        q = min(max(q, 0), 15);
+        label = ba * 16u + (uint32_t)q;
+        gain = bk < plain_ck ? 1.0f : 0.0f;
+    }
+    out[24] = __uint_as_float(label);
+    out[25] = gain;
+    out[26] = (float)n;
+    out[27] = funkey(plain_ck);
+    out[28] = bk == kNoKey ? __int_as_float(0x7F800000) : funkey(bk);
+    out[29] = (float)start;
+}
 
 // Node features (every lane gets all 24). nb: node bounds; cb: centroid
 // bounds (lo xyz, hi xyz); cnt: this lane's 32-bin counts per axis (lane =

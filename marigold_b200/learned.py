@@ -49,6 +49,19 @@ def training_mesh(k: int, seed: int):
     return synth.noisy_icosphere([6, 7, 8][(k // 2) % 3], seed=s)
 
 
+# held-out evaluation meshes (seeds never drawn by training_mesh's streams):
+# the 65,536-triangle random mesh and the level-8 noisy icosphere generators
+EVAL_MESHES = (("random65536_s9001", "random", 65536, 9001),
+               ("icosphere8_s9002", "icosphere", 8, 9002))
+
+
+def eval_mesh(kind: str, size: int, seed: int):
+    from . import synth
+    if kind == "random":
+        return synth.random_triangles(size, seed=seed)
+    return synth.noisy_icosphere(size, seed=seed)
+
+
 def generate_samples(n_target: int, seed: int = 424242, ctx=None, log=print, workers: int = 0):
     """GPU-built training samples: float32 [K, 30] (torch, on the device).
 
@@ -182,7 +195,16 @@ def accuracy(samples, bits):
 
 
 def load_weights() -> np.ndarray:
-    return np.fromfile(WEIGHTS, dtype=np.uint16)
+    """The committed trained parameters (8,945 BF16 values as uint16)."""
+    w = np.fromfile(WEIGHTS, dtype=np.uint16)
+    if w.shape[0] != NPARAM:
+        raise ValueError(f"{WEIGHTS}: {w.shape[0]} values, expected {NPARAM}")
+    return w
+
+
+def load_record() -> dict:
+    with open(RECORD) as f:
+        return json.load(f)
 
 
 def main():
