@@ -1192,6 +1192,7 @@ __global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, __
 }
 
 // One CTA builds the subtree of one medium node (33..1024 objects).
+template <bool kLearn>
 __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* rec0, Rec* rec1,
                                             Task* small, uint32_t cap_small, const Params& P,
                                             const Out& O, const Learn& LN) {
@@ -1314,11 +1315,13 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
                     const float cost = funkey(static_cast<uint32_t>(wk >> 32));
                     if (n <= P.max_leaf && cost >= leaf_cost(n)) leaf = true;
                     n_lt = win.n_lt;
-                    if (!leaf && (LN.w || LN.samples) && B == 32u)
-                        learned_node(S, LN, P, nd, ib, base, s, n, depth, t.tbase, cnt, ext,
-                                     static_cast<uint32_t>(wk >> 32), lane, win, axis, n_lt,
-                                     use_thr);
-                    if (use_thr && lane == 0) atomicAdd(&O.ctr->learned, 1u);
+                    if constexpr (kLearn) {
+                        if (!leaf && (LN.w || LN.samples) && B == 32u)
+                            learned_node(S, LN, P, nd, ib, base, s, n, depth, t.tbase, cnt, ext,
+                                         static_cast<uint32_t>(wk >> 32), lane, win, axis, n_lt,
+                                         use_thr);
+                        if (use_thr && lane == 0) atomicAdd(&O.ctr->learned, 1u);
+                    }
                 }
             }
             if (leaf) {
@@ -1488,6 +1491,9 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
     }
 }
 
+// kLearn: with the learned form's hook (network proposals, training samples);
+// plain builds run the instantiation without it.
+template <bool kLearn>
 __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
@@ -1497,7 +1503,7 @@ __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __re
     const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
     for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
         __syncthreads();
-        medium_task(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
+        medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
     }
 }
 
@@ -2050,8 +2056,12 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
         const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
-        medium_kernel<<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
-            P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
+        if (LN.w || LN.samples)
+            medium_kernel<true><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
+        else
+            medium_kernel<false><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
         launches++;
         if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
         // small subtrees: count read on the device; grid sized for full occupancy
@@ -2772,7 +2782,9 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
         cudaEventCreate(&ctx->evp[0]) != cudaSuccess || cudaEventCreate(&ctx->evp[1]) != cudaSuccess ||
         cudaEventCreate(&ctx->evp[2]) != cudaSuccess ||
         cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
-        cudaFuncSetAttribute(medium_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(medium_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmem)) != cudaSuccess ||
+        cudaFuncSetAttribute(medium_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(MediumSmem)) != cudaSuccess) {
         mgbvh_destroy(ctx);
         return MGBVH_ERR_CUDA;
@@ -3029,7 +3041,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
         if (!g_noalloc_addr[dev]) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MGBVH_ERR_CUDA;
-            if (cudaFuncSetAttribute(medium_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            if (cudaFuncSetAttribute(medium_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(MediumSmem)) != cudaSuccess)
                 return MGBVH_ERR_CUDA;
             int n_sm = 0;
@@ -3071,7 +3083,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
                                                       nullptr, nullptr, S->medium, S->small, O, 0u,
                                                       st->max_depth);
     if (cls == 2)
-        medium_kernel<<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
+        medium_kernel<false><<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
             S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr});
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
