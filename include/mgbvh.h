@@ -309,9 +309,10 @@ MGBVH_API int mgbvh_trace_bruteforce_dev(mgbvh_tracer* tracer, const float* d_ra
 /*
  * Learned split proposer (no counterpart in the reference). A small MLP,
  * 24 -> 64 -> 64 -> 49 with GELU, BF16 parameters and FP32 accumulation,
- * proposes split positions for nodes of 33..1024 objects; the builder scores
- * the proposals exactly with the reference's cost formula and keeps the plain
- * split unless a proposal costs less (mgbvh_set_split_proposer). Parameters:
+ * proposes two (axis, 1/16 position bucket) candidates at every binned node
+ * of 33 or more objects; the builder scores 16 thresholds inside each
+ * candidate exactly with the reference's cost formula and keeps the plain
+ * split unless one costs strictly less (mgbvh_set_split_proposer). Parameters:
  * MGBVH_MLP_PARAMS values, W1[64x24] b1[64] W2[64x64] b2[64] W3[49x64] b3[49].
  * Training on the GPU: the caller zeroes d_grad and d_loss, calls
  * mgbvh_mlp_train_step_dev over a batch (features B x 24 f32, labels B u32 =
@@ -333,7 +334,7 @@ MGBVH_API int mgbvh_mlp_adam_dev(float* d_master, void* d_weights_bf16, const fl
                                  float beta2, float eps, void* cuda_stream);
 
 /* Builds on this context use the learned split proposer at every binned node
-   of 33..1024 objects (d_weights_bf16: MGBVH_MLP_PARAMS BF16 values on the
+   of 33 or more objects (d_weights_bf16: MGBVH_MLP_PARAMS BF16 values on the
    device, copied by this call, which returns once the copy is done; NULL
    turns the proposer off). gate != 0: only where the network's refine logit
    is positive. The trees then differ from the reference's (the plain split
@@ -341,8 +342,10 @@ MGBVH_API int mgbvh_mlp_adam_dev(float* d_master, void* d_weights_bf16, const fl
 MGBVH_API int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate);
 /* Builds on this context also write one training sample (30 floats: 24
    features, label bits, gain, n, plain cost, full-sweep cost, node start) per
-   binned node of 33..1024 objects to d_samples (device, capacity samples) and
-   count them in *d_count (device; the caller zeroes it). NULL turns it off. */
+   binned node of 33..8192 objects to d_samples (device, capacity samples) and
+   count them in *d_count (device; the caller zeroes it). The label is the
+   exact full sweep's optimum (every centroid a threshold on every axis),
+   computed by the builder. NULL turns it off. */
 MGBVH_API int mgbvh_set_sample_output(mgbvh_ctx* ctx, float* d_samples, uint32_t capacity,
                                       uint32_t* d_count);
 
