@@ -374,14 +374,16 @@ def run_reference(args):
 def run_mixed(args):
     """The large mixed scene: 16,777,216 triangles (8,388,608 in 64 Gaussian
     blobs, a 2048 x 1024-quad ground grid, 4,194,304 thin 1:200 triangles),
-    built with the reference profile, then 8,388,608 closest-hit rays with
-    origins uniform in the scene box grown by 10% and uniform directions. The
-    traversal is checked hit for hit against GPU brute force on a
-    65,536-ray subset (the brute-force kernel is itself checked against the
-    CPU oracle by the test suite)."""
+    built twice, plain (the reference profile) and learned (the committed
+    split proposer, refine gate on), then 8,388,608 closest-hit rays with
+    origins uniform in the scene box grown by 10% and uniform directions on
+    each tree. Each traversal is checked hit for hit against GPU brute force
+    on a 65,536-ray subset (the brute-force kernel is itself checked against
+    the CPU oracle by the test suite)."""
     import ctypes
     import torch
-    from marigold_b200 import BvhSettings, _lib, build_device, synth
+    from marigold_b200 import BvhSettings, _lib, build_device, learned, synth
+    from marigold_b200.bvh import NODE_DTYPE, sah_cost
     torch.cuda.set_device(0)
     t0 = time.perf_counter()
     sc = max(1, args.mixed_scale)
@@ -391,10 +393,11 @@ def run_mixed(args):
 
     v, t = synth.mixed_scene(n_blob=8388608 // sc, grid=(2048, 1024 // sc), n_thin=4194304 // sc)
     n = t.shape[0]
-    rays = synth.rays_in_box(8388608 // sc, v.min(0), v.max(0))
+    rays = synth.rays_in_box(8388608 // sc, v[:, :3].min(0), v[:, :3].max(0))
     gen_s = time.perf_counter() - t0
     log(f"generated {n} triangles, {rays.shape[0]} rays")
     ctx = _lib.Context(0)
+    ctx.set_tuning(1024)
     dv = torch.from_numpy(v).cuda()
     dt = torch.from_numpy(t.view(np.int32)).cuda()
     cap = 2 * n - 1
@@ -404,65 +407,77 @@ def run_mixed(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
     settings = BvhSettings(name="mixed", max_depth=32)
-    build_ms, count, st = [], 0, {}
-    for k in range(max(args.warmup, 1) + args.steps):
-        flush.fill_(k & 0xFF)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        count, rc, st = build_device(ctx, settings, d_nodes, d_perm, vertices=dv, triangles=dt,
-                                     out_lens=d_lens, stream=stream)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if k >= max(args.warmup, 1):
-            build_ms.append(e0.elapsed_time(e1))
-        log(f"build {k}: {e0.elapsed_time(e1):.2f} ms, {count} nodes, height {st.get('height')}")
+    weights = torch.from_numpy(learned.load_weights().view(np.int16)).cuda()
+    dr = torch.from_numpy(rays).cuda()
+    m = rays.shape[0]
+    sub = min(65536, m)
     tr = _lib.Tracer(0)
     L = tr.L
     sp = ctypes.c_void_p(stream.cuda_stream)
-    vp = lambda x: ctypes.c_void_p(x.data_ptr())
-    tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 12, v.shape[0],
-                                         vp(dt), vp(d_perm), n, sp))
-    dr = torch.from_numpy(rays).cuda()
-    m = rays.shape[0]
+    vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
     ht = torch.empty(m, dtype=torch.float32, device="cuda")
     hp = torch.empty(m, dtype=torch.int32, device="cuda")
-    counts = (ctypes.c_uint64 * 3)()
-    secs = ctypes.c_double(0)
-    trace_ms = []
-    for k in range(max(args.warmup, 1) + args.steps):
-        flush.fill_(k & 0xFF)
-        tr.check(L.mgbvh_trace_closest_dev(tr.ptr, vp(dr), m, vp(ht), vp(hp), counts,
-                                           ctypes.byref(secs), sp))
-        if k >= max(args.warmup, 1):
-            trace_ms.append(secs.value * 1e3)
-        log(f"trace {k}: {secs.value * 1e3:.2f} ms, counts {list(counts)}")
-    # check: 65,536-ray subset against GPU brute force, 16 rays against the CPU
-    sub = min(65536, m)
     bt = torch.empty(sub, dtype=torch.float32, device="cuda")
     bp = torch.empty(sub, dtype=torch.int32, device="cuda")
-    tb = time.perf_counter()
-    tr.check(L.mgbvh_trace_bruteforce_dev(tr.ptr, vp(dr), sub, vp(bt), vp(bp), sp))
-    brute_s = time.perf_counter() - tb
-    log(f"brute force {sub} rays: {brute_s:.1f} s")
-    gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
-    btn, bpn = bt.cpu().numpy(), bp.cpu().numpy().view(np.uint32)
-    mism = int(((gp != bpn) | (gt.view(np.uint32) != btn.view(np.uint32))).sum())
-    hits = int((hp.cpu().numpy().view(np.uint32) != 0xFFFFFFFF).sum())
-    bms = float(np.mean(build_ms))
-    tms = float(np.mean(trace_ms))
+    forms = {}
+    brute = None
+    for form in ("plain", "learned"):
+        ctx.set_split_proposer(weights if form == "learned" else None, True)
+        build_ms, count, st = [], 0, {}
+        for k in range(max(args.warmup, 1) + args.steps):
+            flush.fill_(k & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            count, rc, st = build_device(ctx, settings, d_nodes, d_perm, vertices=dv, triangles=dt,
+                                         out_lens=d_lens, stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ctx.check(rc)
+            if k >= max(args.warmup, 1):
+                build_ms.append(e0.elapsed_time(e1))
+            log(f"{form} build {k}: {e0.elapsed_time(e1):.2f} ms, {count} nodes")
+        sah = sah_cost(d_nodes[: count * 8].cpu().numpy().view(NODE_DTYPE),
+                       d_lens[:count].cpu().numpy().view(np.uint32))
+        tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 4 * v.shape[1], v.shape[0],
+                                             vp(dt), vp(d_perm), n, sp))
+        counts = (ctypes.c_uint64 * 3)()
+        secs = ctypes.c_double(0)
+        trace_ms = []
+        for k in range(max(args.warmup, 1) + args.steps):
+            flush.fill_(k & 0xFF)
+            tr.check(L.mgbvh_trace_closest_dev(tr.ptr, vp(dr), m, vp(ht), vp(hp), counts,
+                                               ctypes.byref(secs), sp))
+            if k >= max(args.warmup, 1):
+                trace_ms.append(secs.value * 1e3)
+            log(f"{form} trace {k}: {secs.value * 1e3:.2f} ms")
+        if brute is None:  # the closest hit does not depend on the tree
+            tb = time.perf_counter()
+            tr.check(L.mgbvh_trace_bruteforce_dev(tr.ptr, vp(dr), sub, vp(bt), vp(bp), sp))
+            torch.cuda.synchronize()
+            brute = (bt.cpu().numpy(), bp.cpu().numpy().view(np.uint32), time.perf_counter() - tb)
+            log(f"brute force {sub} rays: {brute[2]:.1f} s")
+        gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
+        mism = int(((gp != brute[1]) | (gt.view(np.uint32) != brute[0].view(np.uint32))).sum())
+        bms, tms = float(np.mean(build_ms)), float(np.mean(trace_ms))
+        forms[form] = {
+            "build": {"value": round(n / (bms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms": round(bms, 3),
+                      "nodes": count, "height": st.get("height"), "sah": round(sah, 4),
+                      "learned_splits": st.get("learned_splits"),
+                      "phase_ms": [round(x * 1e3, 3) for x in st.get("phase_seconds", [])]},
+            "trace": {"value": round(m / (tms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms": round(tms, 3),
+                      "hit_rays": int((hp != -1).sum().item()), "nodes_visited": counts[0],
+                      "box_tests": counts[1], "triangle_tests": counts[2]},
+            "check": {"subset_rays": sub, "mismatches_vs_gpu_bruteforce": mism},
+        }
+    ctx.set_split_proposer(None)
     out = {
         "metric": "BVH build Mtri/s; closest-hit Mrays/s", "workload": "mixed scene",
         "config": {"triangles": n, "rays": m, "blobs": 64, "grid_quads": [2048, 1024 // sc],
                    "thin": 4194304 // sc, "scale": sc, "max_depth": 32, "leaf": 1,
-                   "profile": "reference"},
-        "build": {"value": round(n / (bms * 1e-3) / 1e6, 2), "unit": "Mtri/s",
-                  "ms": round(bms, 3), "nodes": count, "height": st.get("height"),
-                  "phase_ms": [round(x * 1e3, 3) for x in st.get("phase_seconds", [])]},
-        "trace": {"value": round(m / (tms * 1e-3) / 1e6, 2), "unit": "Mrays/s",
-                  "ms": round(tms, 3), "hit_rays": hits,
-                  "nodes_visited": counts[0], "box_tests": counts[1], "triangle_tests": counts[2]},
-        "check": {"subset_rays": sub, "mismatches_vs_gpu_bruteforce": mism,
-                  "bruteforce_s": round(brute_s, 2)},
+                   "profile": "reference", "learned": "committed proposer, gate on"},
+        "build": forms["plain"]["build"], "trace": forms["plain"]["trace"],
+        "check": dict(forms["plain"]["check"], bruteforce_s=round(brute[2], 2)),
+        "learned": forms["learned"],
         "steps": args.steps, "warmup": args.warmup, "generation_s": round(gen_s, 1),
         "l2": "flushed before every build and trace",
     }
@@ -535,16 +550,17 @@ def run_batched(args):
     print(json.dumps(out), flush=True)
 
 
-def _trace_rate(tr, d_nodes, count, dv, nv, dt, d_perm, n, dr, m, stream, flush, reps):
+def _trace_rate(tr, d_nodes, count, dv, dt, d_perm, n, dr, m, stream, flush, reps, check=4096):
     """Closest-hit Mrays/s of one built tree (median of reps traces, L2
-    flushed before each) and the number of rays that hit."""
+    flushed before each), the number of rays that hit, and the number of the
+    first `check` rays whose hit differs from GPU brute force."""
     import ctypes
     import torch
     L = tr.L
     sp = ctypes.c_void_p(stream.cuda_stream)
     vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
-    tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 12, nv, vp(dt),
-                                         vp(d_perm), n, sp))
+    tr.check(L.mgbvh_tracer_set_blas_dev(tr.ptr, vp(d_nodes), count, None, vp(dv), 4 * dv.shape[1],
+                                         dv.shape[0], vp(dt), vp(d_perm), n, sp))
     ht = torch.empty(m, dtype=torch.float32, device="cuda")
     hp = torch.empty(m, dtype=torch.int32, device="cuda")
     counts = (ctypes.c_uint64 * 3)()
@@ -557,7 +573,13 @@ def _trace_rate(tr, d_nodes, count, dv, nv, dt, d_perm, n, dr, m, stream, flush,
         if k:
             ms.append(secs.value * 1e3)
     hits = int((hp != -1).sum().item())
-    return m / (statistics.median(ms) * 1e-3) / 1e6, hits, list(counts)
+    c = min(check, m)
+    bt = torch.empty(c, dtype=torch.float32, device="cuda")
+    bp = torch.empty(c, dtype=torch.int32, device="cuda")
+    tr.check(L.mgbvh_trace_bruteforce_dev(tr.ptr, vp(dr), c, vp(bt), vp(bp), sp))
+    torch.cuda.synchronize()
+    mism = int(((hp[:c] != bp) | (ht[:c].view(torch.int32) != bt.view(torch.int32))).sum().item())
+    return m / (statistics.median(ms) * 1e-3) / 1e6, hits, mism
 
 
 def run_learned(args):
@@ -615,13 +637,13 @@ def run_learned(args):
                     ms.append(e0.elapsed_time(e1))
             nh = d_nodes[: count * 8].cpu().numpy().view(NODE_DTYPE)
             sah = sah_cost(nh, d_lens[:count].cpu().numpy().view(np.uint32))
-            mrays, hits, _ = _trace_rate(tr, d_nodes, count, dv, v.shape[0], dt, d_perm, n, dr,
-                                         rays.shape[0], stream, flush, 5)
+            mrays, hits, mism = _trace_rate(tr, d_nodes, count, dv, dt, d_perm, n, dr, rays.shape[0],
+                                            stream, flush, 5)
             bms = statistics.median(ms)
             row[form] = {"build_mtris": round(n / (bms * 1e-3) / 1e6, 2), "build_ms": round(bms, 3),
                          "sah": round(sah, 4), "vs_full_sweep_pct": round(100 * (sah / full - 1), 4),
                          "learned_splits": st["learned_splits"], "mrays": round(mrays, 2),
-                         "hit_rays": hits}
+                         "hit_rays": hits, "trace_mismatches_vs_bruteforce_4096": mism}
             if form == "plain":
                 plain_sah = sah
             else:
