@@ -43,7 +43,7 @@ namespace mgbvh {
 constexpr uint32_t kMediumMax = 1024;
 constexpr uint32_t kTile = 2048;
 constexpr int kTileThreads = 256;
-constexpr int kMediumWarps = 8;
+constexpr int kMediumWarps = 4;
 constexpr int kMediumThreads = kMediumWarps * 32;
 constexpr uint32_t kBinWords = 3 * 32 * 7;  // [axis][bin]{count, lo key xyz, hi key xyz}
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -2055,7 +2055,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
     if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
-        const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 2u);
+        const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 4u);
         if (LN.w || LN.samples)
             medium_kernel<true><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
                 P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
