@@ -47,7 +47,6 @@ constexpr int kMediumWarps = 4;
 constexpr int kMediumThreads = kMediumWarps * 32;
 constexpr uint32_t kBinWords = 3 * 32 * 7;  // [axis][bin]{count, lo key xyz, hi key xyz}
 constexpr uint32_t kNone = 0xFFFFFFFFu;
-constexpr uint32_t kMediumListCap = kMediumMax / (kSmallMax + 1) + 1;
 
 struct Rec {
     float4 lo;  // min xyz, object id (bits)
@@ -997,19 +996,29 @@ struct MNodeExtra {
     uint32_t depth, ib;
 };
 
-struct MediumSmem {
-    float4 rlo[kMediumMax];
-    float4 rhi[kMediumMax];
-    uint16_t idx[2][kMediumMax];
-    MNode list[2][kMediumListCap];
-    MNodeExtra list_x[2][kMediumListCap];
+// Shared memory of one subtree CTA for subtrees of up to kCap objects: the
+// records, two index lists, two node lists (every listed node holds more than
+// 32 objects and the nodes of one list are disjoint, so kCap / 33 + 1 entries
+// suffice), per-warp bins and exchange space.
+template <uint32_t kCap>
+struct MediumSmemT {
+    static constexpr uint32_t kListCap = kCap / (kSmallMax + 1) + 1;
+    float4 rlo[kCap];
+    float4 rhi[kCap];
+    uint16_t idx[2][kCap];
+    MNode list[2][kListCap];
+    MNodeExtra list_x[2][kListCap];
     uint32_t bins[kMediumWarps][kBinWords];
     XRec xchg[kMediumWarps][32];
     uint32_t list_n[2];
     uint32_t rootk[12];
 };
+using MediumSmem = MediumSmemT<kMediumMax>;
+constexpr uint32_t kMediumSmallCap = 512;  // the instance for medium_max <= 512 (more CTAs per SM)
+using MediumSmemSmall = MediumSmemT<kMediumSmallCap>;
 
-__device__ __forceinline__ void medium_load_warp_records(const MediumSmem& S, uint32_t ib, uint32_t s,
+template <class MS>
+__device__ __forceinline__ void medium_load_warp_records(const MS& S, uint32_t ib, uint32_t s,
                                                          uint32_t n, uint32_t lane, float* lo,
                                                          float* hi, uint32_t& id) {
     if (lane < n) {
@@ -1029,7 +1038,8 @@ __device__ __forceinline__ void medium_load_warp_records(const MediumSmem& S, ui
 }
 
 // Warp: finish a leaf of the medium subtree (record + permutation).
-__device__ __forceinline__ void medium_leaf(const MediumSmem& S, uint32_t ib, uint32_t base,
+template <class MS>
+__device__ __forceinline__ void medium_leaf(const MS& S, uint32_t ib, uint32_t base,
                                             uint32_t s, uint32_t n, uint32_t slot, uint32_t depth,
                                             const float* b, uint32_t nbase, uint32_t tbase,
                                             const Params& P, const Out& O, uint32_t lane) {
@@ -1044,8 +1054,8 @@ __device__ __forceinline__ void medium_leaf(const MediumSmem& S, uint32_t ib, ui
 
 // Warp: stable partition of [s, s+n) from idx[ib] into idx[ib^1] by pred(p);
 // returns the lt count; accumulates child centroid keys.
-template <class Pred>
-__device__ __forceinline__ uint32_t medium_partition(MediumSmem& S, uint32_t ib, uint32_t s,
+template <class MS, class Pred>
+__device__ __forceinline__ uint32_t medium_partition(MS& S, uint32_t ib, uint32_t s,
                                                      uint32_t n, uint32_t n_lt_expect, uint32_t lane,
                                                      Pred pred, uint32_t* k /*12*/) {
     const uint32_t below = (1u << lane) - 1u;
@@ -1097,7 +1107,8 @@ __device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
 //  * with LN.w: run the network, score 16 thresholds inside each of its two
 //    best (axis, bucket) proposals exactly (one per lane), and replace the
 //    plain split when the best of them costs strictly less.
-__device__ __noinline__ void learned_node(const MediumSmem& S, const Learn& LN, const Params& P,
+template <class MS>
+__device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Params& P,
                                           const MNode& nd, uint32_t ib, uint32_t base, uint32_t s,
                                           uint32_t n, uint32_t depth, uint32_t tbase,
                                           const uint32_t* cnt, const float* ext,
@@ -1192,8 +1203,8 @@ __global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, __
 }
 
 // One CTA builds the subtree of one medium node (33..1024 objects).
-template <bool kLearn>
-__device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* rec0, Rec* rec1,
+template <bool kLearn, class MS>
+__device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec* rec1,
                                             Task* small, uint32_t cap_small, const Params& P,
                                             const Out& O, const Learn& LN) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -1493,13 +1504,13 @@ __device__ __forceinline__ void medium_task(MediumSmem& S, const Task t, Rec* re
 
 // kLearn: with the learned form's hook (network proposals, training samples);
 // plain builds run the instantiation without it.
-template <bool kLearn>
+template <bool kLearn, uint32_t kCap>
 __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
                                                                 Learn LN) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MediumSmem& S = *reinterpret_cast<MediumSmem*>(smem_raw);
+    MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
     const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
     for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
         __syncthreads();
@@ -2056,11 +2067,21 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     if (fixed_levels || !ctx->h_ctr->error) {
         // medium subtrees: count read on the device
         const uint32_t mgrid = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 4u);
-        if (LN.w || LN.samples)
-            medium_kernel<true><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+        // subtrees hold at most P.medium_max objects: the smaller-capacity
+        // instance leaves room for more CTAs per SM
+        const bool lrn = LN.w || LN.samples, small_cap = P.medium_max <= kMediumSmallCap;
+        const uint32_t mgrid_s = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 5u);
+        if (lrn && small_cap)
+            medium_kernel<true, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
+                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
+        else if (lrn)
+            medium_kernel<true, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
+        else if (small_cap)
+            medium_kernel<false, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
                 P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
         else
-            medium_kernel<false><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+            medium_kernel<false, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
                 P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
         launches++;
         if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
@@ -2782,10 +2803,16 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
         cudaEventCreate(&ctx->evp[0]) != cudaSuccess || cudaEventCreate(&ctx->evp[1]) != cudaSuccess ||
         cudaEventCreate(&ctx->evp[2]) != cudaSuccess ||
         cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
-        cudaFuncSetAttribute(medium_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(MediumSmem)) != cudaSuccess ||
-        cudaFuncSetAttribute(medium_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmem)) != cudaSuccess) {
+        cudaFuncSetAttribute(medium_kernel<true, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmem)) != cudaSuccess ||
+        cudaFuncSetAttribute(medium_kernel<false, kMediumSmallCap>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmemSmall)) != cudaSuccess ||
+        cudaFuncSetAttribute(medium_kernel<true, kMediumSmallCap>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmemSmall)) != cudaSuccess) {
         mgbvh_destroy(ctx);
         return MGBVH_ERR_CUDA;
     }
@@ -3041,7 +3068,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
         if (!g_noalloc_addr[dev]) {
             void* p = nullptr;
             if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MGBVH_ERR_CUDA;
-            if (cudaFuncSetAttribute(medium_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            if (cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(MediumSmem)) != cudaSuccess)
                 return MGBVH_ERR_CUDA;
             int n_sm = 0;
@@ -3083,7 +3110,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
                                                       nullptr, nullptr, S->medium, S->small, O, 0u,
                                                       st->max_depth);
     if (cls == 2)
-        medium_kernel<false><<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
+        medium_kernel<false, kMediumMax><<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
             S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr});
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
