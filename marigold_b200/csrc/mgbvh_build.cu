@@ -278,13 +278,19 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
 
 // Per-tile bin histograms (count + AABB per axis and bin) of the large nodes
 // with shared-memory atomics, merged into the node's global bins. Grid-stride over
-// the level's tiles; the tile count is read on the device.
+// the level's tiles; the tile count is read on the device. Each thread loads
+// its records of the tile first (kTile / kTileThreads of them), then bins
+// them. Also zeroes the next level's task and tile counts (the previous
+// level's kernels, which read them, have finished).
+constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
+
 __global__ void __launch_bounds__(kTileThreads) lvl_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* __restrict__ bins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
     uint32_t* __restrict__ tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
-    const Rec* __restrict__ rec1, const Counters* __restrict__ ctr, uint32_t lv, Params P) {
+    const Rec* __restrict__ rec1, Counters* __restrict__ ctr, uint32_t lv, Params P) {
     __shared__ uint32_t sb[kBinWords];
+    if (blockIdx.x == 0 && threadIdx.x < 2) ctr->lvl[lv ^ 1u][threadIdx.x] = 0;
     const uint32_t ntiles = ctr->lvl[lv][1];
     const uint32_t B = P.bins ? P.bins : 32u;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -301,10 +307,20 @@ __global__ void __launch_bounds__(kTileThreads) lvl_bin_kernel(
             cmn[a] = funkey(cbkeys[6 * ti + a]);
             ext[a] = __fsub_rn(funkey(cbkeys[6 * ti + 3 + a]), cmn[a]);
         }
+        float4 rl[kRecsPerThread], rh[kRecsPerThread];
+#pragma unroll
+        for (uint32_t k = 0; k < kRecsPerThread; ++k) {
+            const uint32_t i = threadIdx.x + k * kTileThreads;
+            if (i < cnt) {
+                rl[k] = src[i].lo;
+                rh[k] = src[i].hi;
+            }
+        }
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-            const float4 lo = src[i].lo, hi = src[i].hi;
-            const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
+#pragma unroll
+        for (uint32_t k = 0; k < kRecsPerThread; ++k) {
+            if (threadIdx.x + k * kTileThreads >= cnt) break;
+            const float l[3] = {rl[k].x, rl[k].y, rl[k].z}, h[3] = {rh[k].x, rh[k].y, rh[k].z};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (ext[a] == 0.0f) continue;  // block-uniform
@@ -898,17 +914,25 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
         if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
         if (threadIdx.x == 0) sbad = 0;
         const uint32_t w0 = warp * (32u * kPartPerLane);
-        // pass 1: sides
+        // pass 1: sides (the split axis's bounds of all this lane's records
+        // are loaded first)
         uint32_t bal[kPartPerLane];
         uint32_t lt_w = 0;
+        float pl[kPartPerLane], ph[kPartPerLane];
+#pragma unroll
+        for (uint32_t j = 0; j < kPartPerLane; ++j) {
+            const uint32_t i = w0 + j * 32u + lane;
+            if (i < cnt) {
+                pl[j] = reinterpret_cast<const float*>(&src[i].lo)[axis];
+                ph[j] = reinterpret_cast<const float*>(&src[i].hi)[axis];
+            }
+        }
 #pragma unroll
         for (uint32_t j = 0; j < kPartPerLane; ++j) {
             const uint32_t i = w0 + j * 32u + lane;
             bool pred = false;
             if (i < cnt) {
-                const float* lo = reinterpret_cast<const float*>(&src[i].lo);
-                const float* hi = reinterpret_cast<const float*>(&src[i].hi);
-                const float c = center_of(lo[axis], hi[axis]);
+                const float c = center_of(pl[j], ph[j]);
                 pred = use_thr ? c < thr : bin_of(c, cmin, ext, nbins) < split_bin;
             }
             bal[j] = __ballot_sync(kFull, pred);
@@ -2008,7 +2032,6 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 P_<Task>(ctx->tasks[lv]), P_<uint32_t>(ctx->cbkeys[lv]), P_<uint32_t>(ctx->bins[lv]),
                 P_<uint32_t>(ctx->tile_task[lv]), P_<uint32_t>(ctx->tile_begin[lv]),
                 P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, d_ctr, lv, P);
-            MG_CUDA(cudaMemsetAsync(&d_ctr->lvl[nx][0], 0, 8, sm));
             EvalArgs A;
             A.tasks = P_<Task>(ctx->tasks[lv]);
             A.lv = lv;
