@@ -666,39 +666,33 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             box_empty(bgt[a]);
         }
         const uint32_t maxn = __reduce_max_sync(kFull, work ? n : 0u);
-        const float kInf = __int_as_float(0x7F800000), kNegInf = __int_as_float(0xFF800000);
         for (uint32_t r = 0; r < maxn; ++r) {
             const bool use = work && r < n;
             const uint32_t src = use ? s + r : lane;
-            float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
-                  jl2 = __shfl_sync(kFull, lo[2], src);
-            float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
-                  jh2 = __shfl_sync(kFull, hi[2], src);
-            // an unused slot becomes the empty box: its centroid is NaN, so it
-            // lands on the gt side and merging it changes nothing
-            jl0 = use ? jl0 : kInf;
-            jl1 = use ? jl1 : kInf;
-            jl2 = use ? jl2 : kInf;
-            jh0 = use ? jh0 : kNegInf;
-            jh1 = use ? jh1 : kNegInf;
-            jh2 = use ? jh2 : kNegInf;
+            const float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
+                        jl2 = __shfl_sync(kFull, lo[2], src);
+            const float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
+                        jh2 = __shfl_sync(kFull, hi[2], src);
+            if (!use) continue;  // lanes past their segment's objects merge nothing
             const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                const bool L = jc[a] < thr[a];  // bvh/src/lib.rs:308
-                blt[a][0] = fminf(blt[a][0], L ? jl0 : kInf);
-                blt[a][1] = fminf(blt[a][1], L ? jl1 : kInf);
-                blt[a][2] = fminf(blt[a][2], L ? jl2 : kInf);
-                blt[a][3] = fmaxf(blt[a][3], L ? jh0 : kNegInf);
-                blt[a][4] = fmaxf(blt[a][4], L ? jh1 : kNegInf);
-                blt[a][5] = fmaxf(blt[a][5], L ? jh2 : kNegInf);
-                bgt[a][0] = fminf(bgt[a][0], L ? kInf : jl0);
-                bgt[a][1] = fminf(bgt[a][1], L ? kInf : jl1);
-                bgt[a][2] = fminf(bgt[a][2], L ? kInf : jl2);
-                bgt[a][3] = fmaxf(bgt[a][3], L ? kNegInf : jh0);
-                bgt[a][4] = fmaxf(bgt[a][4], L ? kNegInf : jh1);
-                bgt[a][5] = fmaxf(bgt[a][5], L ? kNegInf : jh2);
-                nlt[a] += L ? 1u : 0u;
+                if (jc[a] < thr[a]) {  // bvh/src/lib.rs:308
+                    blt[a][0] = fminf(blt[a][0], jl0);
+                    blt[a][1] = fminf(blt[a][1], jl1);
+                    blt[a][2] = fminf(blt[a][2], jl2);
+                    blt[a][3] = fmaxf(blt[a][3], jh0);
+                    blt[a][4] = fmaxf(blt[a][4], jh1);
+                    blt[a][5] = fmaxf(blt[a][5], jh2);
+                    nlt[a]++;
+                } else {
+                    bgt[a][0] = fminf(bgt[a][0], jl0);
+                    bgt[a][1] = fminf(bgt[a][1], jl1);
+                    bgt[a][2] = fminf(bgt[a][2], jl2);
+                    bgt[a][3] = fmaxf(bgt[a][3], jh0);
+                    bgt[a][4] = fmaxf(bgt[a][4], jh1);
+                    bgt[a][5] = fmaxf(bgt[a][5], jh2);
+                }
             }
         }
         Cand best;
