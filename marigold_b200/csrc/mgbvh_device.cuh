@@ -666,14 +666,15 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             box_empty(bgt[a]);
         }
         const uint32_t maxn = __reduce_max_sync(kFull, work ? n : 0u);
+        // every lane's object in shared memory; the lanes of a segment read
+        // its objects in turn (one address per segment: broadcast loads)
+        xchg[lane].lo = make_float4(lo[0], lo[1], lo[2], 0.0f);
+        xchg[lane].hi = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        __syncwarp();
         for (uint32_t r = 0; r < maxn; ++r) {
-            const bool use = work && r < n;
-            const uint32_t src = use ? s + r : lane;
-            const float jl0 = __shfl_sync(kFull, lo[0], src), jl1 = __shfl_sync(kFull, lo[1], src),
-                        jl2 = __shfl_sync(kFull, lo[2], src);
-            const float jh0 = __shfl_sync(kFull, hi[0], src), jh1 = __shfl_sync(kFull, hi[1], src),
-                        jh2 = __shfl_sync(kFull, hi[2], src);
-            if (!use) continue;  // lanes past their segment's objects merge nothing
+            if (!(work && r < n)) continue;  // lanes past their segment's objects merge nothing
+            const float4 ja = xchg[s + r].lo, jb = xchg[s + r].hi;
+            const float jl0 = ja.x, jl1 = ja.y, jl2 = ja.z, jh0 = jb.x, jh1 = jb.y, jh2 = jb.z;
             const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -695,6 +696,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
                 }
             }
         }
+        __syncwarp();  // reads of xchg done before the exchanges below rewrite it
         Cand best;
         best.key = ~0ull;
         best.n_lt = 0;
