@@ -408,6 +408,32 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, t.pair, lane);
     if (lane == 0) atomicMax(&O.ctr->height, t.depth);
     const uint32_t n_gt = t.len - d.n_lt;
+    // each child's class (0 leaf, 1 next-level task, 2 medium, 3 small), then
+    // one atomic per list for both children
+    uint32_t cls[2], ntl[2];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const uint32_t len = c == 0 ? n_gt : d.n_lt;
+        const uint32_t depth = t.depth + 1u;
+        const bool cleaf = len <= 1u || depth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
+        cls[c] = cleaf ? 0u : (len > P.medium_max ? 1u : (len > kSmallMax ? 2u : 3u));
+        ntl[c] = cls[c] == 1u ? (len + kTile - 1) / kTile : 0u;
+    }
+    uint32_t slot_task = 0, slot_tile = 0, slot_med = 0, slot_small = 0;
+    if (lane == 0) {
+        const uint32_t nl = (cls[0] == 1u) + (cls[1] == 1u), nm = (cls[0] == 2u) + (cls[1] == 2u),
+                       ns = (cls[0] == 3u) + (cls[1] == 3u);
+        if (nl) {
+            slot_task = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][0], nl);
+            slot_tile = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][1], ntl[0] + ntl[1]);
+        }
+        if (nm) slot_med = atomicAdd(&O.ctr->n_medium, nm);
+        if (ns) slot_small = atomicAdd(&O.ctr->n_small, ns);
+    }
+    slot_task = __shfl_sync(kFull, slot_task, 0);
+    slot_tile = __shfl_sync(kFull, slot_tile, 0);
+    slot_med = __shfl_sync(kFull, slot_med, 0);
+    slot_small = __shfl_sync(kFull, slot_small, 0);
     for (int c = 0; c < 2; ++c) {
         const uint32_t len = c == 0 ? n_gt : d.n_lt;
         const uint32_t start = c == 0 ? t.start + d.n_lt : t.start;
@@ -415,7 +441,6 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
         const uint32_t pair = c == 0 ? t.pair + 2u : t.pair + 2u * n_gt;
         const uint32_t depth = t.depth + 1u;
         const float* cb = c == 0 ? d.gtb : d.ltb;
-        const bool cleaf = len <= 1u || depth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
         Task ct;
         for (int a = 0; a < 3; ++a) {
             ct.lo[a] = cb[a];
@@ -430,22 +455,19 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
         ct.tile0 = ct.ntiles = 0;
         ct.nbase = t.nbase;
         ct.tbase = t.tbase;
-        if (cleaf) {
+        // this child's place in its list: after the gt child when both share it
+        const uint32_t before = (c == 1 && cls[0] == cls[1]) ? 1u : 0u;
+        if (cls[c] == 0u) {
             warp_store_node(O, t.nbase + slot, cb, start - t.tbase, len, 0u, lane);
             d.child_leaf[c] = 1;
             if (lane == 0 && len > 1) {
                 atomicAdd(&O.ctr->holes, 1u);
                 if (depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
             }
-        } else if (len > P.medium_max) {
-            const uint32_t nt = (len + kTile - 1) / kTile;
-            uint32_t ti = 0, t0 = 0;
-            if (lane == 0) {
-                ti = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][0], 1u);
-                t0 = atomicAdd(&O.ctr->lvl[A.lv ^ 1u][1], nt);
-            }
-            ti = __shfl_sync(kFull, ti, 0);
-            t0 = __shfl_sync(kFull, t0, 0);
+        } else if (cls[c] == 1u) {
+            const uint32_t nt = ntl[c];
+            const uint32_t ti = slot_task + before;
+            const uint32_t t0 = slot_tile + (c == 1 && cls[0] == 1u ? ntl[0] : 0u);
             if (ti >= A.cap_tasks || t0 + nt > A.cap_tiles) {
                 if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
                 continue;
@@ -460,19 +482,15 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
                 A.next_tile_begin[t0 + i] = i * kTile;
             }
             d.child_task[c] = ti;
-        } else if (len > kSmallMax) {
-            uint32_t mi = 0;
-            if (lane == 0) mi = atomicAdd(&O.ctr->n_medium, 1u);
-            mi = __shfl_sync(kFull, mi, 0);
+        } else if (cls[c] == 2u) {
+            const uint32_t mi = slot_med + before;
             if (mi >= A.cap_medium) {
                 if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
                 continue;
             }
             if (lane == 0) A.medium[mi] = ct;
         } else {
-            uint32_t si = 0;
-            if (lane == 0) si = atomicAdd(&O.ctr->n_small, 1u);
-            si = __shfl_sync(kFull, si, 0);
+            const uint32_t si = slot_small + before;
             if (si >= A.cap_small) {
                 if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
                 continue;
@@ -2174,8 +2192,11 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
 
     Out O;
-    O.nodes = P_<mgbvh_node>(ctx->nodes);
-    O.lens = P_<uint32_t>(ctx->lens);
+    // with room for every slot, nodes (and lens) go straight to the caller's
+    // buffers; scratch copies are made only when holes must be compacted
+    const bool direct = cap >= C.nodes;
+    O.nodes = direct ? d_nodes : P_<mgbvh_node>(ctx->nodes);
+    O.lens = (direct && d_lens) ? d_lens : P_<uint32_t>(ctx->lens);
     O.used = P_<uint8_t>(ctx->used);
     O.perm = d_perm;
     O.ctr = d_ctr;
@@ -2224,6 +2245,12 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     // node count and compaction
     uint32_t count = C.nodes;
     if (hc.holes > 0) {
+        if (direct) {  // the compaction reads the slots from scratch
+            MG_CUDA(cudaMemcpyAsync(ctx->nodes.p, d_nodes, sizeof(mgbvh_node) * (size_t)C.nodes,
+                                    cudaMemcpyDeviceToDevice, sm));
+            if (d_lens)
+                MG_CUDA(cudaMemcpyAsync(ctx->lens.p, d_lens, 4ull * C.nodes, cudaMemcpyDeviceToDevice, sm));
+        }
         if ((rc = ensure(ctx, ctx->newidx, 4ull * C.nodes)) != MGBVH_OK) return rc;
         if ((rc = ensure(ctx, ctx->widened, 4ull * C.nodes)) != MGBVH_OK) return rc;
         widen_used_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
@@ -2248,14 +2275,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
             P_<uint32_t>(ctx->newidx), C.nodes, d_nodes, d_lens);
         MG_CUDA(cudaGetLastError());
         launches += 2;
-    } else {
+    } else if (!direct) {
         if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
         MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
                                 cudaMemcpyDeviceToDevice, sm));
         if (d_lens)
             MG_CUDA(cudaMemcpyAsync(d_lens, ctx->lens.p, 4ull * count, cudaMemcpyDeviceToDevice, sm));
     }
-    MG_CUDA(cudaStreamSynchronize(sm));
+    if (hc.holes > 0 || !direct) MG_CUDA(cudaStreamSynchronize(sm));
     *out_count = count;
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
@@ -2417,7 +2444,7 @@ Params params_of(const mgbvh_ctx* ctx, const mgbvh_settings* st) {
 // array to the caller's outputs and the counters to pinned host memory.
 int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh_settings* st,
                   uint32_t fixed_levels, mgbvh_node* d_nodes, uint32_t* d_lens, uint32_t* d_perm,
-                  uint32_t& launches, uint32_t& levels) {
+                  uint32_t& launches, uint32_t& levels, bool direct) {
     const cudaStream_t sm = ctx->stream;
     const uint32_t nm = B.nm, n = B.n;
     const Params P = params_of(ctx, st);
@@ -2435,8 +2462,9 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
     MG_CUDA(cudaMemcpyAsync(ctx->noff_buf.p, h_noffs, 4ull * (nm + 1), cudaMemcpyHostToDevice, sm));
     MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
     Out O;
-    O.nodes = P_<mgbvh_node>(ctx->nodes);
-    O.lens = P_<uint32_t>(ctx->lens);
+    // direct: the caller's buffers hold every slot; nodes (and lens) go there
+    O.nodes = direct ? d_nodes : P_<mgbvh_node>(ctx->nodes);
+    O.lens = (direct && d_lens) ? d_lens : P_<uint32_t>(ctx->lens);
     O.used = P_<uint8_t>(ctx->used);
     O.perm = d_perm;
     O.ctr = d_ctr;
@@ -2461,7 +2489,7 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
     int rc = run_pipeline(ctx, C, P, O, rec0, rec1, B.n_large > 0, fixed_levels, launches, levels);
     if (rc != MGBVH_OK) return rc;
     if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->ev1, sm));
-    if (fixed_levels) {
+    if (fixed_levels && !direct) {
         MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)B.slots,
                                 cudaMemcpyDeviceToDevice, sm));
         if (d_lens)
@@ -2584,7 +2612,8 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         }
     }
     if (!done) {
-        if ((rc = enqueue_batch(ctx, B, C, st, 0, d_nodes, d_lens, d_perm, launches, levels)) != MGBVH_OK)
+        if ((rc = enqueue_batch(ctx, B, C, st, 0, d_nodes, d_lens, d_perm, launches, levels,
+                                cap >= B.slots)) != MGBVH_OK)
             return rc;
         MG_CUDA(cudaStreamSynchronize(sm));
     }
@@ -2597,7 +2626,14 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     }
     const std::vector<uint32_t>& noffs = B.noffs;
     uint32_t count = B.slots;
+    const bool direct = cap >= B.slots;
     if (hc.holes > 0) {
+        if (direct) {  // the compaction reads the slots from scratch
+            MG_CUDA(cudaMemcpyAsync(ctx->nodes.p, d_nodes, sizeof(mgbvh_node) * (size_t)C.nodes,
+                                    cudaMemcpyDeviceToDevice, sm));
+            if (d_lens)
+                MG_CUDA(cudaMemcpyAsync(ctx->lens.p, d_lens, 4ull * C.nodes, cudaMemcpyDeviceToDevice, sm));
+        }
         if ((rc = ensure(ctx, ctx->newidx, 4ull * C.nodes)) != MGBVH_OK) return rc;
         if ((rc = ensure(ctx, ctx->widened, 4ull * C.nodes)) != MGBVH_OK) return rc;
         widen_used_kernel<<<std::min<uint32_t>((C.nodes + 255) / 256, 4096u), 256, 0, sm>>>(
@@ -2625,7 +2661,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     } else {
         if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the trees");
         for (uint32_t m = 0; m <= nm; ++m) out_offsets[m] = noffs[m];
-        if (!from_graph) {
+        if (!from_graph && !direct) {
             MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)count,
                                     cudaMemcpyDeviceToDevice, sm));
             if (d_lens)
@@ -2647,7 +2683,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         if (cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
         } else {
-        const int erc = enqueue_batch(ctx, B, C, st, fixed, d_nodes, d_lens, d_perm, gl, glev);
+        const int erc = enqueue_batch(ctx, B, C, st, fixed, d_nodes, d_lens, d_perm, gl, glev, true);
         const cudaError_t ce = cudaStreamEndCapture(sm, &g);
         if (erc == MGBVH_OK && ce == cudaSuccess && g) {
             if (cudaGraphInstantiate(&ctx->graph_exec, g, 0) == cudaSuccess) {
