@@ -284,7 +284,15 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
 // level's kernels, which read them, have finished).
 constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 
-__global__ void __launch_bounds__(kTileThreads) lvl_bin_kernel(
+#ifndef MGBVH_BIN_MIN_BLOCKS
+#define MGBVH_BIN_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
+#endif
+#ifndef MGBVH_PART_UNROLL
+#define MGBVH_PART_UNROLL 2  // records in flight per lane in the scatter pass (tuning knob)
+#endif
+constexpr int kPartUnroll = MGBVH_PART_UNROLL;
+
+__global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* __restrict__ bins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
     uint32_t* __restrict__ tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
@@ -968,7 +976,7 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
         init_key12(k);
         bool bad = false;
         // pass 2: scatter
-#pragma unroll 2
+#pragma unroll(kPartUnroll)
         for (uint32_t j = 0; j < kPartPerLane; ++j) {
             const uint32_t i = w0 + j * 32u + lane;
             if (i < cnt) {
@@ -1155,7 +1163,8 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
                                           uint32_t n, uint32_t depth, uint32_t tbase,
                                           const uint32_t* cnt, const float* ext,
                                           uint32_t plain_ck, uint32_t lane, Cand& win,
-                                          uint32_t& axis, uint32_t& n_lt, bool& use_thr) {
+                                          uint32_t& axis, uint32_t& n_lt, bool& use_thr,
+                                          uint32_t* wb) {
     float f[24];
     node_features(nd.b, nd.cb, n, depth, cnt, f);
     const float sa_p = surface_area6(nd.b);
@@ -1216,12 +1225,87 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
         float refine = 0.0f;
         mgbvh_mlp::warp_forward_t(f, LN.w, lane, top0, top1, refine);
         if (!LN.gate || refine > 0.0f) {
-            const int prop = (lane >> 4) ? top1 : top0;
-            const uint32_t pa = (uint32_t)prop >> 4, bucket = (uint32_t)prop & 15u;
-            const uint32_t k = lane & 15u;
-            const float thr = proposal_threshold(nd.cb[pa], ext[pa], bucket, k);
+            // Interval bins (the warp's bin area is free once the binned
+            // candidates are in registers): every object goes to the interval
+            // of its centroid among each proposal's 16 thresholds; lane
+            // p * 16 + k then scores threshold k of proposal p with lt =
+            // intervals 0..k and gt = k + 1..16, the same object sets as
+            // testing centroid < threshold object by object.
+            uint32_t pa[2], pb[2];
+            float pc[2], pe[2];
+            bool act[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const uint32_t prop = (uint32_t)(q ? top1 : top0);
+                pa[q] = min(prop >> 4, 2u);
+                pb[q] = prop & 15u;
+                pc[q] = nd.cb[pa[q]];
+                pe[q] = ext[pa[q]];
+                act[q] = pe[q] > 0.0f;
+            }
+            for (uint32_t i = lane; i < kRBinWords; i += 32) {
+                const uint32_t f7 = i % 7u;
+                wb[i] = f7 == 0 ? 0u : (f7 <= 3 ? kKeyPosInf : kKeyNegInf);
+            }
+            __syncwarp();
+            for (uint32_t j = lane; j < n; j += 32) {
+                float lo[3], hi[3];
+                fetch(j, lo, hi);
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (!act[q]) continue;  // warp-uniform
+                    const float c = center_of(lo[pa[q]], hi[pa[q]]);
+                    uint32_t a = 0, b = 16;  // interval = number of thresholds thr with !(c < thr)
+#pragma unroll
+                    for (int it = 0; it < 5; ++it) {
+                        if (a < b) {
+                            const uint32_t mid = (a + b) >> 1;
+                            if (!(c < proposal_threshold(pc[q], pe[q], pb[q], mid)))
+                                a = mid + 1;
+                            else
+                                b = mid;
+                        }
+                    }
+                    uint32_t* w = wb + (q * 17 + a) * 7;
+                    atomicAdd(w, 1u);
+                    atomicMin(w + 1, fkey(lo[0]));
+                    atomicMin(w + 2, fkey(lo[1]));
+                    atomicMin(w + 3, fkey(lo[2]));
+                    atomicMax(w + 4, fkey(hi[0]));
+                    atomicMax(w + 5, fkey(hi[1]));
+                    atomicMax(w + 6, fkey(hi[2]));
+                }
+            }
+            __syncwarp();
+            const uint32_t q = lane >> 4, k = lane & 15u;
+            const uint32_t qa = q ? pa[1] : pa[0];
+            const float thr = proposal_threshold(q ? pc[1] : pc[0], q ? pe[1] : pe[0], q ? pb[1] : pb[0], k);
+            const uint32_t* rb = wb + q * 17u * 7u;
             Cand c;
-            score_threshold(fetch, n, pa, thr, ext[pa] > 0.0f, sa_p, P, c, lane);
+            box_empty(c.lt);
+            box_empty(c.gt);
+            uint32_t nl = 0, ng = 0;
+            for (uint32_t j = 0; j < 17; ++j) {
+                const uint32_t* bj = rb + j * 7;
+                const uint32_t cj = bj[0];
+                if (cj == 0) continue;
+                if (j <= k) {
+                    nl += cj;
+                    box_grow(c.lt, funkey(bj[1]), funkey(bj[2]), funkey(bj[3]), funkey(bj[4]),
+                             funkey(bj[5]), funkey(bj[6]));
+                } else {
+                    ng += cj;
+                    box_grow(c.gt, funkey(bj[1]), funkey(bj[2]), funkey(bj[3]), funkey(bj[4]),
+                             funkey(bj[5]), funkey(bj[6]));
+                }
+            }
+            __syncwarp();  // the interval bins are read before the warp's next use of its bin area
+            c.key = ~0ull;
+            c.n_lt = nl;
+            c.thr = thr;
+            if ((q ? act[1] : act[0]) && nl >= P.min_leaf && ng >= P.min_leaf)
+                c.key = cand_key(split_cost(surface_area6(c.lt), surface_area6(c.gt), sa_p, nl, ng), qa,
+                                 lane);
             const uint64_t wk2 = warp_min_key(c.key);
             const uint32_t wlo = static_cast<uint32_t>(wk2);
             if (wlo != kNoKey && static_cast<uint32_t>(wk2 >> 32) < plain_ck) {
@@ -1372,7 +1456,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                         if (!leaf && (LN.w || LN.samples) && B == 32u)
                             learned_node(S, LN, P, nd, ib, base, s, n, depth, t.tbase, cnt, ext,
                                          static_cast<uint32_t>(wk >> 32), lane, win, axis, n_lt,
-                                         use_thr);
+                                         use_thr, S.bins[warp]);
                         if (use_thr && lane == 0) atomicAdd(&O.ctr->learned, 1u);
                     }
                 }
@@ -1547,7 +1631,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
 // kLearn: with the learned form's hook (network proposals, training samples);
 // plain builds run the instantiation without it.
 template <bool kLearn, uint32_t kCap>
-__global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __restrict__ tasks,
+__global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : 1) medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
                                                                 Learn LN) {
@@ -1566,7 +1650,10 @@ __global__ void __launch_bounds__(kMediumThreads) medium_kernel(const Task* __re
 // builder (every node adaptive with one threshold per object); otherwise the
 // depth-first builder that also covers binned nodes and fixed step counts.
 template <bool kLevels>
-__global__ void __launch_bounds__(256) small_kernel(const Task* __restrict__ tasks,
+#ifndef MGBVH_SMALL_MIN_BLOCKS
+#define MGBVH_SMALL_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
+#endif
+__global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(const Task* __restrict__ tasks,
                                                    const Rec* __restrict__ rec0,
                                                    const Rec* __restrict__ rec1, Params P, Out O) {
     __shared__ XRec xchg[8][32];
