@@ -236,6 +236,21 @@ MGBVH_API int mgbvh_set_graph_capture(mgbvh_ctx* ctx, int enable);
    smaller ones to the per-subtree kernels. */
 MGBVH_API int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max);
 
+/* World AABBs of instances for the TLAS, computed on the GPU as marigold's
+   scene upload computes them on the host (marigold/src/app/data/scene/
+   model.rs:191-234): the 8 corners of each instance's mesh bounds through its
+   column-major 4x4 f32 transform (glam's Mat4 * Vec4 order), min/max over the
+   corners. d_mesh_bounds: mesh_count x 6 floats (min xyz, max xyz);
+   d_instance_mesh: instance_count mesh indices; d_transforms: instance_count x
+   16 floats; d_out_aabbs: instance_count x 6 floats, the input of
+   mgbvh_build_aabbs_dev or of a batched build's TLAS. Runs on the context's
+   stream and returns when done; an index >= mesh_count gives
+   MGBVH_ERR_INVALID_ARG. The uploaded record's inverse transform is not
+   computed here. */
+MGBVH_API int mgbvh_instance_aabbs_dev(mgbvh_ctx* ctx, const float* d_mesh_bounds, uint32_t mesh_count,
+                                       const uint32_t* d_instance_mesh, const float* d_transforms,
+                                       uint32_t instance_count, float* d_out_aabbs);
+
 /*
  * Allocation-free build over device-resident AABBs. This entry point has no
  * counterpart in the reference. It exists for callers that must not allocate

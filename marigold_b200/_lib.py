@@ -34,7 +34,7 @@ EXPORTED = (
     "mgbvh_tracer_set_blas_dev", "mgbvh_trace_closest_dev", "mgbvh_trace_bruteforce_dev",
     "mgbvh_build_batch_dev", "mgbvh_set_tuning", "mgbvh_set_graph_capture",
     "mgbvh_mlp_train_step_dev", "mgbvh_mlp_forward_dev", "mgbvh_mlp_adam_dev",
-    "mgbvh_set_split_proposer", "mgbvh_set_sample_output",
+    "mgbvh_set_split_proposer", "mgbvh_set_sample_output", "mgbvh_instance_aabbs_dev",
 )
 
 
@@ -181,6 +181,8 @@ def load():
         L.mgbvh_set_sample_output.restype = ctypes.c_int
         L.mgbvh_set_graph_capture.argtypes = [P, ctypes.c_int]
         L.mgbvh_set_graph_capture.restype = ctypes.c_int
+        L.mgbvh_instance_aabbs_dev.argtypes = [P, P, u32, P, P, u32, P]
+        L.mgbvh_instance_aabbs_dev.restype = ctypes.c_int
         L.mgbvh_set_tuning.argtypes = [P, u32]
         L.mgbvh_set_tuning.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]

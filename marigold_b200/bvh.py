@@ -310,3 +310,15 @@ def build_batch_device(ctx: Context, settings: BvhSettings, meshes, out_nodes, o
                                  ctypes.c_void_p(out_perm.data_ptr()), offs, ctypes.byref(st))
     ctx.check(rc)
     return list(offs), rc, st.as_dict()
+
+
+def instance_aabbs_device(ctx: Context, mesh_bounds, instance_mesh, transforms, out_aabbs) -> None:
+    """World AABBs of instances on the GPU (the TLAS input of marigold's scene
+    upload, marigold/src/app/data/scene/model.rs:191-234). Device tensors:
+    mesh_bounds float32 [M, 6], instance_mesh int32/uint32 [I], transforms
+    float32 [I, 16] (column-major), out_aabbs float32 [I, 6]. Runs on the
+    context's stream; raises MgbvhError for an index past M."""
+    n = instance_mesh.shape[0]
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    ctx.check(ctx.L.mgbvh_instance_aabbs_dev(ctx.ptr, vp(mesh_bounds), mesh_bounds.shape[0],
+                                             vp(instance_mesh), vp(transforms), n, vp(out_aabbs)))

@@ -1706,6 +1706,57 @@ __global__ void compact_kernel(const mgbvh_node* __restrict__ src, const uint32_
 
 
 
+// ---------------------------------------------------------------- instances
+
+// World AABB of every instance, as marigold's scene upload computes it for
+// the TLAS (marigold/src/app/data/scene/model.rs:191-234): the 8 corners of
+// the instance's mesh bounds, in the order (min,min,min), (min,min,max), ...,
+// (max,max,max), as (x, y, z, 1) through the column-major transform; each
+// component is ((c0 x + c1 y) + c2 z) + c3 * 1 with every product and sum
+// rounded on its own (glam 0.30.10 Mat4 * Vec4: the column products summed
+// in column order, no fused multiply-add), then the running min/max over the
+// corners in that order with a tie taking the later corner (the SSE
+// minps/maxps behind Vec3A::min/max). Grid-stride over instances.
+__global__ void instance_aabbs_kernel(const float* __restrict__ mesh_bounds, uint32_t mesh_count,
+                                      const uint32_t* __restrict__ inst_mesh,
+                                      const float* __restrict__ xf, uint32_t n,
+                                      float* __restrict__ out, Counters* ctr) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t m = inst_mesh[i];
+        if (m >= mesh_count) {
+            set_error(ctr, MGBVH_ERR_INVALID_ARG, kSiteMeshIndex);
+            continue;
+        }
+        const float* b = mesh_bounds + 6 * (size_t)m;
+        const float* t = xf + 16 * (size_t)i;
+        float lo[3], hi[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+            lo[r] = __int_as_float(0x7F800000);
+            hi[r] = __int_as_float(0xFF800000);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float x = b[(c >> 2) & 1 ? 3 : 0], y = b[(c >> 1) & 1 ? 4 : 1], z = b[c & 1 ? 5 : 2];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const float v = __fadd_rn(
+                    __fadd_rn(__fadd_rn(__fmul_rn(t[r], x), __fmul_rn(t[4 + r], y)), __fmul_rn(t[8 + r], z)),
+                    __fmul_rn(t[12 + r], 1.0f));
+                lo[r] = lo[r] < v ? lo[r] : v;
+                hi[r] = hi[r] > v ? hi[r] : v;
+            }
+        }
+        float* o = out + 6 * (size_t)i;
+        o[0] = lo[0];
+        o[1] = lo[1];
+        o[2] = lo[2];
+        o[3] = hi[0];
+        o[4] = hi[1];
+        o[5] = hi[2];
+    }
+}
+
 // ---------------------------------------------------------------- batched builds
 //
 // Many BVHs (the BLAS of every mesh and the TLAS over instances) in one
@@ -2098,6 +2149,7 @@ const char* site_text(uint32_t site) {
             return "forced median split on a node above 1024 objects is not built (no binned split "
                    "passed the MIN_LEAF_OBJECTS filter)";
         case kSiteCapacity: return "internal task list overflow";
+        case kSiteMeshIndex: return "an instance names a mesh past mesh_count";
         default: return "device error";
     }
 }
@@ -3134,6 +3186,28 @@ int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max) {
     if (medium_max < kSmallMax + 1 || medium_max > kMediumMax)
         return fail(ctx, MGBVH_ERR_UNSUPPORTED, "medium_max must be 33..1024");
     ctx->medium_max = medium_max;
+    return MGBVH_OK;
+}
+
+int mgbvh_instance_aabbs_dev(mgbvh_ctx* ctx, const float* d_mesh_bounds, uint32_t mesh_count,
+                             const uint32_t* d_instance_mesh, const float* d_transforms,
+                             uint32_t instance_count, float* d_out_aabbs) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (instance_count == 0) return MGBVH_OK;
+    if (!d_mesh_bounds || !d_instance_mesh || !d_transforms || !d_out_aabbs)
+        return fail(ctx, MGBVH_ERR_INVALID_ARG, "a device pointer is NULL");
+    if ((rc = ensure(ctx, ctx->ctr, sizeof(Counters))) != MGBVH_OK) return rc;
+    const cudaStream_t sm = ctx->stream;
+    Counters* d_ctr = P_<Counters>(ctx->ctr);
+    MG_CUDA(cudaMemsetAsync(d_ctr, 0, 2 * sizeof(uint32_t), sm));  // error, error_site
+    const int blocks = (int)std::min<uint32_t>((instance_count + 255) / 256, (uint32_t)ctx->sm_count * 8u);
+    instance_aabbs_kernel<<<blocks, 256, 0, sm>>>(d_mesh_bounds, mesh_count, d_instance_mesh, d_transforms,
+                                                  instance_count, d_out_aabbs, d_ctr);
+    MG_CUDA(cudaGetLastError());
+    MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, sm));
+    MG_CUDA(cudaStreamSynchronize(sm));
+    if (ctx->h_ctr->error) return fail(ctx, (int)ctx->h_ctr->error, site_text(ctx->h_ctr->error_site));
     return MGBVH_OK;
 }
 

@@ -54,6 +54,7 @@ enum ErrorSite : uint32_t {
     kSiteContain = 3,      // a centroid outside its child's bounds
     kSiteLargeMedian = 4,  // forced median on a node above the CTA size with distinct keys
     kSiteCapacity = 5,
+    kSiteMeshIndex = 6,  // an instance names a mesh past the mesh count
 };
 
 __device__ __forceinline__ void set_error(Counters* c, int status, uint32_t site) {

@@ -288,14 +288,39 @@ def quaternion_matrix(q):
         np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1)], 1)
 
 
-def instance_aabbs(mesh_bounds: np.ndarray, mesh_ids, rot, scale, trans) -> np.ndarray:
-    """World AABB of each instance: min/max over the 8 corners of its mesh's
-    bounds under x -> R (s x) + t (marigold/src/app/data/scene/model.rs:191-234)."""
-    b = mesh_bounds[mesh_ids]  # [n, 6]
-    corners = np.stack([np.stack([b[:, 3 * (i >> 2 & 1)], b[:, 1 + 3 * (i >> 1 & 1)],
-                                  b[:, 2 + 3 * (i & 1)]], -1) for i in range(8)], 1)  # [n, 8, 3]
-    w = np.einsum("nij,nkj->nki", rot, corners * scale[:, None, None]) + trans[:, None, :]
-    return _f32(np.concatenate([w.min(axis=1), w.max(axis=1)], axis=1))
+def instance_transforms(rot, scale, trans) -> np.ndarray:
+    """Column-major f32 4x4 matrices x -> R (s x) + t, 16 floats per instance
+    (glam's Mat4 layout: x_axis, y_axis, z_axis, w_axis columns)."""
+    n = rot.shape[0]
+    m = np.zeros((n, 4, 4), np.float64)  # [instance, column, row]
+    for c in range(3):
+        m[:, c, 0:3] = rot[:, :, c] * scale[:, None]
+    m[:, 3, 0:3] = trans
+    m[:, 3, 3] = 1.0
+    return _f32(m.reshape(n, 16))
+
+
+def instance_aabbs(mesh_bounds: np.ndarray, mesh_ids, transforms) -> np.ndarray:
+    """World AABB of each instance as marigold's scene upload computes it
+    (marigold/src/app/data/scene/model.rs:191-234), in f32: the 8 corners of
+    the mesh's bounds as (x, y, z, 1) through the column-major matrix, each
+    component ((c0 x + c1 y) + c2 z) + c3 * 1 with every product and sum
+    rounded (glam 0.30 Mat4 * Vec4), then min/max over the corners in corner
+    order with ties taking the later corner (SSE minps/maxps)."""
+    b = np.asarray(mesh_bounds, np.float32)[np.asarray(mesh_ids)]
+    m = np.asarray(transforms, np.float32).reshape(-1, 4, 4)  # [instance, column, row]
+    lo = np.full((b.shape[0], 3), np.inf, np.float32)
+    hi = np.full((b.shape[0], 3), -np.inf, np.float32)
+    one = np.float32(1.0)
+    for i in range(8):
+        x = b[:, 3 if (i >> 2) & 1 else 0]
+        y = b[:, 4 if (i >> 1) & 1 else 1]
+        z = b[:, 5 if i & 1 else 2]
+        w = ((m[:, 0, 0:3] * x[:, None] + m[:, 1, 0:3] * y[:, None]) + m[:, 2, 0:3] * z[:, None]) \
+            + m[:, 3, 0:3] * one
+        lo = np.where(lo < w, lo, w)
+        hi = np.where(hi > w, hi, w)
+    return np.concatenate([lo, hi], axis=1).astype(np.float32)
 
 
 def batched_scene(seed: int = 3, n_meshes: int = 512, n_instances: int = 4096,
@@ -328,11 +353,20 @@ def batched_scene(seed: int = 3, n_meshes: int = 512, n_instances: int = 4096,
             t = f[:n].astype(np.uint32)
         meshes.append((v, np.ascontiguousarray(t, dtype=np.uint32)))
     bounds = np.stack([mesh_bounds(v) for v, _ in meshes])
+    ids, xf = scene_instances(seed, n_meshes, n_instances)
+    inst = instance_aabbs(bounds, ids, xf)
+    return meshes, bounds, inst
+
+
+def scene_instances(seed: int, n_meshes: int, n_instances: int):
+    """Instances of the batched scene: mesh ids (uint32 [I], uniform) and f32
+    column-major transforms [I, 16] (rotation from a normalised 4-D Gaussian
+    quaternion, uniform scale in [0.5, 2], translation uniform in
+    [-100, 100]^3)."""
     j = np.arange(n_instances, dtype=np.uint32)
-    ids = np.minimum((uniform(seed, 3, j) * n_meshes).astype(np.int64), n_meshes - 1)
+    ids = np.minimum((uniform(seed, 3, j) * n_meshes).astype(np.int64), n_meshes - 1).astype(np.uint32)
     q = np.stack([gaussian(seed, 10 + 2 * k, j) for k in range(4)], -1)
     q = q / np.sqrt((q * q).sum(axis=1, keepdims=True))
     scale = 0.5 + 1.5 * uniform(seed, 20, j)
     trans = np.stack([uniform(seed, 21 + k, j) * 200.0 - 100.0 for k in range(3)], -1)
-    inst = instance_aabbs(bounds.astype(np.float64), ids, quaternion_matrix(q), scale, trans)
-    return meshes, bounds, inst
+    return ids, instance_transforms(quaternion_matrix(q), scale, trans)

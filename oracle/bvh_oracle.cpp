@@ -882,6 +882,45 @@ uint32_t oracle_sample_nodes(const float* verts, uint32_t vertex_stride_bytes, c
     return count;
 }
 
+// World AABBs of instances as marigold's scene upload computes them
+// (marigold/src/app/data/scene/model.rs:191-234): corners (min,min,min),
+// (min,min,max), ..., (max,max,max) of the mesh bounds as (x, y, z, 1)
+// through the column-major transform; glam 0.30.10's Mat4 * Vec4 (SSE2)
+// multiplies each column by the vector's matching component and adds the
+// four products in column order, so component r is ((c0 x + c1 y) + c2 z) +
+// c3 * 1; Vec3A::min/max are minps/maxps, which return the second operand on
+// a tie. out: n x 6 floats. Returns the number of instances whose mesh index
+// is out of range (their boxes are left unwritten).
+uint32_t oracle_instance_aabbs(const float* mesh_bounds, uint32_t mesh_count, const uint32_t* inst_mesh,
+                               const float* xf, uint32_t n, float* out) {
+    uint32_t bad = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (inst_mesh[i] >= mesh_count) {
+            ++bad;
+            continue;
+        }
+        const float* b = mesh_bounds + 6 * (size_t)inst_mesh[i];
+        const float* t = xf + 16 * (size_t)i;
+        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+        for (int c = 0; c < 8; ++c) {
+            const float x = b[(c >> 2) & 1 ? 3 : 0], y = b[(c >> 1) & 1 ? 4 : 1], z = b[c & 1 ? 5 : 2];
+            for (int r = 0; r < 3; ++r) {
+                float v = t[r] * x;
+                v = v + t[4 + r] * y;
+                v = v + t[8 + r] * z;
+                v = v + t[12 + r] * 1.0f;
+                lo[r] = lo[r] < v ? lo[r] : v;  // minps(lo, v)
+                hi[r] = hi[r] > v ? hi[r] : v;  // maxps(hi, v)
+            }
+        }
+        for (int r = 0; r < 3; ++r) {
+            out[6 * (size_t)i + r] = lo[r];
+            out[6 * (size_t)i + 3 + r] = hi[r];
+        }
+    }
+    return bad;
+}
+
 // Closest hit of each ray against every triangle: the Moller-Trumbore test of
 // marigold/assets/shaders/slang/lib/scene.slang:19-89 (|det| < 1e-6 and
 // t < 1e-6 reject), every product and sum as written, lowest triangle index

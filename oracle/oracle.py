@@ -92,6 +92,8 @@ def lib():
             L.oracle_trace_bruteforce.argtypes = [P, u32, P, u32, P, u32, P, P]
             L.oracle_trace_bruteforce.restype = None
             L.oracle_sample_nodes.argtypes = [P, u32, P, u32, u32, P, u32]
+            L.oracle_instance_aabbs.argtypes = [P, u32, P, P, u32, P]
+            L.oracle_instance_aabbs.restype = u32
             L.oracle_sample_nodes.restype = u32
             _lib = L
     return _lib
@@ -174,3 +176,16 @@ def sample_nodes(vertices, triangles, min_n=33):
     out = np.zeros((cap, SAMPLE_WIDTH), np.float32)
     k = L.oracle_sample_nodes(_ptr(v), v.shape[1] * 4, _ptr(t), t.shape[0], min_n, _ptr(out), cap)
     return out[:k].copy()
+
+
+def instance_aabbs(mesh_bounds, instance_mesh, transforms):
+    """World AABBs of instances (marigold/src/app/data/scene/model.rs:191-234,
+    glam's Mat4 * Vec4 order): float32 [I, 6] and the count of instances whose
+    mesh index is out of range."""
+    L = lib()
+    b = np.ascontiguousarray(mesh_bounds, dtype=np.float32)
+    m = np.ascontiguousarray(instance_mesh, dtype=np.uint32)
+    x = np.ascontiguousarray(transforms, dtype=np.float32)
+    out = np.zeros((m.shape[0], 6), np.float32)
+    bad = L.oracle_instance_aabbs(_ptr(b), b.shape[0], _ptr(m), _ptr(x), m.shape[0], _ptr(out))
+    return out, bad
