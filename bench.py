@@ -64,6 +64,24 @@ def parse_args():
     return p.parse_args()
 
 
+def max_over_ranks(x: float, device="cuda") -> float:
+    """The largest of every rank's x (the slowest rank's time); x itself when
+    no process group is running."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(per_rank_units: int, world: int, ms_per_step: float) -> float:
+    """Millions of units per second over all ranks: every rank's units of one
+    step / the slowest rank's step time."""
+    return world * per_rank_units / (ms_per_step * 1e-3) / 1e6
+
+
 def dist_env():
     return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
             int(os.environ.get("LOCAL_RANK", 0)))
@@ -230,12 +248,8 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
     ms = [a.elapsed_time(b) for a, b in ev]
-    ms_per_step = float(np.mean(ms))
-    if world > 1:
-        tt = torch.tensor([ms_per_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_per_step = float(tt.item())
-    value = world * n / (ms_per_step * 1e-3) / 1e6
+    ms_per_step = max_over_ranks(float(np.mean(ms)))
+    value = whole_job_rate(n, world, ms_per_step)
 
     # tree statistics for the algorithmic byte counts (S = sum of inner lens)
     nodes_h = d_nodes.cpu().numpy().view(np.uint32).reshape(-1, 8)[:count]
@@ -309,11 +323,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         e2e_one()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_step = float(np.mean(e2e_ms))
-    if world > 1:
-        tt = torch.tensor([e2e_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_step = float(tt.item())
+    e2e_step = max_over_ranks(float(np.mean(e2e_ms)))
     h2d = v.nbytes + t.nbytes
     d2h = cnt.value * 32 + cnt.value * 4 + n * 4
 
@@ -326,7 +336,7 @@ def run_ours(args):
                    "min_leaf": 1, "max_leaf": 1, "max_depth": 32, "bins": 32,
                    "adaptive_max_n": 32, "parallelism": f"replicas x{world}",
                    "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
-        "e2e": {"value": round(world * n / (e2e_step * 1e-3) / 1e6, 3), "unit": UNIT,
+        "e2e": {"value": round(whole_job_rate(n, world, e2e_step), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": round(e2e_step, 4)},
         "roofline": {"bound": "hbm", "kernel": "small_kernel (subtrees of <= 32 objects)",
