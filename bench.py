@@ -468,6 +468,23 @@ def run_mixed(args):
             log(f"brute force {sub} rays: {brute[2]:.1f} s")
         gt, gp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
         mism = int(((gp != brute[1]) | (gt.view(np.uint32) != brute[0].view(np.uint32))).sum())
+        # the same tree collapsed to the 8-wide BVH with quantized boxes
+        wcount = ctypes.c_uint32(0)
+        tw = time.perf_counter()
+        tr.check(L.mgbvh_tracer_build_wide(tr.ptr, sp, ctypes.byref(wcount)))
+        wide_build_s = time.perf_counter() - tw
+        wcounts = (ctypes.c_uint64 * 3)()
+        wide_ms = []
+        for k in range(max(args.warmup, 1) + args.steps):
+            flush.fill_(k & 0xFF)
+            tr.check(L.mgbvh_trace_closest_wide_dev(tr.ptr, vp(dr), m, vp(ht), vp(hp), wcounts,
+                                                    ctypes.byref(secs), sp))
+            if k >= max(args.warmup, 1):
+                wide_ms.append(secs.value * 1e3)
+            log(f"{form} wide trace {k}: {secs.value * 1e3:.2f} ms")
+        wgt, wgp = ht[:sub].cpu().numpy(), hp[:sub].cpu().numpy().view(np.uint32)
+        wmism = int(((wgp != brute[1]) | (wgt.view(np.uint32) != brute[0].view(np.uint32))).sum())
+        wms = float(np.mean(wide_ms))
         bms, tms = float(np.mean(build_ms)), float(np.mean(trace_ms))
         forms[form] = {
             "build": {"value": round(n / (bms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms": round(bms, 3),
@@ -478,6 +495,10 @@ def run_mixed(args):
                       "hit_rays": int((hp != -1).sum().item()), "nodes_visited": counts[0],
                       "box_tests": counts[1], "triangle_tests": counts[2]},
             "check": {"subset_rays": sub, "mismatches_vs_gpu_bruteforce": mism},
+            "wide_trace": {"value": round(m / (wms * 1e-3) / 1e6, 2), "unit": "Mrays/s", "ms": round(wms, 3),
+                           "wide_nodes": wcount.value, "collapse_s": round(wide_build_s, 4),
+                           "nodes_visited": wcounts[0], "box_tests": wcounts[1],
+                           "triangle_tests": wcounts[2], "mismatches_vs_gpu_bruteforce": wmism},
         }
     ctx.set_split_proposer(None)
     out = {
@@ -486,6 +507,7 @@ def run_mixed(args):
                    "thin": 4194304 // sc, "scale": sc, "max_depth": 32, "leaf": 1,
                    "profile": "reference", "learned": "committed proposer, gate on"},
         "build": forms["plain"]["build"], "trace": forms["plain"]["trace"],
+        "wide_trace": forms["plain"]["wide_trace"],
         "check": dict(forms["plain"]["check"], bruteforce_s=round(brute[2], 2)),
         "learned": forms["learned"],
         "steps": args.steps, "warmup": args.warmup, "generation_s": round(gen_s, 1),

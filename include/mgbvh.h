@@ -315,6 +315,25 @@ MGBVH_API int mgbvh_tracer_set_blas_dev(mgbvh_tracer* tracer, const mgbvh_node* 
 MGBVH_API int mgbvh_trace_closest_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
                                       float* d_hit_t, uint32_t* d_hit_prim, uint64_t* out_counts,
                                       double* out_seconds, void* cuda_stream);
+/* Wide BVH (no counterpart in the reference, which names compressed wide
+   BVHs as its next step): collapses the bound binary tree into an 8-wide BVH
+   whose child boxes are quantized to 8-bit steps on a per-node power-of-two
+   grid, widened outward so that every stored box contains its exact box.
+   112-byte nodes: origin xyz (f32), per-axis step exponents (u8, step =
+   2^(e - 127)), child count (u8), child box steps lo x/y/z[8], hi x/y/z[8]
+   (u8), child refs[8] (u32: wide node index, or first triangle | 0x80000000
+   for a leaf), leaf triangle counts[8] (u8), 8 bytes of padding; node 0 is
+   the root. Runs on cuda_stream and returns when done. */
+MGBVH_API int mgbvh_tracer_build_wide(mgbvh_tracer* tracer, void* cuda_stream, uint32_t* out_wide_count);
+/* The wide nodes of the last mgbvh_tracer_build_wide (device pointer, owned by the tracer). */
+MGBVH_API int mgbvh_tracer_wide_nodes(mgbvh_tracer* tracer, const void** out_d_wide_nodes,
+                                      uint32_t* out_wide_count);
+/* Closest hit of every ray through the wide BVH: same results as
+   mgbvh_trace_closest_dev (same triangle test and tie rule; conservative
+   boxes). out_counts: wide nodes visited, child boxes tested, triangle tests. */
+MGBVH_API int mgbvh_trace_closest_wide_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
+                                           float* d_hit_t, uint32_t* d_hit_prim, uint64_t* out_counts,
+                                           double* out_seconds, void* cuda_stream);
 /* Closest hit of every ray against every triangle of the bound BLAS, with
    the same triangle test: the check for mgbvh_trace_closest_dev. */
 MGBVH_API int mgbvh_trace_bruteforce_dev(mgbvh_tracer* tracer, const float* d_rays,

@@ -35,6 +35,7 @@ EXPORTED = (
     "mgbvh_build_batch_dev", "mgbvh_set_tuning", "mgbvh_set_graph_capture",
     "mgbvh_mlp_train_step_dev", "mgbvh_mlp_forward_dev", "mgbvh_mlp_adam_dev",
     "mgbvh_set_split_proposer", "mgbvh_set_sample_output", "mgbvh_instance_aabbs_dev",
+    "mgbvh_tracer_build_wide", "mgbvh_tracer_wide_nodes", "mgbvh_trace_closest_wide_dev",
 )
 
 
@@ -163,6 +164,13 @@ def load():
         L.mgbvh_trace_closest_dev.argtypes = [P, P, u32, P, P, ctypes.POINTER(ctypes.c_uint64),
                                               ctypes.POINTER(ctypes.c_double), P]
         L.mgbvh_trace_closest_dev.restype = ctypes.c_int
+        L.mgbvh_tracer_build_wide.argtypes = [P, P, pu32]
+        L.mgbvh_tracer_build_wide.restype = ctypes.c_int
+        L.mgbvh_tracer_wide_nodes.argtypes = [P, ctypes.POINTER(P), pu32]
+        L.mgbvh_tracer_wide_nodes.restype = ctypes.c_int
+        L.mgbvh_trace_closest_wide_dev.argtypes = [P, P, u32, P, P, ctypes.POINTER(ctypes.c_uint64),
+                                                   ctypes.POINTER(ctypes.c_double), P]
+        L.mgbvh_trace_closest_wide_dev.restype = ctypes.c_int
         L.mgbvh_trace_bruteforce_dev.argtypes = [P, P, u32, P, P, P]
         L.mgbvh_trace_bruteforce_dev.restype = ctypes.c_int
         L.mgbvh_build_batch_dev.argtypes = [P, ctypes.POINTER(MeshDesc), u32, ctypes.POINTER(Settings),

@@ -230,6 +230,321 @@ __global__ void gather_kernel(const float* __restrict__ verts, uint32_t stride_f
     }
 }
 
+
+// ---------------------------------------------------------------- wide BVH
+//
+// An 8-wide BVH with quantized child boxes, collapsed from the binary tree
+// (the compressed wide BVH of Ylitie, Karras and Laine, "Efficient Incoherent
+// Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017, in a layout
+// of this library's own). Each wide node holds up to 8 children, found by
+// opening, from the node's two binary children, the internal child of largest
+// surface area until 8 children or only leaves remain. Child boxes are stored
+// as 8-bit steps on a per-node grid: origin p (the node box's minimum) and a
+// power-of-two step per axis, each child box widened outward to whole steps,
+// checked in float with the traversal's own dequantization (p + q * step), so
+// the stored box always contains the exact one.
+
+constexpr uint32_t kWideLeaf = 0x80000000u;  // ref of a leaf child: first triangle | kWideLeaf
+constexpr int kWideStack = 128;
+
+struct WNode {           // 112 bytes
+    float px, py, pz;    // grid origin
+    uint8_t e[3];        // grid step per axis: 2^(e - 127)
+    uint8_t nchild;
+    uint8_t qlo[3][8];   // child boxes in grid steps
+    uint8_t qhi[3][8];
+    uint32_t ref[8];     // wide node index, or first triangle | kWideLeaf
+    uint8_t cnt[8];      // triangles of a leaf child
+    uint32_t pad[2];
+};
+static_assert(sizeof(WNode) == 112, "wide node layout");
+
+__device__ __forceinline__ float box_sa(const float4& lo, const float4& hi) {
+    const float w = hi.x - lo.x, h = hi.y - lo.y, d = hi.z - lo.z;
+    return w * h + w * d + h * d;
+}
+
+__device__ __forceinline__ float wstep(uint8_t e) { return __int_as_float(static_cast<uint32_t>(e) << 23); }
+
+__device__ __forceinline__ float wdeq(float p, uint32_t q, float step) {
+    return __fadd_rn(p, __fmul_rn(__uint2float_rn(q), step));
+}
+
+// One level of the collapse: wide nodes [range[0], range[1]) whose binary
+// node is binid[w] with binlen[w] objects; their children that stay internal
+// become wide nodes of the next level (slots taken from *counter, their
+// binary nodes and lengths recorded in binid/binlen). A child's length comes
+// from the start indices (the lt child starts where its parent starts, the
+// gt child after the lt child's objects), so the collapse needs no per-node
+// lengths. A child of at most kWideLeafMax objects becomes a leaf child over
+// its contiguous range of triangles.
+#ifndef MGBVH_WIDE_LEAF_MAX
+#define MGBVH_WIDE_LEAF_MAX 2  // largest subtree kept as one leaf child (tuning knob)
+#endif
+constexpr uint32_t kWideLeafMax = MGBVH_WIDE_LEAF_MAX;
+
+__global__ void __launch_bounds__(128) wide_level_kernel(const float4* __restrict__ nodes,
+                                                         uint32_t* __restrict__ binid,
+                                                         uint32_t* __restrict__ binlen,
+                                                         const uint32_t* __restrict__ range,
+                                                         uint32_t* __restrict__ counter, WNode* __restrict__ wn,
+                                                         uint32_t cap, int* err) {
+    const uint32_t begin = range[0], end = range[1];
+    for (uint32_t w = begin + blockIdx.x * blockDim.x + threadIdx.x; w < end; w += gridDim.x * blockDim.x) {
+        const uint32_t b = binid[w], blen = binlen[w];
+        uint32_t c[8], cl[8];
+        uint32_t m = 0;
+        auto internal = [&](uint32_t node, uint32_t len) {
+            return __float_as_uint(nodes[2 * node + 1].w) != 0 && len > kWideLeafMax;
+        };
+        auto open = [&](uint32_t node, uint32_t len, uint32_t& gt, uint32_t& gl, uint32_t& lt, uint32_t& ll) {
+            const uint32_t ch = __float_as_uint(nodes[2 * node + 1].w);
+            gt = ch;
+            lt = ch + 1;
+            ll = __float_as_uint(nodes[2 * ch].w) - __float_as_uint(nodes[2 * (ch + 1)].w);
+            gl = len - ll;
+        };
+        if (!internal(b, blen)) {
+            c[0] = b;
+            cl[0] = blen;
+            m = 1;  // a small root: one leaf child
+        } else {
+            open(b, blen, c[0], cl[0], c[1], cl[1]);
+            m = 2;
+            while (m < 8) {
+                int pick = -1;
+                float psa = -1.0f;
+                for (uint32_t j = 0; j < m; ++j) {
+                    if (!internal(c[j], cl[j])) continue;
+                    const float sa = box_sa(nodes[2 * c[j]], nodes[2 * c[j] + 1]);
+                    if (sa > psa) {
+                        psa = sa;
+                        pick = (int)j;
+                    }
+                }
+                if (pick < 0) break;
+                open(c[pick], cl[pick], c[pick], cl[pick], c[m], cl[m]);
+                ++m;
+            }
+        }
+        uint32_t nint = 0;
+        float4 blo[8], bhi[8];
+        float lo[3] = {__int_as_float(0x7F800000), __int_as_float(0x7F800000), __int_as_float(0x7F800000)};
+        float hi[3] = {__int_as_float(0xFF800000), __int_as_float(0xFF800000), __int_as_float(0xFF800000)};
+        for (uint32_t j = 0; j < m; ++j) {
+            blo[j] = nodes[2 * c[j]];
+            bhi[j] = nodes[2 * c[j] + 1];
+            if (internal(c[j], cl[j])) ++nint;
+            lo[0] = fminf(lo[0], blo[j].x);
+            lo[1] = fminf(lo[1], blo[j].y);
+            lo[2] = fminf(lo[2], blo[j].z);
+            hi[0] = fmaxf(hi[0], bhi[j].x);
+            hi[1] = fmaxf(hi[1], bhi[j].y);
+            hi[2] = fmaxf(hi[2], bhi[j].z);
+        }
+        const uint32_t base = nint ? atomicAdd(counter, nint) : 0u;
+        if (base + nint > cap) {
+            atomicExch(err, 3);
+            continue;
+        }
+        WNode out;
+        out.px = lo[0];
+        out.py = lo[1];
+        out.pz = lo[2];
+        out.nchild = (uint8_t)m;
+        out.pad[0] = out.pad[1] = 0;
+        // smallest step 2^k with p + 255 * 2^k >= the node's maximum, per axis
+        for (int a = 0; a < 3; ++a) {
+            const float ext = __fsub_rn(hi[a], lo[a]);
+            int k = -126;
+            if (ext > 0.0f) {
+                int ex;
+                frexpf(__fdiv_rn(ext, 255.0f), &ex);  // ext / 255 < 2^ex
+                k = max(ex - 1, -126);
+                while (k < 127 && wdeq(lo[a], 255u, wstep((uint8_t)(k + 127))) < hi[a]) ++k;
+            }
+            out.e[a] = (uint8_t)(k + 127);
+        }
+        const float p[3] = {lo[0], lo[1], lo[2]};
+        uint32_t next = base;
+        for (uint32_t j = 0; j < 8; ++j) {
+            if (j >= m) {
+                for (int a = 0; a < 3; ++a) out.qlo[a][j] = out.qhi[a][j] = 0;
+                out.ref[j] = 0;
+                out.cnt[j] = 0;
+                continue;
+            }
+            const float cl3[3] = {blo[j].x, blo[j].y, blo[j].z}, ch3[3] = {bhi[j].x, bhi[j].y, bhi[j].z};
+            for (int a = 0; a < 3; ++a) {
+                const float st = wstep(out.e[a]);
+                const float ql = floorf(__fdiv_rn(__fsub_rn(cl3[a], p[a]), st));
+                const float qh = ceilf(__fdiv_rn(__fsub_rn(ch3[a], p[a]), st));
+                uint32_t qa = (uint32_t)fminf(fmaxf(ql, 0.0f), 255.0f);
+                uint32_t qb = (uint32_t)fminf(fmaxf(qh, 0.0f), 255.0f);
+                while (qa > 0 && wdeq(p[a], qa, st) > cl3[a]) --qa;
+                while (qb < 255 && wdeq(p[a], qb, st) < ch3[a]) ++qb;
+                out.qlo[a][j] = (uint8_t)qa;
+                out.qhi[a][j] = (uint8_t)qb;
+            }
+            if (internal(c[j], cl[j])) {
+                out.ref[j] = next;
+                out.cnt[j] = 0;
+                binid[next] = c[j];
+                binlen[next] = cl[j];
+                ++next;
+            } else {
+                if (cl[j] > 255u) atomicExch(err, 4);
+                out.ref[j] = __float_as_uint(blo[j].w) | kWideLeaf;
+                out.cnt[j] = (uint8_t)min(cl[j], 255u);
+            }
+        }
+        wn[w] = out;
+    }
+}
+
+// The next level's range: the slots taken by the level that just ran.
+__global__ void wide_advance_kernel(const uint32_t* cur, uint32_t* next, const uint32_t* counter) {
+    next[0] = cur[1];
+    next[1] = *counter;
+}
+
+// Closest hit through the wide BVH: the hit children of a node in order of
+// entry distance; leaf children's triangles tested at once, internal ones
+// pushed (with their entry distance, so that a popped node already beyond
+// the closest hit is skipped). Same triangle test and tie rule as the binary
+// traversal, and conservative boxes, so the same hits as brute force.
+__global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict__ wn,
+                                                         const TriRec* __restrict__ tris,
+                                                         const float4* __restrict__ rays, uint32_t n_rays,
+                                                         float* __restrict__ hit_t,
+                                                         uint32_t* __restrict__ hit_prim, Counts* counts,
+                                                         int* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
+    if (i < n_rays) {
+        const float4 o = rays[2 * i], d = rays[2 * i + 1];
+        const float ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
+        float best = __int_as_float(0x7F800000);
+        uint32_t best_prim = kNoHit;
+        uint32_t st_node[kWideStack];
+        float st_t[kWideStack];
+        int sp = 0;
+        st_node[sp] = 0;
+        st_t[sp] = 0.0f;
+        ++sp;
+        bool overflow = false;
+        while (sp > 0) {
+            --sp;
+            if (st_t[sp] > best) continue;
+            const uint32_t ni = st_node[sp];
+            c_nodes++;
+            const float4* q4 = reinterpret_cast<const float4*>(wn + ni);
+            const float4 h0 = q4[0], h1 = q4[1], h2 = q4[2], h3 = q4[3], h4 = q4[4], h5 = q4[5], h6 = q4[6];
+            const uint32_t ew = __float_as_uint(h0.w);
+            const float sx = wstep(ew & 0xFFu), sy = wstep((ew >> 8) & 0xFFu), sz = wstep((ew >> 16) & 0xFFu);
+            const uint32_t m = ew >> 24;
+            const uint32_t ql[3][2] = {{__float_as_uint(h1.x), __float_as_uint(h1.y)},
+                                       {__float_as_uint(h1.z), __float_as_uint(h1.w)},
+                                       {__float_as_uint(h2.x), __float_as_uint(h2.y)}};
+            const uint32_t qh[3][2] = {{__float_as_uint(h2.z), __float_as_uint(h2.w)},
+                                       {__float_as_uint(h3.x), __float_as_uint(h3.y)},
+                                       {__float_as_uint(h3.z), __float_as_uint(h3.w)}};
+            const uint32_t refs[8] = {__float_as_uint(h4.x), __float_as_uint(h4.y), __float_as_uint(h4.z),
+                                      __float_as_uint(h4.w), __float_as_uint(h5.x), __float_as_uint(h5.y),
+                                      __float_as_uint(h5.z), __float_as_uint(h5.w)};
+            const uint32_t cnt2[2] = {__float_as_uint(h6.x), __float_as_uint(h6.y)};
+            float ent[8];
+            uint32_t hitm = 0, leafm = 0;
+#pragma unroll
+            for (uint32_t j = 0; j < 8; ++j) {
+                ent[j] = __int_as_float(0x7FFFFFFF);
+                if (j < m) {
+                    const uint32_t sh = (j & 3u) * 8u, wd = j >> 2;
+                    const float4 lo = make_float4(wdeq(h0.x, (ql[0][wd] >> sh) & 0xFFu, sx),
+                                                  wdeq(h0.y, (ql[1][wd] >> sh) & 0xFFu, sy),
+                                                  wdeq(h0.z, (ql[2][wd] >> sh) & 0xFFu, sz), 0.0f);
+                    const float4 hi = make_float4(wdeq(h0.x, (qh[0][wd] >> sh) & 0xFFu, sx),
+                                                  wdeq(h0.y, (qh[1][wd] >> sh) & 0xFFu, sy),
+                                                  wdeq(h0.z, (qh[2][wd] >> sh) & 0xFFu, sz), 0.0f);
+                    c_boxes++;
+                    ent[j] = box_entry(o.x, o.y, o.z, ix, iy, iz, lo, hi, best);
+                    if (ent[j] <= best) hitm |= 1u << j;
+                    if (refs[j] & kWideLeaf) leafm |= 1u << j;
+                }
+            }
+            // leaf children, nearest first (selections over a bit mask: no
+            // indexed arrays, everything stays in registers)
+            uint32_t lm = hitm & leafm;
+            while (lm) {
+                float be = __int_as_float(0x7F800000);
+                uint32_t bj = 0, br = 0, bc = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j)
+                    if (((lm >> j) & 1u) && !(ent[j] >= be)) {
+                        be = ent[j];
+                        bj = j;
+                        br = refs[j];
+                        bc = (cnt2[j >> 2] >> ((j & 3u) * 8u)) & 0xFFu;
+                    }
+                lm &= ~(1u << bj);
+                if (be > best) continue;
+                const uint32_t start = br & ~kWideLeaf;
+                for (uint32_t q = start; q < start + bc; ++q) {
+                    const TriRec t = tris[q];
+                    c_tris++;
+                    const float tt = intersect_tri(o.x, o.y, o.z, d.x, d.y, d.z, t);
+                    const uint32_t prim = __float_as_uint(t.a.w);
+                    if (tt >= 0.0f && (tt < best || (tt == best && prim < best_prim))) {
+                        best = tt;
+                        best_prim = prim;
+                    }
+                }
+            }
+            // internal children pushed farthest first (popped nearest first)
+            uint32_t im = hitm & ~leafm;
+            while (im) {
+                float be = -1.0f;
+                uint32_t bj = 0, br = 0;
+#pragma unroll
+                for (uint32_t j = 0; j < 8; ++j)
+                    if (((im >> j) & 1u) && ent[j] >= be) {
+                        be = ent[j];
+                        bj = j;
+                        br = refs[j];
+                    }
+                im &= ~(1u << bj);
+                if (be > best) continue;
+                if (sp >= kWideStack) {
+                    overflow = true;
+                    break;
+                }
+                st_node[sp] = br;
+                st_t[sp] = be;
+                ++sp;
+            }
+            if (overflow) {
+                atomicExch(err, 1);
+                break;
+            }
+        }
+        hit_t[i] = best_prim == kNoHit ? -1.0f : best;
+        hit_prim[i] = best_prim;
+    }
+    if (counts) {
+        unsigned long long a = c_nodes, b = c_boxes, c = c_tris;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(kFull, a, off);
+            b += __shfl_down_sync(kFull, b, off);
+            c += __shfl_down_sync(kFull, c, off);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicAdd(&counts->nodes, a);
+            atomicAdd(&counts->boxes, b);
+            atomicAdd(&counts->tris, c);
+        }
+    }
+}
+
 }  // namespace mgbvh_trace
 
 using namespace mgbvh_trace;
@@ -246,6 +561,13 @@ struct mgbvh_tracer {
     int* d_err = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
+    // the wide BVH of the bound tree (mgbvh_tracer_build_wide)
+    WNode* wide = nullptr;
+    uint32_t* wbin = nullptr;
+    uint32_t* wlen = nullptr;
+    uint32_t* wmeta = nullptr;  // [0..1], [2..3]: level ranges; [4]: slots taken
+    size_t wide_cap = 0;
+    uint32_t wide_count = 0;
 };
 
 namespace {
@@ -281,6 +603,10 @@ void mgbvh_tracer_destroy(mgbvh_tracer* t) {
     if (!t) return;
     cudaSetDevice(t->device);
     if (t->tris) cudaFree(t->tris);
+    if (t->wide) cudaFree(t->wide);
+    if (t->wbin) cudaFree(t->wbin);
+    if (t->wlen) cudaFree(t->wlen);
+    if (t->wmeta) cudaFree(t->wmeta);
     if (t->d_counts) cudaFree(t->d_counts);
     if (t->d_err) cudaFree(t->d_err);
     if (t->ev0) cudaEventDestroy(t->ev0);
@@ -319,6 +645,105 @@ int mgbvh_tracer_set_blas_dev(mgbvh_tracer* t, const mgbvh_node* d_nodes, uint32
     t->lens = d_lens;
     t->node_count = node_count;
     t->n_tris = triangle_count;
+    t->wide_count = 0;  // a wide BVH of an earlier tree no longer applies
+    return MGBVH_OK;
+}
+
+int mgbvh_tracer_build_wide(mgbvh_tracer* t, void* stream, uint32_t* out_wide_count) {
+    if (!t || !t->nodes) return MGBVH_ERR_INVALID_ARG;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    const size_t cap = t->node_count;  // one wide node per internal binary node at most (or the leaf root)
+    if (t->wide_cap < cap) {
+        if (t->wide) cudaFree(t->wide);
+        if (t->wbin) cudaFree(t->wbin);
+        if (t->wlen) cudaFree(t->wlen);
+        t->wide = nullptr;
+        t->wbin = nullptr;
+        t->wlen = nullptr;
+        t->wide_cap = 0;
+        if (cudaMalloc(&t->wide, sizeof(WNode) * cap) != cudaSuccess ||
+            cudaMalloc(&t->wbin, sizeof(uint32_t) * cap) != cudaSuccess ||
+            cudaMalloc(&t->wlen, sizeof(uint32_t) * cap) != cudaSuccess)
+            return MGBVH_ERR_CUDA;
+        t->wide_cap = cap;
+    }
+    if (!t->wmeta && cudaMalloc(&t->wmeta, 8 * sizeof(uint32_t)) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const uint32_t init[8] = {0, 1, 0, 0, 1, 0, 0, 0};  // level 0 = [0, 1), one slot taken
+    uint32_t hm[8];
+    if (cudaMemcpyAsync(t->wmeta, init, sizeof(init), cudaMemcpyHostToDevice, sm) != cudaSuccess ||
+        cudaMemsetAsync(t->wbin, 0, sizeof(uint32_t), sm) != cudaSuccess ||  // wide root = binary root
+        cudaMemcpyAsync(t->wlen, &t->n_tris, sizeof(uint32_t), cudaMemcpyHostToDevice, sm) != cudaSuccess ||
+        cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    const float4* nodes = reinterpret_cast<const float4*>(t->nodes);
+    int level = 0;
+    bool done = false;
+    while (!done) {
+        for (int k = 0; k < 8; ++k, ++level) {
+            uint32_t* cur = t->wmeta + 2 * (level & 1);
+            uint32_t* nxt = t->wmeta + 2 * ((level + 1) & 1);
+            wide_level_kernel<<<148 * 8, 128, 0, sm>>>(nodes, t->wbin, t->wlen, cur, t->wmeta + 4, t->wide,
+                                                       (uint32_t)cap, t->d_err);
+            wide_advance_kernel<<<1, 1, 0, sm>>>(cur, nxt, t->wmeta + 4);
+        }
+        int herr = 0;
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(hm, t->wmeta, sizeof(hm), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+            cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+            cudaStreamSynchronize(sm) != cudaSuccess)
+            return MGBVH_ERR_CUDA;
+        if (herr) return herr == 4 ? MGBVH_ERR_UNSUPPORTED : MGBVH_ERR_CAPACITY;
+        const uint32_t* cur = hm + 2 * (level & 1);
+        done = cur[0] == cur[1];
+        if (!done && level >= 256) return MGBVH_ERR_CAPACITY;  // deeper than any tree of the builder
+    }
+    t->wide_count = hm[4];
+    if (out_wide_count) *out_wide_count = t->wide_count;
+    return MGBVH_OK;
+}
+
+int mgbvh_tracer_wide_nodes(mgbvh_tracer* t, const void** d_wide_nodes, uint32_t* wide_count) {
+    if (!t || !t->wide_count) return MGBVH_ERR_INVALID_ARG;
+    if (d_wide_nodes) *d_wide_nodes = t->wide;
+    if (wide_count) *wide_count = t->wide_count;
+    return MGBVH_OK;
+}
+
+int mgbvh_trace_closest_wide_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_rays, float* d_hit_t,
+                                 uint32_t* d_hit_prim, uint64_t* out_counts, double* out_seconds,
+                                 void* stream) {
+    if (!t || !t->wide_count || (n_rays && (!d_rays || !d_hit_t || !d_hit_prim))) return MGBVH_ERR_INVALID_ARG;
+    if (n_rays == 0) return MGBVH_OK;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(t->d_counts, 0, sizeof(Counts), sm) != cudaSuccess ||
+        cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    cudaEventRecord(t->ev0, sm);
+    trace_wide_kernel<<<(n_rays + 127) / 128, 128, 0, sm>>>(t->wide, t->tris,
+                                                             reinterpret_cast<const float4*>(d_rays), n_rays,
+                                                             d_hit_t, d_hit_prim,
+                                                             out_counts ? t->d_counts : nullptr, t->d_err);
+    cudaEventRecord(t->ev1, sm);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    Counts hc;
+    int herr = 0;
+    if (cudaMemcpyAsync(&hc, t->d_counts, sizeof(Counts), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (herr) return MGBVH_ERR_CAPACITY;  // traversal stack would have overflowed
+    if (out_counts) {
+        out_counts[0] = hc.nodes;
+        out_counts[1] = hc.boxes;
+        out_counts[2] = hc.tris;
+    }
+    if (out_seconds) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t->ev0, t->ev1);
+        *out_seconds = ms * 1e-3;
+    }
     return MGBVH_OK;
 }
 
