@@ -43,7 +43,13 @@ namespace mgbvh {
 constexpr uint32_t kMediumMax = 1024;
 constexpr uint32_t kTile = 2048;
 constexpr int kTileThreads = 256;
-constexpr int kMediumWarps = 4;
+#ifndef MGBVH_MEDIUM_WARPS
+#define MGBVH_MEDIUM_WARPS 4  // warps per subtree CTA (tuning knob)
+#endif
+#ifndef MGBVH_MEDIUM_SMALL_CTAS
+#define MGBVH_MEDIUM_SMALL_CTAS 5  // CTAs per SM of the 512-object instance (tuning knob)
+#endif
+constexpr int kMediumWarps = MGBVH_MEDIUM_WARPS;
 constexpr int kMediumThreads = kMediumWarps * 32;
 constexpr uint32_t kBinWords = 3 * 32 * 7;  // [axis][bin]{count, lo key xyz, hi key xyz}
 constexpr uint32_t kNone = 0xFFFFFFFFu;
@@ -1631,7 +1637,8 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
 // kLearn: with the learned form's hook (network proposals, training samples);
 // plain builds run the instantiation without it.
 template <bool kLearn, uint32_t kCap>
-__global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : 1) medium_kernel(const Task* __restrict__ tasks,
+__global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : MGBVH_MEDIUM_SMALL_CTAS)
+    medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
                                                                 Learn LN) {
@@ -2250,7 +2257,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
         // subtrees hold at most P.medium_max objects: the smaller-capacity
         // instance leaves room for more CTAs per SM
         const bool lrn = LN.w || LN.samples, small_cap = P.medium_max <= kMediumSmallCap;
-        const uint32_t mgrid_s = std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * 5u);
+        const uint32_t mgrid_s =
+            std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * (uint32_t)MGBVH_MEDIUM_SMALL_CTAS);
         if (lrn && small_cap)
             medium_kernel<true, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
                 P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
