@@ -733,9 +733,13 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
     box_empty(lt);
     box_empty(gt);
     uint32_t nl = 0, ng = 0;
+    uint32_t cj[17];
+#pragma unroll
+    for (uint32_t j = 0; j < 17; ++j) cj[j] = rb[j * 7];  // all counts in flight at once
+#pragma unroll
     for (uint32_t j = 0; j < 17; ++j) {
         const uint32_t* b = rb + j * 7;
-        const uint32_t c = b[0];
+        const uint32_t c = cj[j];
         if (c == 0) continue;
         float* bx = j <= k ? lt : gt;
         if (j <= k)
@@ -1254,9 +1258,14 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
                 wb[i] = f7 == 0 ? 0u : (f7 <= 3 ? kKeyPosInf : kKeyNegInf);
             }
             __syncwarp();
-            for (uint32_t j = lane; j < n; j += 32) {
-                float lo[3], hi[3];
-                fetch(j, lo, hi);
+            // lane q * 16 + k holds threshold k of proposal q; the searches read it by shuffle
+            const float lthr = proposal_threshold((lane >> 4) ? pc[1] : pc[0], (lane >> 4) ? pe[1] : pe[0],
+                                                  (lane >> 4) ? pb[1] : pb[0], lane & 15u);
+            for (uint32_t j0 = 0; j0 < n; j0 += 32) {  // warp-uniform trip count
+                const uint32_t j = j0 + lane;
+                const bool valid = j < n;
+                float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+                if (valid) fetch(j, lo, hi);
 #pragma unroll
                 for (int q = 0; q < 2; ++q) {
                     if (!act[q]) continue;  // warp-uniform
@@ -1264,14 +1273,16 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
                     uint32_t a = 0, b = 16;  // interval = number of thresholds thr with !(c < thr)
 #pragma unroll
                     for (int it = 0; it < 5; ++it) {
+                        const uint32_t mid = min((a + b) >> 1, 15u);
+                        const float tm = __shfl_sync(kFull, lthr, q * 16 + mid);
                         if (a < b) {
-                            const uint32_t mid = (a + b) >> 1;
-                            if (!(c < proposal_threshold(pc[q], pe[q], pb[q], mid)))
+                            if (!(c < tm))
                                 a = mid + 1;
                             else
                                 b = mid;
                         }
                     }
+                    if (!valid) continue;
                     uint32_t* w = wb + (q * 17 + a) * 7;
                     atomicAdd(w, 1u);
                     atomicMin(w + 1, fkey(lo[0]));

@@ -28,9 +28,10 @@ constexpr uint32_t kSampleLargeMax = 8192;  // level-pass nodes sampled up to th
 
 // Threshold k (0..15) inside proposal bucket `bucket` (0..15) of an axis with
 // centroid range [cmin, cmin + ext]: cmin + ext * ((bucket * 16 + k + 1) / 256).
-// Nondecreasing in bucket * 16 + k.
+// Nondecreasing in bucket * 16 + k. The fraction is exact: an integer of at
+// most 256 times 2^-8 (the same value a division by 256 gives).
 __device__ __forceinline__ float proposal_threshold(float cmin, float ext, uint32_t bucket, uint32_t k) {
-    return __fadd_rn(cmin, __fmul_rn(ext, __fdiv_rn((float)(bucket * 16u + k + 1u), 256.0f)));
+    return __fadd_rn(cmin, __fmul_rn(ext, __fmul_rn((float)(bucket * 16u + k + 1u), 0.00390625f)));
 }
 
 // A level-pass node waiting for its proposals to be scored.
