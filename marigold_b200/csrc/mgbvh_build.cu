@@ -2079,6 +2079,7 @@ struct mgbvh_ctx {
     uint32_t learn_cap = 0;
     uint32_t* learn_count = nullptr;
     Counters* h_ctr = nullptr;
+    Counters* h_init = nullptr;  // pinned, constant: the counters every build starts from
 };
 
 namespace {
@@ -2177,8 +2178,13 @@ const char* site_text(uint32_t site) {
 // fixed_levels > 0: launch exactly that many level passes and never read
 // back (the form a CUDA graph captures); 0: read the next level's count at
 // the end of each batch of levels.
+// optimistic (single builds with a level-count hint from an earlier build):
+// launch exactly the hinted number of levels and go on to the subtree
+// kernels without a host read in between; the caller checks afterwards that
+// no task was left for a further level (and rebuilds if one was).
 int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, Rec* rec0, Rec* rec1,
-                 bool has_large, uint32_t fixed_levels, uint32_t& launches, uint32_t& levels) {
+                 bool has_large, uint32_t fixed_levels, uint32_t& launches, uint32_t& levels,
+                 bool optimistic = false) {
     const cudaStream_t sm = ctx->stream;
     Counters* d_ctr = O.ctr;
     // Level passes over the large nodes. Kernels read their task and tile
@@ -2197,8 +2203,9 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     LN.count = ctx->learn_count;
     bool first_batch = true;
     while (more) {
-        const uint32_t batch =
-            fixed_levels ? fixed_levels : (first_batch ? std::max(ctx->levels_hint, 4u) : 2u);
+        const uint32_t batch = fixed_levels ? fixed_levels
+                                            : (optimistic ? ctx->levels_hint
+                                                          : (first_batch ? std::max(ctx->levels_hint, 4u) : 2u));
         first_batch = false;
         for (uint32_t bl = 0; bl < batch; ++bl, ++level) {
             const uint32_t lv = level & 1u, nx = lv ^ 1u;
@@ -2251,14 +2258,14 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
         }
         MG_CUDA(cudaGetLastError());
-        if (fixed_levels) break;
+        if (fixed_levels || optimistic) break;
         MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
         MG_CUDA(cudaStreamSynchronize(sm));
         if (ctx->h_ctr->error) break;
         more = ctx->h_ctr->lvl[level & 1u][0] > 0;
     }
     if (has_large) {
-        if (!fixed_levels) ctx->levels_hint = level;
+        if (!fixed_levels && !optimistic) ctx->levels_hint = level;
         levels = level;
     }
     if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
@@ -2342,11 +2349,9 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     P.adaptive_steps = st->adaptive_steps;
     P.medium_max = ctx->medium_max;
 
-    Counters init;
-    std::memset(&init, 0, sizeof(init));
-    for (int i = 0; i < 12; ++i) init.root_keys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
     Counters* d_ctr = P_<Counters>(ctx->ctr);
-    MG_CUDA(cudaMemcpyAsync(d_ctr, &init, sizeof(init), cudaMemcpyHostToDevice, sm));
+    // from pinned memory: an asynchronous copy (a pageable source would stall the host)
+    MG_CUDA(cudaMemcpyAsync(d_ctr, ctx->h_init, sizeof(Counters), cudaMemcpyHostToDevice, sm));
     MG_CUDA(cudaMemsetAsync(ctx->used.p, 0, (size_t)C.nodes, sm));
 
     Out O;
@@ -2388,12 +2393,19 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     uint32_t launches = 2, levels = 0;
     (void)ntiles0;
 
-    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, cls == 3, 0, launches, levels)) != MGBVH_OK)
+    const bool optimistic = cls == 3 && ctx->levels_hint > 0;
+    if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, cls == 3, 0, launches, levels, optimistic)) != MGBVH_OK)
         return rc;
     MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
     MG_CUDA(cudaStreamSynchronize(sm));
     const Counters hc = *ctx->h_ctr;
+    if (optimistic && hc.lvl[levels & 1u][0] != 0) {
+        // the tree needs more level passes than the hint: build again, reading
+        // the task count after every batch of levels
+        ctx->levels_hint = 0;
+        return run_build(ctx, in, st, d_nodes, cap, d_lens, d_perm, out_count, stats);
+    }
     if (hc.error) {
         return fail(ctx, (int)hc.error, site_text(hc.error_site));
     }
@@ -3020,6 +3032,7 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
         cudaEventCreate(&ctx->evp[0]) != cudaSuccess || cudaEventCreate(&ctx->evp[1]) != cudaSuccess ||
         cudaEventCreate(&ctx->evp[2]) != cudaSuccess ||
         cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
+        cudaMallocHost(&ctx->h_init, sizeof(Counters)) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)sizeof(MediumSmem)) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<true, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -3033,6 +3046,8 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
         mgbvh_destroy(ctx);
         return MGBVH_ERR_CUDA;
     }
+    std::memset(ctx->h_init, 0, sizeof(Counters));
+    for (int i = 0; i < 12; ++i) ctx->h_init->root_keys[i] = ((i % 6) < 3) ? kKeyPosInf : kKeyNegInf;
     ctx->own_stream = true;
     *out_ctx = ctx;
     return MGBVH_OK;
@@ -3052,6 +3067,7 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
+    if (ctx->h_init) cudaFreeHost(ctx->h_init);
     if (ctx->pin) cudaFreeHost(ctx->pin);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);

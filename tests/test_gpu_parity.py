@@ -8,7 +8,7 @@ reference (treecheck.check_tree) are checked on the GPU result as well.
 import numpy as np
 import pytest
 
-from marigold_b200 import synth
+from marigold_b200 import _lib, synth
 from tests.gpuhelp import gpu_build
 from tests.treecheck import check_tree, compare_exact
 
@@ -169,3 +169,22 @@ def test_device_entry_point_matches_host_entry_point(oracle, gpu_ctx):
     msg = compare_exact(gw, lens.cpu().numpy().view(np.uint32), perm.cpu().numpy().view(np.uint32),
                         o["nodes"], o["lens"], o["perm"])
     assert msg is None, msg
+
+
+def test_level_hint_across_meshes(oracle):
+    """A context launches the level passes its previous build needed without
+    reading counts in between; a deeper tree than the hint is rebuilt with
+    counts read, a shallower one runs empty passes. Every tree equals the
+    oracle's."""
+    from marigold_b200 import synth as _synth
+    ctx = _lib.Context(0)
+    try:
+        small = _synth.random_triangles(5000, seed=71)
+        large = _synth.random_triangles(200000, seed=72)
+        for v, t in (small, large, large, small, large):
+            g = gpu_build(ctx, v, t)
+            o = oracle.build(v, t)
+            assert g["status"] == o["status"] == 0
+            assert compare_exact(g["nodes"], g["lens"], g["perm"], o["nodes"], o["lens"], o["perm"]) is None
+    finally:
+        ctx.close()
