@@ -86,6 +86,20 @@ struct Decision {
 
 // ---------------------------------------------------------------- helpers
 
+// Grows the lt (k[0..5]: min keys xyz, max keys xyz) or gt (k[6..11])
+// centroid key bounds by centroid c; selects with constant indexes keep k in
+// registers.
+__device__ __forceinline__ void grow_keys12(uint32_t* k, bool lt, const float* c) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t f = fkey(c[a]);
+        k[a] = lt ? min(k[a], f) : k[a];
+        k[3 + a] = lt ? max(k[3 + a], f) : k[3 + a];
+        k[6 + a] = lt ? k[6 + a] : min(k[6 + a], f);
+        k[9 + a] = lt ? k[9 + a] : max(k[9 + a], f);
+    }
+}
+
 __device__ __forceinline__ void block_reduce_keys_to_global(uint32_t* keys /*12*/, uint32_t* smem12,
                                                             uint32_t* global12) {
     // keys[0..5]: min keys; keys[6..11] : max keys ; layout per call site
@@ -350,8 +364,18 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_ke
             }
         }
         __syncthreads();
-        for (uint32_t w = threadIdx.x; w < 96; w += blockDim.x)
-            tile_hist[(size_t)w * cap_tiles + tile] = sb[w * 7];
+        if (threadIdx.x < 96) {
+            // per axis (one warp each): the tile's count of objects in the
+            // bins below each bin, an exclusive scan over the 32 bins
+            const uint32_t lane = threadIdx.x & 31u, c = sb[threadIdx.x * 7];
+            uint32_t inc = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t u = __shfl_up_sync(kFull, inc, off);
+                if (lane >= static_cast<uint32_t>(off)) inc += u;
+            }
+            tile_hist[(size_t)threadIdx.x * cap_tiles + tile] = inc - c;
+        }
         uint32_t* gb = bins + (size_t)ti * kBinWords;
         for (uint32_t k = threadIdx.x; k < kBinWords; k += blockDim.x) {
             const uint32_t bin = k / 7u, f = k % 7u;
@@ -372,7 +396,7 @@ struct EvalArgs {
     uint32_t lv;  // level parity: counts in ctr->lvl[lv], next level's in ctr->lvl[lv ^ 1]
     const uint32_t* bins;
     const uint32_t* cbkeys;
-    const uint32_t* tile_hist;
+    const uint32_t* tile_hist;  // [axis * 32 + bin][tile]: objects of the tile in the axis's bins below bin
     uint32_t* tile_lt;
     Decision* dec;
     Task* next_tasks;
@@ -389,36 +413,39 @@ struct EvalArgs {
     int lgate;
     LvlRefine* refine;
     uint32_t* rbins;
-    const uint32_t* tile_hist2;  // [proposal * 17 + interval][tile]
+    const uint32_t* tile_hist2;  // [proposal * 17 + interval][tile]: objects in intervals 0..interval
 };
 
 // Writes the node and its children of a decided split: the per-tile lt
-// counts (exclusive scan across the node's tiles of the sum of `nrows`
-// histogram rows from row0: the bins, or the intervals, left of the split),
-// the node record, and each child as a leaf, a next-level task, a medium or
-// a small subtree.
+// counts (exclusive scan across the node's tiles of histogram row `row`:
+// each tile's objects left of the split), the node record, and each child as
+// a leaf, a next-level task, a medium or a small subtree. Each lane scans a
+// contiguous run of the node's tiles (independent loads), runs joined by a
+// warp scan.
 __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane,
-                           const Task& t, Decision& d, const uint32_t* hist, uint32_t row0,
-                           uint32_t nrows) {
+                           const Task& t, Decision& d, const uint32_t* hist, uint32_t row) {
     const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-    uint32_t carry = 0;
-    for (uint32_t b0 = 0; b0 < t.ntiles; b0 += 32) {
-        const uint32_t ti = b0 + lane;
-        uint32_t v = 0;
-        if (ti < t.ntiles) {
-            const uint32_t* h = hist + (size_t)row0 * A.cap_tiles + t.tile0 + ti;
-            for (uint32_t b = 0; b < nrows; ++b) v += h[(size_t)b * A.cap_tiles];
-        }
-        uint32_t inc = v;
+    const uint32_t* h = hist + (size_t)row * A.cap_tiles + t.tile0;
+    uint32_t* lt = A.tile_lt + t.tile0;
+    const uint32_t per = (t.ntiles + 31u) >> 5;
+    const uint32_t i0 = min(lane * per, t.ntiles), i1 = min(i0 + per, t.ntiles);
+    uint32_t sum = 0;
+#pragma unroll 8
+    for (uint32_t i = i0; i < i1; ++i) sum += h[i];
+    uint32_t inc = sum;
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const uint32_t u = __shfl_up_sync(kFull, inc, off);
-            if (lane >= static_cast<uint32_t>(off)) inc += u;
-        }
-        if (ti < t.ntiles) A.tile_lt[t.tile0 + ti] = carry + inc - v;
-        carry += __shfl_sync(kFull, inc, 31);
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t u = __shfl_up_sync(kFull, inc, off);
+        if (lane >= static_cast<uint32_t>(off)) inc += u;
     }
-    if (carry != d.n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
+    const uint32_t total = __shfl_sync(kFull, inc, 31);
+    uint32_t run = inc - sum;
+    for (uint32_t i = i0; i < i1; ++i) {
+        const uint32_t v = h[i];
+        lt[i] = run;
+        run += v;
+    }
+    if (total != d.n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
     warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, t.len, t.pair, lane);
     if (lane == 0) atomicMax(&O.ctr->height, t.depth);
     const uint32_t n_gt = t.len - d.n_lt;
@@ -619,7 +646,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
             return;
         }
     }
-    emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u, d.split_bin);
+    emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u + d.split_bin);
 }
 
 __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
@@ -633,7 +660,7 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
 // Interval bins of the pending nodes: for each proposal, the node's objects
 // by the interval of their centroid among the proposal's 16 thresholds
 // (count + AABB keys), with shared-memory atomics, merged into the node's
-// global interval bins; per-tile counts go to tile_hist2. Grid-stride over
+// global interval bins; per-tile running counts go to tile_hist2. Grid-stride over
 // the level's tiles.
 __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys,
@@ -699,8 +726,19 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
             }
         }
         __syncthreads();
-        for (uint32_t r = threadIdx.x; r < 34; r += blockDim.x)
-            tile_hist2[(size_t)r * cap_tiles + tile] = sb[r * 7];
+        if (threadIdx.x < 64) {
+            // per proposal (one warp each): the tile's count of objects in
+            // intervals 0..j, an inclusive scan over the 17 intervals
+            const uint32_t lane = threadIdx.x & 31u, p = threadIdx.x >> 5;
+            const uint32_t c = lane < 17 ? sb[(p * 17 + lane) * 7] : 0u;
+            uint32_t inc = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t u = __shfl_up_sync(kFull, inc, off);
+                if (lane >= static_cast<uint32_t>(off)) inc += u;
+            }
+            if (lane < 17) tile_hist2[(size_t)(p * 17 + lane) * cap_tiles + tile] = inc;
+        }
         uint32_t* gb = rbins + (size_t)ti * kRBinWords;
         for (uint32_t k = threadIdx.x; k < kRBinWords; k += blockDim.x) {
             const uint32_t r = k / 7u, f7 = k % 7u;
@@ -766,9 +804,9 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
             d.gtb[i] = __shfl_sync(kFull, gt[i], src);
         }
         if (lane == 0) atomicAdd(&O.ctr->learned, 1u);
-        emit_split(A, P, O, w, lane, t, d, A.tile_hist2, (src >> 4) * 17u, (src & 15u) + 1u);
+        emit_split(A, P, O, w, lane, t, d, A.tile_hist2, (src >> 4) * 17u + (src & 15u));
     } else {
-        emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u, d.split_bin);
+        emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u + d.split_bin);
     }
 }
 
@@ -919,7 +957,11 @@ __global__ void __launch_bounds__(256) lvl_sample_kernel(const Task* __restrict_
 // children's centroid bounds.
 constexpr uint32_t kPartPerLane = kTile / kTileThreads;  // 8
 
-__global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
+#ifndef MGBVH_PART_MIN_BLOCKS
+#define MGBVH_PART_MIN_BLOCKS 5  // CTAs per SM the register budget must allow (tuning knob)
+#endif
+
+__global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_kernel(
     const Task* __restrict__ tasks, const Decision* __restrict__ dec,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
     const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, uint32_t* next_cbkeys, uint32_t lv,
@@ -1003,13 +1045,8 @@ __global__ void __launch_bounds__(kTileThreads) lvl_part_kernel(
                     bad = true;  // inconsistent counts; never write outside the node
                 }
                 bad |= !box_contains(pred ? d.ltb : d.gtb, c0, c1, c2);
-                uint32_t* kk = pred ? k : k + 6;
-                kk[0] = min(kk[0], fkey(c0));
-                kk[1] = min(kk[1], fkey(c1));
-                kk[2] = min(kk[2], fkey(c2));
-                kk[3] = max(kk[3], fkey(c0));
-                kk[4] = max(kk[4], fkey(c1));
-                kk[5] = max(kk[5], fkey(c2));
+                const float c[3] = {c0, c1, c2};
+                grow_keys12(k, pred, c);
             }
             run += __popc(bal[j]);
         }
@@ -1140,12 +1177,7 @@ __device__ __forceinline__ uint32_t medium_partition(MS& S, uint32_t ib, uint32_
             const uint32_t dst = pr ? s + lt_run + __popc(m & below)
                                     : s + n_lt_expect + gt_run + __popc(vm & ~m & below);
             if (dst < s + n) S.idx[ib ^ 1u][dst] = static_cast<uint16_t>(r);
-            uint32_t* kk = pr ? k : k + 6;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                kk[a] = min(kk[a], fkey(c[a]));
-                kk[3 + a] = max(kk[3 + a], fkey(c[a]));
-            }
+            grow_keys12(k, pr, c);
         }
         lt_run += __popc(m);
         gt_run += __popc(vm & ~m);
@@ -1552,11 +1584,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                     const uint32_t r = S.idx[ob][p];
                     const float4 lo = S.rlo[r], hi = S.rhi[r];
                     const float c[3] = {center_of(lo.x, hi.x), center_of(lo.y, hi.y), center_of(lo.z, hi.z)};
-                    uint32_t* kk = p < s + m ? ck : ck + 6;
-                    for (int a = 0; a < 3; ++a) {
-                        kk[a] = min(kk[a], fkey(c[a]));
-                        kk[3 + a] = max(kk[3 + a], fkey(c[a]));
-                    }
+                    grow_keys12(ck, p < s + m, c);
                 }
             }
             // containment of centroids in child bounds (bvh/src/lib.rs:637-646)
