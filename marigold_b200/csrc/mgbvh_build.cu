@@ -475,6 +475,7 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     slot_tile = __shfl_sync(kFull, slot_tile, 0);
     slot_med = __shfl_sync(kFull, slot_med, 0);
     slot_small = __shfl_sync(kFull, slot_small, 0);
+#pragma unroll
     for (int c = 0; c < 2; ++c) {
         const uint32_t len = c == 0 ? n_gt : d.n_lt;
         const uint32_t start = c == 0 ? t.start + d.n_lt : t.start;
@@ -610,8 +611,8 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         return;
     }
     d.kind = 0;
-    d.cmin = cmn[d.axis];
-    d.ext = ext[d.axis];
+    d.cmin = sel3(cmn, d.axis);
+    d.ext = sel3(ext, d.axis);
     d.n_lt = win.n_lt;
     for (int i = 0; i < 6; ++i) {
         d.ltb[i] = win.lt[i];
@@ -779,12 +780,12 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
         const uint32_t* b = rb + j * 7;
         const uint32_t c = cj[j];
         if (c == 0) continue;
-        float* bx = j <= k ? lt : gt;
         if (j <= k)
             nl += c;
         else
             ng += c;
-        box_grow(bx, funkey(b[1]), funkey(b[2]), funkey(b[3]), funkey(b[4]), funkey(b[5]), funkey(b[6]));
+        box_grow2(lt, gt, j <= k, funkey(b[1]), funkey(b[2]), funkey(b[3]), funkey(b[4]), funkey(b[5]),
+                  funkey(b[6]));
     }
     const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
     uint64_t key = ~0ull;
@@ -1259,7 +1260,7 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
             }
         }
         if (lane == 0)
-            write_sample(LN, f, bk, ba, bthr, ba < 3 ? nd.cb[ba] : 0.0f, ba < 3 ? ext[ba] : 0.0f,
+            write_sample(LN, f, bk, ba, bthr, ba < 3 ? sel3(nd.cb, ba) : 0.0f, ba < 3 ? sel3(ext, ba) : 0.0f,
                          plain_ck, n, base + s - tbase);
     }
     if (LN.w) {
@@ -1477,15 +1478,19 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                 }
                 __syncwarp();
                 uint32_t cnt[3];
-                float box[3][6];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const uint32_t* bw = wb + (a * 32 + lane) * 7;
-                    cnt[a] = bw[0];
-                    for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
-                }
+                for (int a = 0; a < 3; ++a) cnt[a] = wb[(a * 32 + lane) * 7];
+                // each axis's bin read from the warp's bins as the sweep
+                // reaches it (fewer live registers)
                 Cand best;
-                binned_candidates(cnt, box, axis_ok, B, n, surface_area6(nd.b), P, lane, best);
+                binned_candidates_f(
+                    [&](uint32_t a, uint32_t& ca, float* ba) {
+                        const uint32_t* bw = wb + (a * 32 + lane) * 7;
+                        ca = bw[0];
+#pragma unroll
+                        for (int i = 0; i < 6; ++i) ba[i] = funkey(bw[1 + i]);
+                    },
+                    axis_ok, B, n, surface_area6(nd.b), P, lane, best);
                 const uint64_t wk = warp_min_key(best.key);
                 const uint32_t wlo = static_cast<uint32_t>(wk);
                 if (wlo == kNoKey) {
@@ -1518,12 +1523,13 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
             init_key12(ck);
             uint32_t ob = ib ^ 1u;
             if (!median) {
-                const float cmin = nd.cb[axis], ex = ext[axis], thr = win.thr;
+                const float cmin = sel3(nd.cb, axis), ex = sel3(ext, axis), thr = win.thr;
                 const bool by_thr = use_thr;
                 const uint32_t got = medium_partition(
                     S, ib, s, n, n_lt, lane,
                     [&](uint32_t, const float* c) {
-                        return by_thr ? c[axis] < thr : bin_of(c[axis], cmin, ex, B) < sbin;
+                        const float ca = sel3(c, axis);
+                        return by_thr ? ca < thr : bin_of(ca, cmin, ex, B) < sbin;
                     },
                     ck);
                 if (got != n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
@@ -1539,7 +1545,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                     medium_partition(
                         S, cb, s, n, m, lane,
                         [&](uint32_t p, const float* c) {
-                            const uint32_t key = fkey(c[a]);
+                            const uint32_t key = fkey(sel3(c, a));
                             uint32_t rank = 0;
                             for (uint32_t q = s; q < s + n; ++q) {
                                 const uint32_t r = S.idx[cb][q];
@@ -1558,7 +1564,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                     for (uint32_t p = s + lane; p < s + n; p += 32) {
                         const uint32_t r = S.idx[cb][p];
                         const float4 lo = S.rlo[r], hi = S.rhi[r];
-                        box_grow(p < s + m ? blt : bgt, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z);
+                        box_grow2(blt, bgt, p < s + m, lo.x, lo.y, lo.z, hi.x, hi.y, hi.z);
                     }
                     for (int i = 0; i < 3; ++i) {
                         blt[i] = funkey(__reduce_min_sync(kFull, fkey(blt[i])));
@@ -1592,8 +1598,8 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
             for (uint32_t p = s + lane; p < s + n; p += 32) {
                 const uint32_t r = S.idx[ob][p];
                 const float4 lo = S.rlo[r], hi = S.rhi[r];
-                bad |= !box_contains(p < s + n_lt ? win.lt : win.gt, center_of(lo.x, hi.x),
-                                     center_of(lo.y, hi.y), center_of(lo.z, hi.z));
+                bad |= !box_contains2(win.lt, win.gt, p < s + n_lt, center_of(lo.x, hi.x),
+                                      center_of(lo.y, hi.y), center_of(lo.z, hi.z));
             }
             if (__any_sync(kFull, bad) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
             warp_reduce_keys12(ck);
@@ -1601,6 +1607,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
             any_split = true;
             hmax = max(hmax, depth);
             const uint32_t n_gt = n - n_lt;
+#pragma unroll  // constant c: the child's box and keys stay in registers
             for (int c = 0; c < 2; ++c) {
                 const uint32_t len = c == 0 ? n_gt : n_lt;
                 const uint32_t cs = c == 0 ? s + n_lt : s;

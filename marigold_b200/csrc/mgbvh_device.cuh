@@ -122,6 +122,35 @@ __device__ __forceinline__ bool box_contains(const float* b, float x, float y, f
     return !empty && x >= b[0] && y >= b[1] && z >= b[2] && x <= b[3] && y <= b[4] && z <= b[5];
 }
 
+// v[i] for i < 3 with selects: a run-time index into a local array would
+// put the array in local memory.
+__device__ __forceinline__ float sel3(const float* v, uint32_t i) {
+    return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
+}
+
+// box_contains on box a (first) or box b, chosen with selects on constant
+// indexes (a pointer chosen at run time would put both boxes in local memory).
+__device__ __forceinline__ bool box_contains2(const float* a, const float* b, bool first, float x, float y,
+                                              float z) {
+    float bb[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) bb[i] = first ? a[i] : b[i];
+    return box_contains(bb, x, y, z);
+}
+
+// box_grow on box a (first) or box b, with selects on constant indexes.
+__device__ __forceinline__ void box_grow2(float* a, float* b, bool first, float lx, float ly, float lz,
+                                          float hx, float hy, float hz) {
+    const float l[3] = {lx, ly, lz}, h[3] = {hx, hy, hz};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        a[i] = first ? fminf(a[i], l[i]) : a[i];
+        a[3 + i] = first ? fmaxf(a[3 + i], h[i]) : a[3 + i];
+        b[i] = first ? b[i] : fminf(b[i], l[i]);
+        b[3 + i] = first ? b[3 + i] : fmaxf(b[3 + i], h[i]);
+    }
+}
+
 // Warp union of the boxes of the lanes in `mask` (exact: min/max on keys).
 __device__ __forceinline__ void warp_box_union(bool in, const float* lo, const float* hi,
                                                float* out) {
@@ -198,16 +227,22 @@ struct Cand {
     float thr;  // adaptive threshold (unused for binned)
 };
 
-__device__ __forceinline__ void binned_candidates(const uint32_t* cnt, const float (*box)[6],
-                                                  const bool* axis_ok, uint32_t bins, uint32_t n,
-                                                  float sa_p, const Params& P, uint32_t lane,
-                                                  Cand& best) {
+// load(a, cnt, box6): this lane's bin on axis a.
+template <class Load>
+__device__ __forceinline__ void binned_candidates_f(Load load, const bool* axis_ok, uint32_t bins,
+                                                    uint32_t n, float sa_p, const Params& P,
+                                                    uint32_t lane, Cand& best) {
     best.key = ~0ull;
 #pragma unroll 1
     for (uint32_t a = 0; a < 3; ++a) {
-        if (!axis_ok[a]) continue;  // warp-uniform
+        // selects, not a run-time index: axis_ok stays in registers
+        const bool ok = a == 0 ? axis_ok[0] : (a == 1 ? axis_ok[1] : axis_ok[2]);
+        if (!ok) continue;  // warp-uniform
+        uint32_t ca;
+        float ba[6];
+        load(a, ca, ba);
         BinScan s;
-        bin_scan(cnt[a], box[a], lane, s);
+        bin_scan(ca, ba, lane, s);
         // lt of candidate i = prefix through bin i-1
         uint32_t lt_cnt = __shfl_up_sync(kFull, s.pre_cnt, 1);
         float lt[6];
@@ -232,6 +267,21 @@ __device__ __forceinline__ void binned_candidates(const uint32_t* cnt, const flo
             }
         }
     }
+}
+
+// The bins held in registers per axis (read by selects: run-time indexes
+// into cnt and box would put them in local memory).
+__device__ __forceinline__ void binned_candidates(const uint32_t* cnt, const float (*box)[6],
+                                                  const bool* axis_ok, uint32_t bins, uint32_t n,
+                                                  float sa_p, const Params& P, uint32_t lane,
+                                                  Cand& best) {
+    binned_candidates_f(
+        [&](uint32_t a, uint32_t& ca, float* ba) {
+            ca = a == 0 ? cnt[0] : (a == 1 ? cnt[1] : cnt[2]);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) ba[i] = a == 0 ? box[0][i] : (a == 1 ? box[1][i] : box[2][i]);
+        },
+        axis_ok, bins, n, sa_p, P, lane, best);
 }
 
 // Pull a candidate's payload from lane `src` to all lanes.
@@ -448,7 +498,7 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
                 const uint32_t m = n / 2u;
                 uint32_t best_ck = 0;
                 for (uint32_t a = 0; a < 3; ++a) {
-                    const float ca = center_of(lo[a], hi[a]);
+                    const float ca = center_of(sel3(lo, a), sel3(hi, a));
                     const uint32_t key = fkey(ca);
                     uint32_t rank = 0;
                     for (uint32_t j = s; j < s + n; ++j) {
@@ -505,7 +555,7 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
         const uint32_t ltm = __ballot_sync(kFull, in_seg && pred);
         if (static_cast<uint32_t>(__popc(ltm)) != n_lt) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
         // containment of centroids in child bounds (bvh/src/lib.rs:637-646)
-        const bool ok = !in_seg || box_contains(pred ? win.lt : win.gt, c[0], c[1], c[2]);
+        const bool ok = !in_seg || box_contains2(win.lt, win.gt, pred, c[0], c[1], c[2]);
         if (__ballot_sync(kFull, !ok)) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
         warp_store_node(O, nbase + slot, nb, base + s - tbase, n, pair, lane);
         if (!median) warp_stable_permute(in_seg, pred, s, n_lt, lane, lo, hi, id, xchg);
@@ -747,7 +797,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             const uint32_t half = n / 2u;
             uint32_t best_ck = 0;
             for (uint32_t a = 0; a < 3; ++a) {
-                const uint32_t key = fkey(center_of(lo[a], hi[a]));
+                const uint32_t key = fkey(center_of(sel3(lo, a), sel3(hi, a)));
                 uint32_t rank = 0;
                 for (uint32_t r = 0; r < maxn; ++r) {
                     const bool use = median && r < n;
@@ -806,7 +856,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         const uint32_t ltm = __ballot_sync(kFull, split && pred);
         if (split && lane == s && static_cast<uint32_t>(__popc(ltm & m)) != n_lt)
             set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
-        const bool ok = !split || box_contains(pred ? win.lt : win.gt, c[0], c[1], c[2]);
+        const bool ok = !split || box_contains2(win.lt, win.gt, pred, c[0], c[1], c[2]);
         if (__any_sync(kFull, !ok) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
         if (split && leader) {
             lane_store_node(O, nbase + slot, nb, base + s - tbase, n, pair);
