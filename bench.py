@@ -41,8 +41,8 @@ METRIC = "BVH build Mtri/s"
 UNIT = "Mtri/s"
 SAMPLE_TRIS = 131072
 # dram__bytes_read.sum + dram__bytes_write.sum of one small_kernel launch on
-# this workload, from an ncu capture (cold cache): 47.16 MB + 53.11 MB
-SMALL_KERNEL_TRAFFIC = 100269568
+# this workload, from an ncu capture (cold cache): 47.33 MB + 48.36 MB
+SMALL_KERNEL_TRAFFIC = 95681024
 WORKLOAD = ("noisy icosphere L8 (1,310,720 tris, 655,362 verts), leaf 1, max_depth 32, "
             "reference split profile")
 
