@@ -1697,6 +1697,52 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : MGBVH_MEDIUM_SMAL
     }
 }
 
+// ---------------------------------------------------------------- streamed output
+
+// Counts the subtrees of <= 32 objects per slot chunk (the chunk of their
+// children pair) and writes each subtree's root node. With one object per
+// leaf the root splits, so this is the node the small kernel writes there
+// too; after this pass a chunk launch of the small kernel writes only slots
+// from its subtrees' children pairs on.
+__global__ void __launch_bounds__(256) small_count_kernel(const Task* __restrict__ tasks, Out O,
+                                                          uint32_t slots) {
+    const uint32_t n = O.ctr->n_small;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Task t = tasks[i];
+        atomicAdd(&O.ctr->sbk[stream_chunk(t.nbase + t.pair, slots)], 1u);
+        const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+        lane_store_node(O, t.nbase + t.slot, b, t.start - t.tbase, t.len, t.pair);
+    }
+}
+
+// Sorts the subtrees of <= 32 objects by slot chunk (counted in sbk) into
+// `out`; chunk c's subtrees land in [srange[c], srange[c + 1]). Order within
+// a chunk is free: every subtree writes its own slots.
+__global__ void __launch_bounds__(256) small_sort_kernel(const Task* __restrict__ in, Task* __restrict__ out,
+                                                         Counters* __restrict__ ctr, uint32_t slots) {
+    uint32_t off[kStreamChunks + 1];
+    off[0] = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < kStreamChunks; ++c) off[c + 1] = off[c] + ctr->sbk[c];
+    const uint32_t n = ctr->n_small;
+    if (blockIdx.x == 0 && threadIdx.x <= kStreamChunks) {
+#pragma unroll
+        for (uint32_t c = 0; c <= kStreamChunks; ++c)
+            if (threadIdx.x == c) ctr->srange[c] = min(off[c], n);
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Task t = in[i];
+        const uint32_t c = stream_chunk(t.nbase + t.pair, slots);
+        uint32_t base = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < kStreamChunks; ++q)
+            if (q == c) base = off[q];
+        const uint32_t pos = base + atomicAdd(&ctr->sbcur[c], 1u);
+        if (pos < n) out[pos] = t;  // counts agree by construction; never write past the list
+        else set_error(ctr, MGBVH_ERR_ASSERT, kSiteCount);
+    }
+}
+
 // ---------------------------------------------------------------- small
 
 // One warp per subtree of <= 32 objects. kLevels: the level-synchronous
@@ -1706,13 +1752,16 @@ template <bool kLevels>
 #ifndef MGBVH_SMALL_MIN_BLOCKS
 #define MGBVH_SMALL_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
 #endif
+// range (nullable): build tasks [range[0], range[1]) instead of all of them.
 __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(const Task* __restrict__ tasks,
                                                    const Rec* __restrict__ rec0,
-                                                   const Rec* __restrict__ rec1, Params P, Out O) {
+                                                   const Rec* __restrict__ rec1, Params P, Out O,
+                                                   const uint32_t* range) {
     __shared__ XRec xchg[8][32];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
-    const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
-    for (uint32_t w = blockIdx.x * 8 + wib; w < n_tasks; w += gridDim.x * 8) {
+    const uint32_t w0 = range ? range[0] : 0u;
+    const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
+    for (uint32_t w = w0 + blockIdx.x * 8 + wib; w < n_tasks; w += gridDim.x * 8) {
         const Task t = tasks[w];
         const Rec* src = (t.buf ? rec1 : rec0) + t.start;
         float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
@@ -2115,6 +2164,15 @@ struct mgbvh_ctx {
     uint32_t* learn_count = nullptr;
     Counters* h_ctr = nullptr;
     Counters* h_init = nullptr;  // pinned, constant: the counters every build starts from
+    // streamed output of host-pointer builds: the caller's page-locked node
+    // and lens arrays receive slot chunks on cstream while the build runs
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t evs[kStreamChunks] = {};
+    DevBuf small2;  // subtrees of <= 32 objects sorted by slot chunk
+    mgbvh_node* h_nodes_out = nullptr;
+    uint32_t* h_lens_out = nullptr;
+    bool streamed = false;  // the last build sent its node chunks on cstream
+    uint32_t stream_slots = 0;  // > 0: this build streams (its node slot count)
 };
 
 namespace {
@@ -2327,11 +2385,39 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
         launches++;
         if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
         // small subtrees: count read on the device; grid sized for full occupancy
-        if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
-            small_kernel<true><<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
-        else
-            small_kernel<false><<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O);
-        launches++;
+        auto small = (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax) ? small_kernel<true>
+                                                                              : small_kernel<false>;
+        if (ctx->stream_slots && ctx->h_nodes_out) {
+            // streamed output: subtrees sorted by slot chunk, one launch per
+            // chunk. After launch c no later launch changes chunk c's slots
+            // (their children pairs start in later chunks; their roots, which
+            // may lie anywhere before, hold their final words already), so
+            // the chunk goes to the host on the copy stream while the next
+            // launches run.
+            const uint32_t S = ctx->stream_slots;
+            small_count_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->small), O, S);
+            small_sort_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->small), P_<Task>(ctx->small2),
+                                                                  d_ctr, S);
+            launches += 2;
+            for (uint32_t c = 0; c < kStreamChunks; ++c) {
+                small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small2), rec0, rec1, P, O,
+                                                         d_ctr->srange + c);
+                launches++;
+                MG_CUDA(cudaEventRecord(ctx->evs[c], sm));
+                MG_CUDA(cudaStreamWaitEvent(ctx->cstream, ctx->evs[c], 0));
+                const uint32_t r0 = stream_chunk_begin(c, S), r1 = stream_chunk_begin(c + 1, S);
+                if (r1 <= r0) continue;
+                MG_CUDA(cudaMemcpyAsync(ctx->h_nodes_out + r0, O.nodes + r0, sizeof(mgbvh_node) * (size_t)(r1 - r0),
+                                        cudaMemcpyDeviceToHost, ctx->cstream));
+                if (ctx->h_lens_out)
+                    MG_CUDA(cudaMemcpyAsync(ctx->h_lens_out + r0, O.lens + r0, 4ull * (r1 - r0),
+                                            cudaMemcpyDeviceToHost, ctx->cstream));
+            }
+            ctx->streamed = true;
+        } else {
+            small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
+            launches++;
+        }
         MG_CUDA(cudaGetLastError());
     } else {
         MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
@@ -2413,6 +2499,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     const bool root_leaf = n <= 1 || st->max_depth == 0 ||
                            (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
     const uint32_t cls = root_leaf ? 0u : (n <= kSmallMax ? 1u : (n <= P.medium_max ? 2u : 3u));
+    // streamed output (host-pointer builds into page-locked arrays): with one
+    // object per leaf every subtree of <= 32 objects splits at its root, whose
+    // words are then known before the small kernel runs
+    ctx->stream_slots = 0;
+    if (ctx->h_nodes_out && direct && st->max_leaf_objects == 1 && cls >= 2) {
+        if ((rc = ensure(ctx, ctx->small2, sizeof(Task) * (size_t)C.small)) != MGBVH_OK) return rc;
+        ctx->stream_slots = C.nodes;
+    }
     const uint32_t ntiles0 = (n + kTile - 1) / kTile;
     const float* bb = st->bounds;
     {
@@ -2955,6 +3049,17 @@ int build_common(mgbvh_ctx* ctx, const Input& in_dev, const mgbvh_settings* s, m
 }
 
 // Host-pointer builds: copy inputs in, build into scratch, copy results out.
+// Page-locked host memory (cudaMallocHost, cudaHostAlloc, cudaHostRegister):
+// copies from the device into it run asynchronously.
+bool host_page_locked(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 int build_host(mgbvh_ctx* ctx, Input in, const mgbvh_settings* s, mgbvh_node* out_nodes, uint32_t cap,
                uint32_t* out_count, uint32_t* out_lens, uint32_t* out_perm, mgbvh_stats* stats) {
     int rc = check_ctx(ctx);
@@ -2986,15 +3091,32 @@ int build_host(mgbvh_ctx* ctx, Input in, const mgbvh_settings* s, mgbvh_node* ou
     if ((rc = ensure(ctx, ctx->out_nodes, sizeof(mgbvh_node) * (size_t)full))) return rc;
     if ((rc = ensure(ctx, ctx->out_lens, 4ull * full))) return rc;
     if ((rc = ensure(ctx, ctx->perm, 4ull * in.n))) return rc;
+    // page-locked node (and lens) arrays with room for every slot take the
+    // nodes in chunks while the subtree kernels still run (run_pipeline)
+    const bool stream = cap >= full && host_page_locked(out_nodes) && (!out_lens || host_page_locked(out_lens));
+    if (stream && !ctx->cstream) {
+        MG_CUDA(cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking));
+        for (cudaEvent_t& e : ctx->evs) MG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    ctx->h_nodes_out = stream ? out_nodes : nullptr;
+    ctx->h_lens_out = stream ? out_lens : nullptr;
+    ctx->streamed = false;
     uint32_t count = 0;
     rc = run_build(ctx, d, s, P_<mgbvh_node>(ctx->out_nodes), full, P_<uint32_t>(ctx->out_lens),
                    P_<uint32_t>(ctx->perm), &count, stats);
+    ctx->h_nodes_out = nullptr;
+    ctx->h_lens_out = nullptr;
+    // no chunk copy may still be writing the caller's arrays after this call
+    if (ctx->streamed) MG_CUDA(cudaStreamSynchronize(ctx->cstream));
     if (rc < 0) return rc;
     if (count > cap) return fail(ctx, MGBVH_ERR_CAPACITY, "node_capacity is smaller than the tree");
-    MG_CUDA(cudaMemcpyAsync(out_nodes, ctx->out_nodes.p, sizeof(mgbvh_node) * (size_t)count,
-                            cudaMemcpyDeviceToHost, sm));
-    if (out_lens)
-        MG_CUDA(cudaMemcpyAsync(out_lens, ctx->out_lens.p, 4ull * count, cudaMemcpyDeviceToHost, sm));
+    // the streamed chunks are the result when no slot was compacted away
+    if (!(ctx->streamed && count == full)) {
+        MG_CUDA(cudaMemcpyAsync(out_nodes, ctx->out_nodes.p, sizeof(mgbvh_node) * (size_t)count,
+                                cudaMemcpyDeviceToHost, sm));
+        if (out_lens)
+            MG_CUDA(cudaMemcpyAsync(out_lens, ctx->out_lens.p, 4ull * count, cudaMemcpyDeviceToHost, sm));
+    }
     MG_CUDA(cudaMemcpyAsync(out_perm, ctx->perm.p, 4ull * in.n, cudaMemcpyDeviceToHost, sm));
     MG_CUDA(cudaStreamSynchronize(sm));
     *out_count = count;
@@ -3105,6 +3227,10 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
     if (ctx->h_init) cudaFreeHost(ctx->h_init);
     if (ctx->pin) cudaFreeHost(ctx->pin);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    for (cudaEvent_t e : ctx->evs)
+        if (e) cudaEventDestroy(e);
+    if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
+    if (ctx->small2.p) cudaFree(ctx->small2.p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (cudaEvent_t e : ctx->evp)
@@ -3405,9 +3531,9 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
         if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
-            small_kernel<true><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O);
+            small_kernel<true><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
         else
-            small_kernel<false><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O);
+            small_kernel<false><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
     }
     noalloc_finish_kernel<<<1, 1024, 0, sm>>>(S, slots, d_out_nodes, d_out_lens, node_capacity);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;

@@ -31,6 +31,21 @@ struct Params {
     uint32_t medium_max;      // nodes above this go through the level passes (<= 1024)
 };
 
+// Streamed output: the node slots split into kStreamChunks ranges; a subtree
+// of <= 32 objects whose children pair starts in range c is built by the
+// c-th launch of the small kernel.
+constexpr uint32_t kStreamChunks = 8;
+
+__host__ __device__ __forceinline__ uint32_t stream_chunk(uint32_t pair, uint32_t slots) {
+    const uint32_t c = static_cast<uint32_t>((static_cast<uint64_t>(pair) * kStreamChunks) / slots);
+    return c < kStreamChunks ? c : kStreamChunks - 1u;
+}
+
+// First slot of chunk c (c = kStreamChunks: the slot count).
+__host__ __device__ __forceinline__ uint32_t stream_chunk_begin(uint32_t c, uint32_t slots) {
+    return static_cast<uint32_t>((static_cast<uint64_t>(c) * slots + kStreamChunks - 1u) / kStreamChunks);
+}
+
 // Device counters and flags of one build.
 struct Counters {
     uint32_t error;         // first mgbvh_status error code, 0 if none
@@ -45,6 +60,10 @@ struct Counters {
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
     uint32_t learned;        // nodes where a proposal of the split network replaced the binned split
     uint32_t pad_;
+    uint32_t sbk[8];         // streamed output: subtrees of <= 32 objects per slot chunk
+    uint32_t sbcur[8];       // their placement cursors
+    uint32_t srange[9];      // chunk c's subtrees: [srange[c], srange[c + 1]) of the sorted list
+    uint32_t pad2_;
 };
 
 enum ErrorSite : uint32_t {
