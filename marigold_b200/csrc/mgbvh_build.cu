@@ -1152,10 +1152,14 @@ __device__ __forceinline__ void medium_leaf(const MS& S, uint32_t ib, uint32_t b
 
 // Warp: stable partition of [s, s+n) from idx[ib] into idx[ib^1] by pred(p);
 // returns the lt count; accumulates child centroid keys.
+// With clt non-null, also checks each centroid against its side's child box
+// (clt for lt, cgt for gt) and sets bad where one lies outside.
 template <class MS, class Pred>
 __device__ __forceinline__ uint32_t medium_partition(MS& S, uint32_t ib, uint32_t s,
                                                      uint32_t n, uint32_t n_lt_expect, uint32_t lane,
-                                                     Pred pred, uint32_t* k /*12*/) {
+                                                     Pred pred, uint32_t* k /*12*/,
+                                                     const float* clt = nullptr,
+                                                     const float* cgt = nullptr, bool* bad = nullptr) {
     const uint32_t below = (1u << lane) - 1u;
     uint32_t lt_run = 0, gt_run = 0;
     for (uint32_t b0 = s; b0 < s + n; b0 += 32) {
@@ -1179,6 +1183,7 @@ __device__ __forceinline__ uint32_t medium_partition(MS& S, uint32_t ib, uint32_
                                     : s + n_lt_expect + gt_run + __popc(vm & ~m & below);
             if (dst < s + n) S.idx[ib ^ 1u][dst] = static_cast<uint16_t>(r);
             grow_keys12(k, pr, c);
+            if (clt) *bad |= !box_contains2(clt, cgt, pr, c[0], c[1], c[2]);
         }
         lt_run += __popc(m);
         gt_run += __popc(vm & ~m);
@@ -1522,6 +1527,9 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
             uint32_t ck[12];
             init_key12(ck);
             uint32_t ob = ib ^ 1u;
+            // containment of centroids in child bounds (bvh/src/lib.rs:637-646),
+            // checked on the pass that places each object
+            bool bad = false;
             if (!median) {
                 const float cmin = sel3(nd.cb, axis), ex = sel3(ext, axis), thr = win.thr;
                 const bool by_thr = use_thr;
@@ -1531,7 +1539,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                         const float ca = sel3(c, axis);
                         return by_thr ? ca < thr : bin_of(ca, cmin, ex, B) < sbin;
                     },
-                    ck);
+                    ck, win.lt, win.gt, &bad);
                 if (got != n_lt && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteCount);
             } else {
                 // median_split on axes 0, 1, 2 over the same list (bvh/src/lib.rs:444-491,
@@ -1591,15 +1599,8 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                     const float4 lo = S.rlo[r], hi = S.rhi[r];
                     const float c[3] = {center_of(lo.x, hi.x), center_of(lo.y, hi.y), center_of(lo.z, hi.z)};
                     grow_keys12(ck, p < s + m, c);
+                    bad |= !box_contains2(win.lt, win.gt, p < s + m, c[0], c[1], c[2]);
                 }
-            }
-            // containment of centroids in child bounds (bvh/src/lib.rs:637-646)
-            bool bad = false;
-            for (uint32_t p = s + lane; p < s + n; p += 32) {
-                const uint32_t r = S.idx[ob][p];
-                const float4 lo = S.rlo[r], hi = S.rhi[r];
-                bad |= !box_contains2(win.lt, win.gt, p < s + n_lt, center_of(lo.x, hi.x),
-                                      center_of(lo.y, hi.y), center_of(lo.z, hi.z));
             }
             if (__any_sync(kFull, bad) && lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
             warp_reduce_keys12(ck);
