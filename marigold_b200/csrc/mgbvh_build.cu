@@ -1688,11 +1688,13 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : MGBVH_MEDIUM_SMAL
     medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
-                                                                Learn LN) {
+                                                                Learn LN, const uint32_t* range) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
-    const uint32_t n_tasks = *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
-    for (uint32_t ti = blockIdx.x; ti < n_tasks; ti += gridDim.x) {
+    // range (nullable): tasks [range[0], range[1]) instead of all of them
+    const uint32_t t0 = range ? range[0] : 0u;
+    const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
+    for (uint32_t ti = t0 + blockIdx.x; ti < n_tasks; ti += gridDim.x) {
         __syncthreads();
         medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
     }
@@ -1700,47 +1702,91 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : MGBVH_MEDIUM_SMAL
 
 // ---------------------------------------------------------------- streamed output
 
-// Counts the subtrees of <= 32 objects per slot chunk (the chunk of their
-// children pair) and writes each subtree's root node. With one object per
-// leaf the root splits, so this is the node the small kernel writes there
-// too; after this pass a chunk launch of the small kernel writes only slots
-// from its subtrees' children pairs on.
-__global__ void __launch_bounds__(256) small_count_kernel(const Task* __restrict__ tasks, Out O,
-                                                          uint32_t slots) {
-    const uint32_t n = O.ctr->n_small;
+// The slot chunk of a subtree: the chunk of its children pair.
+__device__ __forceinline__ uint32_t task_chunk(const Task& t, uint32_t slots) {
+    return stream_chunk(t.nbase + t.pair, slots);
+}
+
+// A subtree's root node as its builder writes it when the root splits (one
+// object per leaf: every queued subtree splits at its root).
+__device__ __forceinline__ void write_task_root(const Out& O, const Task& t) {
+    const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    lane_store_node(O, t.nbase + t.slot, b, t.start - t.tbase, t.len, t.pair);
+}
+
+// Subtree CTA tasks: counts per slot chunk and writes each root node, so
+// that a chunk's launch writes only slots from its subtrees' children pairs
+// on.
+__global__ void __launch_bounds__(256) medium_count_kernel(const Task* __restrict__ tasks, Out O,
+                                                           uint32_t slots) {
+    const uint32_t n = O.ctr->n_medium;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Task t = tasks[i];
-        atomicAdd(&O.ctr->sbk[stream_chunk(t.nbase + t.pair, slots)], 1u);
-        const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-        lane_store_node(O, t.nbase + t.slot, b, t.start - t.tbase, t.len, t.pair);
+        atomicAdd(&O.ctr->mbk[task_chunk(t, slots)], 1u);
+        write_task_root(O, t);
     }
 }
 
-// Sorts the subtrees of <= 32 objects by slot chunk (counted in sbk) into
-// `out`; chunk c's subtrees land in [srange[c], srange[c + 1]). Order within
-// a chunk is free: every subtree writes its own slots.
-__global__ void __launch_bounds__(256) small_sort_kernel(const Task* __restrict__ in, Task* __restrict__ out,
-                                                         Counters* __restrict__ ctr, uint32_t slots) {
+// Sorts the subtree CTA tasks by slot chunk into `out`; chunk c's tasks land
+// in [mrange[c], mrange[c + 1]). Order within a chunk is free: every subtree
+// writes its own slots.
+__global__ void __launch_bounds__(256) medium_sort_kernel(const Task* __restrict__ in, Task* __restrict__ out,
+                                                          Counters* __restrict__ ctr, uint32_t slots) {
     uint32_t off[kStreamChunks + 1];
     off[0] = 0;
 #pragma unroll
-    for (uint32_t c = 0; c < kStreamChunks; ++c) off[c + 1] = off[c] + ctr->sbk[c];
-    const uint32_t n = ctr->n_small;
+    for (uint32_t c = 0; c < kStreamChunks; ++c) off[c + 1] = off[c] + ctr->mbk[c];
+    const uint32_t n = ctr->n_medium;
     if (blockIdx.x == 0 && threadIdx.x <= kStreamChunks) {
 #pragma unroll
         for (uint32_t c = 0; c <= kStreamChunks; ++c)
-            if (threadIdx.x == c) ctr->srange[c] = min(off[c], n);
+            if (threadIdx.x == c) ctr->mrange[c] = min(off[c], n);
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Task t = in[i];
-        const uint32_t c = stream_chunk(t.nbase + t.pair, slots);
+        const uint32_t c = task_chunk(t, slots);
         uint32_t base = 0;
 #pragma unroll
         for (uint32_t q = 0; q < kStreamChunks; ++q)
             if (q == c) base = off[q];
-        const uint32_t pos = base + atomicAdd(&ctr->sbcur[c], 1u);
-        if (pos < n) out[pos] = t;  // counts agree by construction; never write past the list
-        else set_error(ctr, MGBVH_ERR_ASSERT, kSiteCount);
+        const uint32_t pos = base + atomicAdd(&ctr->mbcur[c], 1u);
+        if (pos < n)
+            out[pos] = t;
+        else
+            set_error(ctr, MGBVH_ERR_ASSERT, kSiteCount);  // counts agree by construction
+    }
+}
+
+// Appends the subtrees of <= 32 objects of slot chunk c (all queued once
+// chunk c's subtree CTAs ran) to `out`, and writes the root node of every
+// subtree whose root slot lies in chunk c (all queued by then too: a root
+// slot lies in the block of the subtree CTA or level pass that queued it).
+// A root can lie in an earlier chunk than its children pair, so roots are
+// written by the chunk that holds them, before that chunk is copied. The
+// CTA that finishes last records the end of the chunk's range, srange[c + 1]
+// (srange[c] is the previous chunk's end).
+__global__ void __launch_bounds__(256) small_select_kernel(const Task* __restrict__ in, Task* __restrict__ out,
+                                                           uint32_t cap, Out O, uint32_t c, uint32_t slots) {
+    __shared__ uint32_t last;
+    Counters* ctr = O.ctr;
+    const uint32_t n = ctr->n_small;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const Task t = in[i];
+        if (stream_chunk(t.nbase + t.slot, slots) == c) write_task_root(O, t);
+        if (task_chunk(t, slots) != c) continue;
+        const uint32_t pos = atomicAdd(&ctr->s2n, 1u);
+        if (pos < cap)
+            out[pos] = t;
+        else
+            set_error(ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&ctr->sdone[c], 1u) == gridDim.x - 1u ? 1u : 0u;
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        ctr->srange[c + 1] = min(*reinterpret_cast<volatile uint32_t*>(&ctr->s2n), cap);
     }
 }
 
@@ -2169,7 +2215,7 @@ struct mgbvh_ctx {
     // and lens arrays receive slot chunks on cstream while the build runs
     cudaStream_t cstream = nullptr;
     cudaEvent_t evs[kStreamChunks] = {};
-    DevBuf small2;  // subtrees of <= 32 objects sorted by slot chunk
+    DevBuf small2, medium2;  // subtrees of <= 32 objects and subtree CTA tasks sorted by slot chunk
     mgbvh_node* h_nodes_out = nullptr;
     uint32_t* h_lens_out = nullptr;
     bool streamed = false;  // the last build sent its node chunks on cstream
@@ -2371,39 +2417,45 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
         const bool lrn = LN.w || LN.samples, small_cap = P.medium_max <= kMediumSmallCap;
         const uint32_t mgrid_s =
             std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * (uint32_t)MGBVH_MEDIUM_SMALL_CTAS);
-        if (lrn && small_cap)
-            medium_kernel<true, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
-                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
-        else if (lrn)
-            medium_kernel<true, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
-                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
-        else if (small_cap)
-            medium_kernel<false, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
-                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
-        else
-            medium_kernel<false, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
-                P_<Task>(ctx->medium), rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN);
-        launches++;
-        if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
+        auto medium = [&](const Task* tasks, const uint32_t* range) {
+            if (lrn && small_cap)
+                medium_kernel<true, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
+                    tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
+            else if (lrn)
+                medium_kernel<true, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                    tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
+            else if (small_cap)
+                medium_kernel<false, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
+                    tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
+            else
+                medium_kernel<false, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                    tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
+        };
         // small subtrees: count read on the device; grid sized for full occupancy
         auto small = (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax) ? small_kernel<true>
                                                                               : small_kernel<false>;
         if (ctx->stream_slots && ctx->h_nodes_out) {
-            // streamed output: subtrees sorted by slot chunk, one launch per
-            // chunk. After launch c no later launch changes chunk c's slots
-            // (their children pairs start in later chunks; their roots, which
-            // may lie anywhere before, hold their final words already), so
-            // the chunk goes to the host on the copy stream while the next
-            // launches run.
+            // streamed output: the subtrees of both kinds run chunk by chunk
+            // of node slots (the chunk of their children pair): chunk c's
+            // subtree CTAs, then the subtrees of <= 32 objects of chunk c
+            // (all queued by then: a subtree's children pairs come after its
+            // own). After them no later launch changes chunk c's slots (the
+            // roots of later subtrees, which may lie anywhere before, hold
+            // their final words already), so the chunk goes to the host on
+            // the copy stream while the next chunks run.
             const uint32_t S = ctx->stream_slots;
-            small_count_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->small), O, S);
-            small_sort_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->small), P_<Task>(ctx->small2),
-                                                                  d_ctr, S);
+            if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
+            medium_count_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->medium), O, S);
+            medium_sort_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->medium), P_<Task>(ctx->medium2),
+                                                                   d_ctr, S);
             launches += 2;
             for (uint32_t c = 0; c < kStreamChunks; ++c) {
+                medium(P_<Task>(ctx->medium2), d_ctr->mrange + c);
+                small_select_kernel<<<ctx->sm_count, 256, 0, sm>>>(P_<Task>(ctx->small), P_<Task>(ctx->small2),
+                                                                   C.small, O, c, S);
                 small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small2), rec0, rec1, P, O,
                                                          d_ctr->srange + c);
-                launches++;
+                launches += 3;
                 MG_CUDA(cudaEventRecord(ctx->evs[c], sm));
                 MG_CUDA(cudaStreamWaitEvent(ctx->cstream, ctx->evs[c], 0));
                 const uint32_t r0 = stream_chunk_begin(c, S), r1 = stream_chunk_begin(c + 1, S);
@@ -2416,6 +2468,9 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             }
             ctx->streamed = true;
         } else {
+            medium(P_<Task>(ctx->medium), nullptr);
+            launches++;
+            if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
             small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
             launches++;
         }
@@ -2506,6 +2561,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     ctx->stream_slots = 0;
     if (ctx->h_nodes_out && direct && st->max_leaf_objects == 1 && cls >= 2) {
         if ((rc = ensure(ctx, ctx->small2, sizeof(Task) * (size_t)C.small)) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->medium2, sizeof(Task) * (size_t)C.medium)) != MGBVH_OK) return rc;
         ctx->stream_slots = C.nodes;
     }
     const uint32_t ntiles0 = (n + kTile - 1) / kTile;
@@ -3232,6 +3288,7 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
         if (e) cudaEventDestroy(e);
     if (ctx->cstream) cudaStreamDestroy(ctx->cstream);
     if (ctx->small2.p) cudaFree(ctx->small2.p);
+    if (ctx->medium2.p) cudaFree(ctx->medium2.p);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (cudaEvent_t e : ctx->evp)
@@ -3528,7 +3585,8 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
                                                       st->max_depth);
     if (cls == 2)
         medium_kernel<false, kMediumMax><<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
-            S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr});
+            S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr},
+            nullptr);
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
         if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)

@@ -60,10 +60,16 @@ struct Counters {
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
     uint32_t learned;        // nodes where a proposal of the split network replaced the binned split
     uint32_t pad_;
-    uint32_t sbk[8];         // streamed output: subtrees of <= 32 objects per slot chunk
-    uint32_t sbcur[8];       // their placement cursors
-    uint32_t srange[9];      // chunk c's subtrees: [srange[c], srange[c + 1]) of the sorted list
-    uint32_t pad2_;
+    // streamed output (slot chunks): subtrees of 33..medium_max objects per
+    // chunk, their placement cursors and sorted ranges; subtrees of <= 32
+    // objects selected so far, the sorted range of each chunk's, and the CTAs
+    // of each chunk's selection pass that finished
+    uint32_t mbk[8];
+    uint32_t mbcur[8];
+    uint32_t mrange[9];
+    uint32_t s2n;
+    uint32_t srange[9];
+    uint32_t sdone[8];
 };
 
 enum ErrorSite : uint32_t {
