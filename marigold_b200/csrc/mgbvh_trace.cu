@@ -19,7 +19,14 @@
 //
 // The library is compiled with -fmad=false: every dot and cross product is
 // evaluated as written below, the same way as the CPU cross-check.
+//
+// Rays are traced in a sorted order (ray_key_kernel + a radix sort, inside
+// the timed call): rays that start in nearby cells of the root box and head
+// in similar directions share warps, so their lanes walk similar paths
+// through the tree and reuse the same nodes in cache. Each ray's result is
+// written at its own index; the order changes no hit.
 
+#include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -97,10 +104,11 @@ __global__ void __launch_bounds__(128) trace_kernel(const float4* __restrict__ n
                                                     const float4* __restrict__ rays, uint32_t n_rays,
                                                     float* __restrict__ hit_t,
                                                     uint32_t* __restrict__ hit_prim, Counts* counts,
-                                                    int* err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                    int* err, const uint32_t* __restrict__ order) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
-    if (i < n_rays) {
+    if (j < n_rays) {
+        const uint32_t i = order ? order[j] : j;  // the ray this thread traces
         const float4 o = rays[2 * i], d = rays[2 * i + 1];
         const float ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
         float best = __int_as_float(0x7F800000);
@@ -418,10 +426,11 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
                                                          const float4* __restrict__ rays, uint32_t n_rays,
                                                          float* __restrict__ hit_t,
                                                          uint32_t* __restrict__ hit_prim, Counts* counts,
-                                                         int* err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+                                                         int* err, const uint32_t* __restrict__ order) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
-    if (i < n_rays) {
+    if (j < n_rays) {
+        const uint32_t i = order ? order[j] : j;  // the ray this thread traces
         const float4 o = rays[2 * i], d = rays[2 * i + 1];
         const float ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
         float best = __int_as_float(0x7F800000);
@@ -545,6 +554,50 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
     }
 }
 
+// Ray order per traversal (tuning knobs): 0 as given, 1 direction bin then
+// origin, 2 origin then direction bin. Measured on 8.4M random rays in a
+// 16.8M-triangle scene: binary 34.2 / 44.6 / 49.3 Mrays/s, 8-wide 28.9 /
+// 39.3 / 37.2 Mrays/s for 0 / 1 / 2.
+#ifndef MGBVH_RAY_SORT_BINARY
+#define MGBVH_RAY_SORT_BINARY 2
+#endif
+#ifndef MGBVH_RAY_SORT_WIDE
+#define MGBVH_RAY_SORT_WIDE 1
+#endif
+
+// Sort key of a ray for the tracing order: the direction quantized to 4 bins
+// per component (6 bits) and the origin quantized to 256 cells per axis of
+// the root box, Morton-interleaved (24 bits); `mode` 1 puts the direction
+// bits first, 2 the origin bits. Rays that start near one another in similar
+// directions then share warps. The order changes no hit.
+__device__ __forceinline__ uint32_t spread8(uint32_t v) {  // 8 bits -> every third of 24
+    v &= 0xFFu;
+    v = (v | (v << 8)) & 0x00F00Fu;
+    v = (v | (v << 4)) & 0x0C30C3u;
+    v = (v | (v << 2)) & 0x249249u;
+    return v;
+}
+
+__global__ void ray_key_kernel(const float4* __restrict__ rays, uint32_t n, const float4* __restrict__ root,
+                               uint32_t mode, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    const float4 lo = root[0], hi = root[1];
+    const float sx = 256.0f / fmaxf(hi.x - lo.x, 1e-30f), sy = 256.0f / fmaxf(hi.y - lo.y, 1e-30f),
+                sz = 256.0f / fmaxf(hi.z - lo.z, 1e-30f);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = rays[2 * i], d = rays[2 * i + 1];
+        const uint32_t qx = (uint32_t)fminf(fmaxf((o.x - lo.x) * sx, 0.0f), 255.0f);
+        const uint32_t qy = (uint32_t)fminf(fmaxf((o.y - lo.y) * sy, 0.0f), 255.0f);
+        const uint32_t qz = (uint32_t)fminf(fmaxf((o.z - lo.z) * sz, 0.0f), 255.0f);
+        const uint32_t morton = spread8(qx) | (spread8(qy) << 1) | (spread8(qz) << 2);
+        const uint32_t dx = (uint32_t)fminf(fmaxf((d.x + 1.0f) * 2.0f, 0.0f), 3.0f);
+        const uint32_t dy = (uint32_t)fminf(fmaxf((d.y + 1.0f) * 2.0f, 0.0f), 3.0f);
+        const uint32_t dz = (uint32_t)fminf(fmaxf((d.z + 1.0f) * 2.0f, 0.0f), 3.0f);
+        const uint32_t dir = dx | (dy << 2) | (dz << 4);
+        keys[i] = mode == 1 ? (dir << 24) | morton : (morton << 6) | dir;
+        idx[i] = i;
+    }
+}
+
 }  // namespace mgbvh_trace
 
 using namespace mgbvh_trace;
@@ -568,11 +621,58 @@ struct mgbvh_tracer {
     uint32_t* wmeta = nullptr;  // [0..1], [2..3]: level ranges; [4]: slots taken
     size_t wide_cap = 0;
     uint32_t wide_count = 0;
+    // tracing order: ray keys and indices (two of each for the radix sort)
+    uint32_t* rkey[2] = {nullptr, nullptr};
+    uint32_t* ridx[2] = {nullptr, nullptr};
+    size_t ray_cap = 0;
+    void* sort_tmp = nullptr;
+    size_t sort_tmp_bytes = 0;
 };
 
 namespace {
 
 int trace_check(cudaError_t e) { return e == cudaSuccess ? MGBVH_OK : MGBVH_ERR_CUDA; }
+
+// Buffers of the tracing order for n rays (grown before the timed region).
+int ensure_order_buffers(mgbvh_tracer* t, uint32_t n) {
+    if (t->ray_cap < n) {
+        for (int k = 0; k < 2; ++k) {
+            if (t->rkey[k]) cudaFree(t->rkey[k]);
+            if (t->ridx[k]) cudaFree(t->ridx[k]);
+            t->rkey[k] = t->ridx[k] = nullptr;
+        }
+        t->ray_cap = 0;
+        for (int k = 0; k < 2; ++k)
+            if (cudaMalloc(&t->rkey[k], 4ull * n) != cudaSuccess || cudaMalloc(&t->ridx[k], 4ull * n) != cudaSuccess)
+                return MGBVH_ERR_CUDA;
+        t->ray_cap = n;
+    }
+    size_t need = 0;
+    cub::DoubleBuffer<uint32_t> kb(t->rkey[0], t->rkey[1]), vb(t->ridx[0], t->ridx[1]);
+    if (cub::DeviceRadixSort::SortPairs(nullptr, need, kb, vb, (int)n, 0, 30) != cudaSuccess) return MGBVH_ERR_CUDA;
+    if (t->sort_tmp_bytes < need) {
+        if (t->sort_tmp) cudaFree(t->sort_tmp);
+        t->sort_tmp = nullptr;
+        t->sort_tmp_bytes = 0;
+        if (cudaMalloc(&t->sort_tmp, need) != cudaSuccess) return MGBVH_ERR_CUDA;
+        t->sort_tmp_bytes = need;
+    }
+    return MGBVH_OK;
+}
+
+// Enqueues the tracing order of the rays on stream sm: keys (ray_key_kernel
+// mode), then a radix sort of (key, ray index); returns the sorted ray
+// indices, or nullptr (rays traced as given).
+const uint32_t* ray_order(mgbvh_tracer* t, const float4* rays, uint32_t n, cudaStream_t sm, uint32_t mode) {
+    if (mode == 0) return nullptr;
+    ray_key_kernel<<<1184, 256, 0, sm>>>(rays, n, reinterpret_cast<const float4*>(t->nodes), mode,
+                                         t->rkey[0], t->ridx[0]);
+    cub::DoubleBuffer<uint32_t> kb(t->rkey[0], t->rkey[1]), vb(t->ridx[0], t->ridx[1]);
+    size_t bytes = t->sort_tmp_bytes;
+    if (cub::DeviceRadixSort::SortPairs(t->sort_tmp, bytes, kb, vb, (int)n, 0, 30, sm) != cudaSuccess)
+        return nullptr;
+    return vb.Current();
+}
 
 }  // namespace
 
@@ -609,6 +709,11 @@ void mgbvh_tracer_destroy(mgbvh_tracer* t) {
     if (t->wmeta) cudaFree(t->wmeta);
     if (t->d_counts) cudaFree(t->d_counts);
     if (t->d_err) cudaFree(t->d_err);
+    for (int k = 0; k < 2; ++k) {
+        if (t->rkey[k]) cudaFree(t->rkey[k]);
+        if (t->ridx[k]) cudaFree(t->ridx[k]);
+    }
+    if (t->sort_tmp) cudaFree(t->sort_tmp);
     if (t->ev0) cudaEventDestroy(t->ev0);
     if (t->ev1) cudaEventDestroy(t->ev1);
     delete t;
@@ -720,11 +825,12 @@ int mgbvh_trace_closest_wide_dev(mgbvh_tracer* t, const float* d_rays, uint32_t 
     if (cudaMemsetAsync(t->d_counts, 0, sizeof(Counts), sm) != cudaSuccess ||
         cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
         return MGBVH_ERR_CUDA;
+    if (int rc = ensure_order_buffers(t, n_rays)) return rc;
     cudaEventRecord(t->ev0, sm);
-    trace_wide_kernel<<<(n_rays + 127) / 128, 128, 0, sm>>>(t->wide, t->tris,
-                                                             reinterpret_cast<const float4*>(d_rays), n_rays,
-                                                             d_hit_t, d_hit_prim,
-                                                             out_counts ? t->d_counts : nullptr, t->d_err);
+    const float4* rays = reinterpret_cast<const float4*>(d_rays);
+    const uint32_t* order = ray_order(t, rays, n_rays, sm, MGBVH_RAY_SORT_WIDE);
+    trace_wide_kernel<<<(n_rays + 127) / 128, 128, 0, sm>>>(t->wide, t->tris, rays, n_rays, d_hit_t, d_hit_prim,
+                                                             out_counts ? t->d_counts : nullptr, t->d_err, order);
     cudaEventRecord(t->ev1, sm);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
     Counts hc;
@@ -757,18 +863,20 @@ int mgbvh_trace_closest_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_ray
     if (cudaMemsetAsync(t->d_counts, 0, sizeof(Counts), sm) != cudaSuccess ||
         cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
         return MGBVH_ERR_CUDA;
+    if (int rc = ensure_order_buffers(t, n_rays)) return rc;
     cudaEventRecord(t->ev0, sm);
     const uint32_t grid = (n_rays + 127) / 128;
     const float4* nodes = reinterpret_cast<const float4*>(t->nodes);
     const float4* rays = reinterpret_cast<const float4*>(d_rays);
+    const uint32_t* order = ray_order(t, rays, n_rays, sm, MGBVH_RAY_SORT_BINARY);
     if (t->lens)
         trace_kernel<true><<<grid, 128, 0, sm>>>(nodes, t->lens, t->tris, rays, n_rays, d_hit_t,
                                                  d_hit_prim, out_counts ? t->d_counts : nullptr,
-                                                 t->d_err);
+                                                 t->d_err, order);
     else
         trace_kernel<false><<<grid, 128, 0, sm>>>(nodes, nullptr, t->tris, rays, n_rays, d_hit_t,
                                                   d_hit_prim, out_counts ? t->d_counts : nullptr,
-                                                  t->d_err);
+                                                  t->d_err, order);
     cudaEventRecord(t->ev1, sm);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
     Counts hc;
