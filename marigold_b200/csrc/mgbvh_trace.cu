@@ -555,9 +555,10 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
 }
 
 // Ray order per traversal (tuning knobs): 0 as given, 1 direction bin then
-// origin, 2 origin then direction bin. Measured on 8.4M random rays in a
+// origin, 2 origin cell then direction bin. Measured on 8.4M random rays in a
 // 16.8M-triangle scene: binary 34.2 / 44.6 / 49.3 Mrays/s, 8-wide 28.9 /
-// 39.3 / 37.2 Mrays/s for 0 / 1 / 2.
+// 39.3 / 37.2 Mrays/s for 0 / 1 / 2 (form 2 at 256 cells per axis and 4
+// bins per component); form 2 with 16 cells and 8 bins: binary 54.5.
 #ifndef MGBVH_RAY_SORT_BINARY
 #define MGBVH_RAY_SORT_BINARY 2
 #endif
@@ -565,11 +566,12 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
 #define MGBVH_RAY_SORT_WIDE 1
 #endif
 
-// Sort key of a ray for the tracing order: the direction quantized to 4 bins
-// per component (6 bits) and the origin quantized to 256 cells per axis of
-// the root box, Morton-interleaved (24 bits); `mode` 1 puts the direction
-// bits first, 2 the origin bits. Rays that start near one another in similar
-// directions then share warps. The order changes no hit.
+// Sort key of a ray for the tracing order. Mode 1: the direction quantized
+// to 4 bins per component (6 bits) above the origin quantized to 256 cells
+// per axis of the root box, Morton-interleaved (24 bits). Mode 2: the origin
+// cell at 2^MGBVH_RAY_ORIGIN_BITS per axis (Morton) above the direction at
+// 2^MGBVH_RAY_DIR_BITS bins per component. Rays that start near one another
+// in similar directions then share warps. The order changes no hit.
 __device__ __forceinline__ uint32_t spread8(uint32_t v) {  // 8 bits -> every third of 24
     v &= 0xFFu;
     v = (v | (v << 8)) & 0x00F00Fu;
@@ -577,6 +579,15 @@ __device__ __forceinline__ uint32_t spread8(uint32_t v) {  // 8 bits -> every th
     v = (v | (v << 2)) & 0x249249u;
     return v;
 }
+
+#ifndef MGBVH_RAY_ORIGIN_BITS
+#define MGBVH_RAY_ORIGIN_BITS 4  // origin-first key: origin cells per axis = 2^bits (tuning knob)
+#endif
+#ifndef MGBVH_RAY_DIR_BITS
+#define MGBVH_RAY_DIR_BITS 3  // origin-first key: direction bins per component = 2^bits (tuning knob)
+#endif
+constexpr uint32_t kRayKeyBits2 = 3u * (MGBVH_RAY_ORIGIN_BITS + MGBVH_RAY_DIR_BITS);
+static_assert(kRayKeyBits2 <= 30u, "ray key wider than 30 bits");
 
 __global__ void ray_key_kernel(const float4* __restrict__ rays, uint32_t n, const float4* __restrict__ root,
                                uint32_t mode, uint32_t* __restrict__ keys, uint32_t* __restrict__ idx) {
@@ -593,7 +604,19 @@ __global__ void ray_key_kernel(const float4* __restrict__ rays, uint32_t n, cons
         const uint32_t dy = (uint32_t)fminf(fmaxf((d.y + 1.0f) * 2.0f, 0.0f), 3.0f);
         const uint32_t dz = (uint32_t)fminf(fmaxf((d.z + 1.0f) * 2.0f, 0.0f), 3.0f);
         const uint32_t dir = dx | (dy << 2) | (dz << 4);
-        keys[i] = mode == 1 ? (dir << 24) | morton : (morton << 6) | dir;
+        if (mode == 1) {
+            keys[i] = (dir << 24) | morton;
+        } else {
+            // origin first at MGBVH_RAY_ORIGIN_BITS per axis, then the direction
+            // at MGBVH_RAY_DIR_BITS per component
+            constexpr uint32_t ob = MGBVH_RAY_ORIGIN_BITS, db = MGBVH_RAY_DIR_BITS;
+            const uint32_t m2 = morton >> (3u * (8u - ob));
+            const float nd = (float)(1u << db);
+            const uint32_t ex = (uint32_t)fminf(fmaxf((d.x + 1.0f) * 0.5f * nd, 0.0f), nd - 1.0f);
+            const uint32_t ey = (uint32_t)fminf(fmaxf((d.y + 1.0f) * 0.5f * nd, 0.0f), nd - 1.0f);
+            const uint32_t ez = (uint32_t)fminf(fmaxf((d.z + 1.0f) * 0.5f * nd, 0.0f), nd - 1.0f);
+            keys[i] = (m2 << (3u * db)) | ex | (ey << db) | (ez << (2u * db));
+        }
         idx[i] = i;
     }
 }
