@@ -1683,8 +1683,12 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
 
 // kLearn: with the learned form's hook (network proposals, training samples);
 // plain builds run the instantiation without it.
+#ifndef MGBVH_MEDIUM_LEARN_CTAS
+#define MGBVH_MEDIUM_LEARN_CTAS 4  // learned-form subtree CTAs per SM the register budget must allow (tuning knob)
+#endif
+
 template <bool kLearn, uint32_t kCap>
-__global__ void __launch_bounds__(kMediumThreads, kLearn ? 4 : MGBVH_MEDIUM_SMALL_CTAS)
+__global__ void __launch_bounds__(kMediumThreads, kLearn ? MGBVH_MEDIUM_LEARN_CTAS : MGBVH_MEDIUM_SMALL_CTAS)
     medium_kernel(const Task* __restrict__ tasks,
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,

@@ -558,12 +558,13 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
 // origin, 2 origin cell then direction bin. Measured on 8.4M random rays in a
 // 16.8M-triangle scene: binary 34.2 / 44.6 / 49.3 Mrays/s, 8-wide 28.9 /
 // 39.3 / 37.2 Mrays/s for 0 / 1 / 2 (form 2 at 256 cells per axis and 4
-// bins per component); form 2 with 16 cells and 8 bins: binary 54.5.
+// bins per component); form 2 with 16 cells and 8 bins: binary 54.5,
+// 8-wide 41.9.
 #ifndef MGBVH_RAY_SORT_BINARY
 #define MGBVH_RAY_SORT_BINARY 2
 #endif
 #ifndef MGBVH_RAY_SORT_WIDE
-#define MGBVH_RAY_SORT_WIDE 1
+#define MGBVH_RAY_SORT_WIDE 2
 #endif
 
 // Sort key of a ray for the tracing order. Mode 1: the direction quantized
