@@ -160,6 +160,12 @@ MGBVH_API const char* mgbvh_status_string(int status);
  *   the crate's in-place permutation.
  * out_stats: may be NULL.
  * All pointers are host pointers. Returns mgbvh_status.
+ * When out_nodes (and out_lens, if given) are page-locked host memory
+ * (cudaMallocHost, cudaHostAlloc, cudaHostRegister), node_capacity >=
+ * 2 * triangle_count - 1 and leaves hold one object, finished chunks of the
+ * node array are copied to the caller while the build's last kernels still
+ * run; the result is the same as with pageable arrays, which are filled after
+ * the build.
  */
 MGBVH_API int mgbvh_build_indexed(mgbvh_ctx* ctx, const float* vertices, uint32_t vertex_stride_bytes,
                         uint32_t vertex_count, const uint32_t* triangles, uint32_t triangle_count,
@@ -310,8 +316,13 @@ MGBVH_API int mgbvh_tracer_set_blas_dev(mgbvh_tracer* tracer, const mgbvh_node* 
                                         uint32_t vertex_count, const uint32_t* d_triangles,
                                         const uint32_t* d_perm, uint32_t triangle_count,
                                         void* cuda_stream);
-/* Closest hit of every ray through the BVH. out_seconds (host, nullable):
-   device time of the traversal kernel. */
+/* Closest hit of every ray through the BVH. The call first sorts the rays
+   (by origin cell of the root box, then direction bin) and traces them in
+   that order, so that rays that start near one another in similar directions
+   share warps; every ray's hit is still written at its own index, and the
+   order changes no result. The sort buffers (about 16 bytes per ray) are
+   kept by the tracer and grown on a call with more rays than before.
+   out_seconds (host, nullable): device time of the sort and the traversal. */
 MGBVH_API int mgbvh_trace_closest_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
                                       float* d_hit_t, uint32_t* d_hit_prim, uint64_t* out_counts,
                                       double* out_seconds, void* cuda_stream);
@@ -328,7 +339,8 @@ MGBVH_API int mgbvh_tracer_build_wide(mgbvh_tracer* tracer, void* cuda_stream, u
 /* The wide nodes of the last mgbvh_tracer_build_wide (device pointer, owned by the tracer). */
 MGBVH_API int mgbvh_tracer_wide_nodes(mgbvh_tracer* tracer, const void** out_d_wide_nodes,
                                       uint32_t* out_wide_count);
-/* Closest hit of every ray through the wide BVH: same results as
+/* Closest hit of every ray through the wide BVH, rays in the same sorted
+   order as mgbvh_trace_closest_dev: same results as
    mgbvh_trace_closest_dev (same triangle test and tie rule; conservative
    boxes). out_counts: wide nodes visited, child boxes tested, triangle tests. */
 MGBVH_API int mgbvh_trace_closest_wide_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
