@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(128) trace_kernel(const float4* __restrict__ n
 }
 
 #ifndef MGBVH_TRACE_PERSISTENT
-#define MGBVH_TRACE_PERSISTENT 1  // binary traversal by persistent warps that refill idle lanes (tuning knob)
+#define MGBVH_TRACE_PERSISTENT 1  // traversals by persistent warps that refill idle lanes (tuning knob)
 #endif
 #ifndef MGBVH_TRACE_REFILL
 #define MGBVH_TRACE_REFILL 16  // a warp fetches new rays once this many of its lanes are idle (tuning knob;
@@ -677,6 +677,167 @@ __global__ void __launch_bounds__(128) trace_wide_kernel(const WNode* __restrict
     }
 }
 
+
+// trace_wide_kernel with persistent warps that refill idle lanes
+// (trace_persistent_kernel's scheme): the same node steps, tests and results.
+__global__ void __launch_bounds__(128) trace_wide_persistent_kernel(
+    const WNode* __restrict__ wn, const TriRec* __restrict__ tris, const float4* __restrict__ rays,
+    uint32_t n_rays, float* __restrict__ hit_t, uint32_t* __restrict__ hit_prim, Counts* counts, int* err,
+    const uint32_t* __restrict__ order, uint32_t* __restrict__ next) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
+    bool has = false, exhausted = false;
+    uint32_t ri = 0, best_prim = kNoHit;
+    float ox = 0.f, oy = 0.f, oz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f, ix = 0.f, iy = 0.f, iz = 0.f;
+    float best = 0.f;
+    uint32_t st_node[kWideStack];
+    float st_t[kWideStack];
+    int sp = 0;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(kFull, !has);
+        if (!exhausted && idle != 0u &&
+            (static_cast<uint32_t>(__popc(idle)) >= MGBVH_TRACE_REFILL || idle == kFull)) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(next, static_cast<uint32_t>(__popc(idle)));
+            base = __shfl_sync(kFull, base, 0);
+            if (base >= n_rays) exhausted = true;  // warp-uniform
+            if (!has) {
+                const uint32_t jr = base + static_cast<uint32_t>(__popc(idle & ((1u << lane) - 1u)));
+                if (jr < n_rays) {
+                    ri = order ? order[jr] : jr;
+                    const float4 o = rays[2 * ri], d = rays[2 * ri + 1];
+                    ox = o.x, oy = o.y, oz = o.z, dx = d.x, dy = d.y, dz = d.z;
+                    ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
+                    best = __int_as_float(0x7F800000);
+                    best_prim = kNoHit;
+                    st_node[0] = 0;
+                    st_t[0] = 0.0f;
+                    sp = 1;
+                    has = true;
+                }
+            }
+        }
+        if (!__any_sync(kFull, has)) {
+            if (exhausted) break;
+            continue;  // all lanes idle: the next round refills them
+        }
+        if (has && sp > 0) {
+            --sp;
+            if (!(st_t[sp] > best)) {
+                bool overflow = false;
+                    const uint32_t ni = st_node[sp];
+                    c_nodes++;
+                    const float4* q4 = reinterpret_cast<const float4*>(wn + ni);
+                    const float4 h0 = q4[0], h1 = q4[1], h2 = q4[2], h3 = q4[3], h4 = q4[4], h5 = q4[5], h6 = q4[6];
+                    const uint32_t ew = __float_as_uint(h0.w);
+                    const float sx = wstep(ew & 0xFFu), sy = wstep((ew >> 8) & 0xFFu), sz = wstep((ew >> 16) & 0xFFu);
+                    const uint32_t m = ew >> 24;
+                    const uint32_t ql[3][2] = {{__float_as_uint(h1.x), __float_as_uint(h1.y)},
+                                               {__float_as_uint(h1.z), __float_as_uint(h1.w)},
+                                               {__float_as_uint(h2.x), __float_as_uint(h2.y)}};
+                    const uint32_t qh[3][2] = {{__float_as_uint(h2.z), __float_as_uint(h2.w)},
+                                               {__float_as_uint(h3.x), __float_as_uint(h3.y)},
+                                               {__float_as_uint(h3.z), __float_as_uint(h3.w)}};
+                    const uint32_t refs[8] = {__float_as_uint(h4.x), __float_as_uint(h4.y), __float_as_uint(h4.z),
+                                              __float_as_uint(h4.w), __float_as_uint(h5.x), __float_as_uint(h5.y),
+                                              __float_as_uint(h5.z), __float_as_uint(h5.w)};
+                    const uint32_t cnt2[2] = {__float_as_uint(h6.x), __float_as_uint(h6.y)};
+                    float ent[8];
+                    uint32_t hitm = 0, leafm = 0;
+        #pragma unroll
+                    for (uint32_t j = 0; j < 8; ++j) {
+                        ent[j] = __int_as_float(0x7FFFFFFF);
+                        if (j < m) {
+                            const uint32_t sh = (j & 3u) * 8u, wd = j >> 2;
+                            const float4 lo = make_float4(wdeq(h0.x, (ql[0][wd] >> sh) & 0xFFu, sx),
+                                                          wdeq(h0.y, (ql[1][wd] >> sh) & 0xFFu, sy),
+                                                          wdeq(h0.z, (ql[2][wd] >> sh) & 0xFFu, sz), 0.0f);
+                            const float4 hi = make_float4(wdeq(h0.x, (qh[0][wd] >> sh) & 0xFFu, sx),
+                                                          wdeq(h0.y, (qh[1][wd] >> sh) & 0xFFu, sy),
+                                                          wdeq(h0.z, (qh[2][wd] >> sh) & 0xFFu, sz), 0.0f);
+                            c_boxes++;
+                            ent[j] = box_entry(ox, oy, oz, ix, iy, iz, lo, hi, best);
+                            if (ent[j] <= best) hitm |= 1u << j;
+                            if (refs[j] & kWideLeaf) leafm |= 1u << j;
+                        }
+                    }
+                    // leaf children, nearest first (selections over a bit mask: no
+                    // indexed arrays, everything stays in registers)
+                    uint32_t lm = hitm & leafm;
+                    while (lm) {
+                        float be = __int_as_float(0x7F800000);
+                        uint32_t bj = 0, br = 0, bc = 0;
+        #pragma unroll
+                        for (uint32_t j = 0; j < 8; ++j)
+                            if (((lm >> j) & 1u) && !(ent[j] >= be)) {
+                                be = ent[j];
+                                bj = j;
+                                br = refs[j];
+                                bc = (cnt2[j >> 2] >> ((j & 3u) * 8u)) & 0xFFu;
+                            }
+                        lm &= ~(1u << bj);
+                        if (be > best) continue;
+                        const uint32_t start = br & ~kWideLeaf;
+                        for (uint32_t q = start; q < start + bc; ++q) {
+                            const TriRec t = tris[q];
+                            c_tris++;
+                            const float tt = intersect_tri(ox, oy, oz, dx, dy, dz, t);
+                            const uint32_t prim = __float_as_uint(t.a.w);
+                            if (tt >= 0.0f && (tt < best || (tt == best && prim < best_prim))) {
+                                best = tt;
+                                best_prim = prim;
+                            }
+                        }
+                    }
+                    // internal children pushed farthest first (popped nearest first)
+                    uint32_t im = hitm & ~leafm;
+                    while (im) {
+                        float be = -1.0f;
+                        uint32_t bj = 0, br = 0;
+        #pragma unroll
+                        for (uint32_t j = 0; j < 8; ++j)
+                            if (((im >> j) & 1u) && ent[j] >= be) {
+                                be = ent[j];
+                                bj = j;
+                                br = refs[j];
+                            }
+                        im &= ~(1u << bj);
+                        if (be > best) continue;
+                        if (sp >= kWideStack) {
+                            overflow = true;
+                            break;
+                        }
+                        st_node[sp] = br;
+                        st_t[sp] = be;
+                        ++sp;
+                    }
+                if (overflow) {
+                    atomicExch(err, 1);
+                    sp = 0;
+                }
+            }
+        }
+        if (has && sp == 0) {
+            hit_t[ri] = best_prim == kNoHit ? -1.0f : best;
+            hit_prim[ri] = best_prim;
+            has = false;
+        }
+    }
+    if (counts) {
+        unsigned long long a = c_nodes, b = c_boxes, c = c_tris;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(kFull, a, off);
+            b += __shfl_down_sync(kFull, b, off);
+            c += __shfl_down_sync(kFull, c, off);
+        }
+        if (lane == 0) {
+            atomicAdd(&counts->nodes, a);
+            atomicAdd(&counts->boxes, b);
+            atomicAdd(&counts->tris, c);
+        }
+    }
+}
+
 // Ray order per traversal (tuning knobs): 0 as given, 1 direction bin then
 // origin, 2 origin cell then direction bin. Measured on 8.4M random rays in a
 // 16.8M-triangle scene: binary 34.2 / 44.6 / 49.3 Mrays/s, 8-wide 28.9 /
@@ -984,8 +1145,17 @@ int mgbvh_trace_closest_wide_dev(mgbvh_tracer* t, const float* d_rays, uint32_t 
     cudaEventRecord(t->ev0, sm);
     const float4* rays = reinterpret_cast<const float4*>(d_rays);
     const uint32_t* order = ray_order(t, rays, n_rays, sm, MGBVH_RAY_SORT_WIDE);
-    trace_wide_kernel<<<(n_rays + 127) / 128, 128, 0, sm>>>(t->wide, t->tris, rays, n_rays, d_hit_t, d_hit_prim,
-                                                             out_counts ? t->d_counts : nullptr, t->d_err, order);
+    if (MGBVH_TRACE_PERSISTENT) {
+        cudaMemsetAsync(t->d_next, 0, 4, sm);
+        const int pgrid = (int)std::min<uint32_t>((n_rays + 127) / 128, (uint32_t)t->trace_blocks);
+        trace_wide_persistent_kernel<<<pgrid, 128, 0, sm>>>(t->wide, t->tris, rays, n_rays, d_hit_t, d_hit_prim,
+                                                            out_counts ? t->d_counts : nullptr, t->d_err, order,
+                                                            t->d_next);
+    } else {
+        trace_wide_kernel<<<(n_rays + 127) / 128, 128, 0, sm>>>(t->wide, t->tris, rays, n_rays, d_hit_t,
+                                                                 d_hit_prim, out_counts ? t->d_counts : nullptr,
+                                                                 t->d_err, order);
+    }
     cudaEventRecord(t->ev1, sm);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
     Counts hc;
