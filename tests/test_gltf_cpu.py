@@ -108,3 +108,52 @@ def test_missing_attribute_is_an_error(tmp_path):
                             buf, "gltf")
     with pytest.raises(ValueError, match="normals"):
         gltf.GltfScenes.load(path)
+
+
+def _one_mesh_doc(buf, **prim_kw):
+    qv, qt = _quad()
+    p = gltf_files.mesh_primitive(buf, qv, qt)
+    p.update(prim_kw)
+    return {"meshes": [{"primitives": [p]}], "nodes": [{"mesh": 0}], "scenes": [{"nodes": [0]}]}, p
+
+
+def test_sparse_accessor_is_rejected(tmp_path):
+    buf = gltf_files.buffer()
+    doc, p = _one_mesh_doc(buf)
+    buf.accessors[p["attributes"]["POSITION"]]["sparse"] = {"count": 1}
+    path = gltf_files.write(str(tmp_path / "s"), doc, buf, "gltf")
+    with pytest.raises(ValueError, match="sparse"):
+        gltf.GltfScenes.load(path)
+
+
+def test_missing_indices_is_an_error(tmp_path):
+    buf = gltf_files.buffer()
+    doc, p = _one_mesh_doc(buf)
+    del p["indices"]
+    path = gltf_files.write(str(tmp_path / "i"), doc, buf, "glb")
+    with pytest.raises(ValueError, match="indices"):
+        gltf.GltfScenes.load(path)
+
+
+def test_glb_version_and_cycles(tmp_path):
+    buf = gltf_files.buffer()
+    doc, _ = _one_mesh_doc(buf)
+    path = gltf_files.write(str(tmp_path / "v"), doc, buf, "glb")
+    data = bytearray(open(path, "rb").read())
+    data[4] = 1  # version 1
+    bad = str(tmp_path / "v" / "bad.glb")
+    open(bad, "wb").write(bytes(data))
+    with pytest.raises(ValueError, match="version"):
+        gltf.GltfScenes.load(bad)
+    buf2 = gltf_files.buffer()
+    doc2, _ = _one_mesh_doc(buf2)
+    doc2["nodes"] = [{"mesh": 0, "children": [1]}, {"children": [0]}]
+    path2 = gltf_files.write(str(tmp_path / "c"), doc2, buf2, "gltf")
+    with pytest.raises(ValueError, match="cycle"):
+        gltf.GltfScenes.load(path2)
+
+
+def test_directory_without_gltf(tmp_path):
+    (tmp_path / "empty").mkdir()
+    with pytest.raises(FileNotFoundError):
+        gltf.GltfScenes.load(str(tmp_path / "empty"))
