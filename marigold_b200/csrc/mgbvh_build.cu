@@ -2262,15 +2262,17 @@ struct Caps {
     uint32_t tasks, tiles, medium, small, nodes;
 };
 
-// List capacities for n objects over `meshes` roots. Nodes above medium_max
-// are disjoint at one level (<= n / (medium_max + 1) of them), and a binary
-// tree over n objects has fewer than 2n / medium_max nodes above medium_max,
-// each with two children at most.
+// List capacities for n objects over `meshes` roots, each a bound that no
+// input can exceed: nodes above medium_max are disjoint at one level (<= n /
+// (medium_max + 1) of them, spanning <= n / kTile + that many tiles); the
+// queued subtrees of 33..medium_max objects are disjoint (none lies inside
+// another), so there are <= n / 33 of them, however unbalanced the tree; the
+// queued subtrees of 2..32 objects are disjoint too (<= n / 2).
 Caps caps_for(uint32_t n, uint32_t medium_max, uint32_t meshes, uint32_t node_slots) {
     Caps c;
     c.tasks = n / (medium_max + 1) + 2;
     c.tiles = n / kTile + c.tasks + 2;
-    c.medium = 4 * (n / medium_max) + meshes + 8;
+    c.medium = n / (kSmallMax + 1) + meshes + 8;
     c.small = n / 2 + meshes + 8;
     c.nodes = node_slots;
     return c;
