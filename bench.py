@@ -15,8 +15,8 @@ MIN = MAX = 1, max_depth 32, the reference's split profile (32 bins above
   cpu_baseline / --impl reference: the oracle port (faithful mode: the
          reference's algorithmic form, bvh/src/lib.rs) on host cores, one
          single-threaded build per process like the reference's sample
-         collector (bvh_sample_collector/src/main.rs:41-44), on a bounded
-         sample: the first 131,072 triangles of the same mesh.
+         collector (bvh_sample_collector/src/main.rs:41-44), on the same
+         1,310,720-triangle mesh (a step: one build per core, concurrently).
 
 With torchrun (N > 1) every rank builds its own replica (the path does not
 shard within a mesh); value = all ranks' triangles / the slowest rank's time.
@@ -93,6 +93,10 @@ def workload():
     return v, t, synth.mesh_bounds(v)
 
 
+def workload_triangles() -> int:
+    return 20 * 4 ** 8  # icosphere level 8
+
+
 # ---------------------------------------------------------------- CPU leg
 
 _cpu_mesh = None
@@ -100,17 +104,13 @@ _cpu_mesh = None
 
 def _cpu_init():
     global _cpu_mesh
-    from marigold_b200 import synth
-    v, t, _ = workload()
-    t = np.ascontiguousarray(t[:SAMPLE_TRIS])
-    aabb = synth.triangle_aabbs(v, t)
-    bounds = np.concatenate([aabb[:, 0:3].min(0), aabb[:, 3:6].max(0)]).astype(np.float32)
-    _cpu_mesh = (v, t, bounds)
+    v, t, b = workload()
+    _cpu_mesh = {"full": (v, t, b), "warm": (v, np.ascontiguousarray(t[:SAMPLE_TRIS]), None)}
 
 
-def _cpu_build(_):
+def _cpu_build(which):
     from oracle import oracle
-    v, t, b = _cpu_mesh
+    v, t, b = _cpu_mesh[which]
     t0 = time.perf_counter()
     r = oracle.build(v, t, root_bounds=b, faithful=True)
     dt = time.perf_counter() - t0
@@ -119,23 +119,29 @@ def _cpu_build(_):
 
 
 def cpu_measure(steps: int, warmup: int):
-    """Faithful oracle builds of the sample, one per process on every host core."""
+    """Faithful oracle builds of the whole workload mesh (1,310,720 triangles,
+    the same build the GPU times), one single-threaded build per process on
+    every host core, as the reference's sample collector runs its builds.
+    A step ends when the last core's build ends: Mtri/s = cores * triangles /
+    step time. Warm-up steps build the first SAMPLE_TRIS triangles only (they
+    are untimed and need not be long)."""
     cores = max(1, min(os.cpu_count() or 1, 64))
     ctx = mp.get_context("spawn")
     with ctx.Pool(cores, initializer=_cpu_init) as pool:
         for _ in range(warmup):
-            pool.map(_cpu_build, range(cores))
+            pool.map(_cpu_build, ["warm"] * cores)
         walls = []
         for _ in range(steps):
             t0 = time.perf_counter()
-            pool.map(_cpu_build, range(cores))
+            pool.map(_cpu_build, ["full"] * cores)
             walls.append(time.perf_counter() - t0)
     wall = sum(walls) / len(walls)
-    value = cores * SAMPLE_TRIS / wall / 1e6
+    n = workload_triangles()
+    value = cores * n / wall / 1e6
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {SAMPLE_TRIS} triangles of the workload mesh, one single-threaded "
-                      f"faithful-oracle build per core, {cores} concurrent, mean of {steps} steps",
-            "ms_per_step": wall * 1e3}
+            "sample": f"the whole workload mesh ({n} triangles), one single-threaded faithful-oracle "
+                      f"build per core, {cores} concurrent, mean of {steps} steps",
+            "same_config": True, "ms_per_step": wall * 1e3}
 
 
 # ---------------------------------------------------------------- clocks
@@ -194,6 +200,76 @@ def algorithmic_bytes(n, n_verts, internal_len_sum, node_count):
     """Bytes a build must move at minimum (per object per level of the
     partition: read + write of a 24-byte AABB and a 4-byte index)."""
     return (n * (12 + 3 * 32) + n * 24 + internal_len_sum * 56 + node_count * 32)
+
+
+def learned_leg(ctx, build_dev, c_args, c_count, d_nodes, d_lens, n, plain_sah, flush, stream, steps):
+    """The learned form on the headline mesh (committed proposer, refine gate
+    on): device-timed build Mtri/s as the plain build is timed, and its tree's
+    total SAH against the plain tree's."""
+    import torch
+    from marigold_b200 import learned
+    from marigold_b200.bvh import NODE_DTYPE, sah_cost
+    weights = torch.from_numpy(learned.load_weights().view(np.int16)).cuda()
+    ctx.set_split_proposer(weights, True)
+    try:
+        for _ in range(3):
+            flush.fill_(1)
+            ctx.check(build_dev(*c_args))
+        torch.cuda.synchronize()
+        ms = []
+        for k in range(steps):
+            flush.fill_(k & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(build_dev(*c_args))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        count = c_count.value
+        sah = sah_cost(d_nodes[: count * 8].cpu().numpy().view(NODE_DTYPE),
+                       d_lens[:count].cpu().numpy().view(np.uint32))
+    finally:
+        ctx.set_split_proposer(None)
+    bms = float(np.mean(ms))
+    return {"value": round(n / (bms * 1e-3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(bms, 4),
+            "sah": round(sah, 4), "plain_sah": round(plain_sah, 4),
+            "sah_delta_vs_plain_pct": round(100.0 * (sah / plain_sah - 1.0), 4),
+            "proposer": "marigold_b200/proposer_weights.bin, refine gate on"}
+
+
+def trace_leg(steps, flush, scale=4):
+    """Closest-hit Mrays/s on the mixed scene at 1/scale of its size (blobs,
+    ground grid and thin triangles each divided by scale; rays likewise):
+    plain build, then device-timed traces of every ray (L2 flushed before each);
+    the first 4,096 rays' hits compared with GPU brute force."""
+    import ctypes
+    import torch
+    from marigold_b200 import BvhSettings, _lib, build_device, synth
+    v, t = synth.mixed_scene(n_blob=8388608 // scale, grid=(2048, 1024 // scale), n_thin=4194304 // scale)
+    n = t.shape[0]
+    rays = synth.rays_in_box(8388608 // scale, v[:, :3].min(0), v[:, :3].max(0))
+    m = rays.shape[0]
+    ctx = _lib.Context(0)
+    ctx.set_tuning(1024)
+    tr = _lib.Tracer(0)
+    stream = torch.cuda.current_stream()
+    try:
+        dv = torch.from_numpy(v).cuda()
+        dt = torch.from_numpy(t.view(np.int32)).cuda()
+        dr = torch.from_numpy(rays).cuda()
+        d_nodes = torch.empty((2 * n - 1) * 8, dtype=torch.int32, device="cuda")
+        d_perm = torch.empty(n, dtype=torch.int32, device="cuda")
+        count, rc, _ = build_device(ctx, BvhSettings(max_depth=32), d_nodes, d_perm, vertices=dv,
+                                    triangles=dt, stream=stream)
+        torch.cuda.synchronize()
+        mrays, hits, mism = _trace_rate(tr, d_nodes, count, dv, dt, d_perm, n, dr, m, stream, flush, steps)
+    finally:
+        tr.close()
+        ctx.close()
+    return {"value": round(mrays, 3), "unit": "Mrays/s", "rays": m, "triangles": n, "hit_rays": hits,
+            "mismatches_vs_gpu_bruteforce_4096": mism,
+            "scene": f"mixed scene at 1/{scale} size: 64 Gaussian blobs, 2048 x {1024 // scale}-quad ground grid, "
+                     f"thin 1:200 triangles; rays uniform in the scene box grown by 10%, uniform directions"}
 
 
 def run_ours(args):
@@ -339,6 +415,19 @@ def run_ours(args):
     h2d = v.nbytes + t.nbytes
     d2h = cnt.value * 32 + cnt.value * 4 + n * 4
 
+    # the metric's other two figures, on one GPU: the learned form against the
+    # plain build on this mesh, and closest-hit Mrays/s on a mixed scene
+    extras = {}
+    if world == 1:
+        from marigold_b200.bvh import NODE_DTYPE, sah_cost
+        ctx.set_stream(stream.cuda_stream)
+        plain_sah = sah_cost(nodes_h.reshape(-1).view(NODE_DTYPE), lens_h.astype(np.uint32))
+        with ClockSampler(local) as xclocks:
+            extras["learned"] = learned_leg(ctx, build_dev, c_args, c_count, d_nodes, d_lens, n, plain_sah,
+                                            flush, stream, args.steps)
+            extras["trace"] = trace_leg(max(3, args.steps // 2), flush)
+        extras["learned"]["clocks"] = extras["trace"]["clocks"] = xclocks.summary()
+
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
@@ -365,9 +454,10 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "nodes": int(count),
+        **extras,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_measure(steps=2, warmup=1)
+        out["cpu_baseline"] = cpu_measure(steps=1, warmup=0)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -384,7 +474,7 @@ def run_reference(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(cb["ms_per_step"], 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded noisy icosphere)",
-        "config": {"workload": WORKLOAD, "triangles": 1310720, "sample_triangles": SAMPLE_TRIS,
+        "config": {"workload": WORKLOAD, "triangles": workload_triangles(), "same_config": True,
                    "min_leaf": 1, "max_leaf": 1, "max_depth": 32, "parallelism": "host cores"},
         "cpu_baseline": cb,
         "e2e": {"value": round(cb["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -443,6 +533,7 @@ def run_mixed(args):
     bp = torch.empty(sub, dtype=torch.int32, device="cuda")
     forms = {}
     brute = None
+    clocks = ClockSampler(0).__enter__()  # sampled through every timed build and trace below
     for form in ("plain", "learned"):
         ctx.set_split_proposer(weights if form == "learned" else None, True)
         build_ms, count, st = [], 0, {}
@@ -512,9 +603,11 @@ def run_mixed(args):
                            "nodes_visited": wcounts[0], "box_tests": wcounts[1],
                            "triangle_tests": wcounts[2], "mismatches_vs_gpu_bruteforce": wmism},
         }
+    clocks.__exit__()
     ctx.set_split_proposer(None)
     out = {
         "metric": "BVH build Mtri/s; closest-hit Mrays/s", "workload": "mixed scene",
+        "clocks": clocks.summary(),
         "config": {"triangles": n, "rays": m, "blobs": 64, "grid_quads": [2048, 1024 // sc],
                    "thin": 4194304 // sc, "scale": sc, "max_depth": 32, "leaf": 1,
                    "profile": "reference", "learned": "committed proposer, gate on"},
@@ -569,22 +662,23 @@ def run_batched(args):
     settings = BvhSettings(bins=bins)
     times, replays, eager_ms = [], 0, None
     offs = None
-    for k in range(max(args.warmup, 2) + args.steps):
-        flush.fill_(k & 0xFF)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        ctx.set_stream(stream.cuda_stream)
-        instance_aabbs_device(ctx, d_bounds, d_ids, d_xf, d_inst)
-        offs, rc, st = build_batch_device(ctx, settings, descs, nodes, perm, out_lens=lens,
-                                          stream=stream)
-        e1.record(stream)
-        stream.synchronize()
-        if k == 0:
-            eager_ms = e0.elapsed_time(e1)
-        if k >= max(args.warmup, 2):
-            times.append(e0.elapsed_time(e1))
-            replays += st["graph_replay"]
+    with ClockSampler(0) as clocks:
+        for k in range(max(args.warmup, 2) + args.steps):
+            flush.fill_(k & 0xFF)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.set_stream(stream.cuda_stream)
+            instance_aabbs_device(ctx, d_bounds, d_ids, d_xf, d_inst)
+            offs, rc, st = build_batch_device(ctx, settings, descs, nodes, perm, out_lens=lens,
+                                              stream=stream)
+            e1.record(stream)
+            stream.synchronize()
+            if k == 0:
+                eager_ms = e0.elapsed_time(e1)
+            if k >= max(args.warmup, 2):
+                times.append(e0.elapsed_time(e1))
+                replays += st["graph_replay"]
     from marigold_b200.bvh import NODE_DTYPE, sah_cost
     nh = nodes.cpu().numpy().view(NODE_DTYPE)
     lh = lens.cpu().numpy().view(np.uint32)
@@ -594,6 +688,7 @@ def run_batched(args):
     out = {
         "metric": "BVH build Mtri/s (batched: 512 BLAS + TLAS)", "workload": "batched scene",
         "value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms_per_step": round(ms, 3),
+        "clocks": clocks.summary(),
         "eager_first_build_ms": round(eager_ms, 3), "graph_replays": replays, "steps": args.steps,
         "config": {"meshes": len(meshes), "triangles": n_tris, "instances": int(inst.shape[0]),
                    "trees": len(meshes) + 1, "nodes": int(offs[-1]), "medium_max": medium_max,
@@ -663,6 +758,7 @@ def run_learned(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
     rows = []
+    clocks = ClockSampler(0).__enter__()  # sampled through every timed build and trace below
     for name, kind, size, seed in learned.EVAL_MESHES:
         v, t = learned.eval_mesh(kind, size, seed)
         n = t.shape[0]
@@ -708,11 +804,13 @@ def run_learned(args):
         ctx.set_split_proposer(None)
         rows.append(row)
         print(json.dumps(row), file=sys.stderr, flush=True)
+    clocks.__exit__()
     tr.close()
     rec = learned.load_record()
     out = {
         "metric": "learned split proposer: SAH vs plain binned and full sweep; build Mtri/s; Mrays/s",
         "workload": "learned split proposer, held-out meshes", "dtype": "f32 (network bf16/fp32)",
+        "clocks": clocks.summary(),
         "steps": args.steps, "warmup": args.warmup, "results": rows,
         "network": {"samples": rec.get("samples"), "steps": rec.get("steps"),
                     "heldout_accuracy": rec.get("heldout_accuracy")},

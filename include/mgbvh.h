@@ -272,9 +272,12 @@ MGBVH_API int mgbvh_instance_aabbs_dev(mgbvh_ctx* ctx, const float* d_mesh_bound
  * 140 KB of device memory on every device that loads the library, held until
  * the process exits), shared by all calls: calls whose work overlaps on the
  * GPU (several host threads, or several streams) race on it and must be
- * serialized by the caller. The first call on each device does a one-time
- * set-up on the current device (looks up the array's device address, sets a
- * kernel attribute), so make that first call before any stream capture.
+ * serialized by the caller. Every call sets up on the current device: it
+ * looks up the array's device address there (cudaGetSymbolAddress, which
+ * allocates nothing) and sets a kernel attribute; nothing is cached between
+ * calls, so a call after a device reset uses the new context's array. The
+ * first call on a device also loads the library's device code there (CUDA
+ * loads modules lazily), so make that first call before any stream capture.
  *
  * Same tree, permutation and status codes as mgbvh_build_aabbs_dev.
  * d_aabbs, d_out_nodes, d_out_lens (nullable) and d_out_perm are device
@@ -351,6 +354,68 @@ MGBVH_API int mgbvh_trace_closest_wide_dev(mgbvh_tracer* tracer, const float* d_
 MGBVH_API int mgbvh_trace_bruteforce_dev(mgbvh_tracer* tracer, const float* d_rays,
                                          uint32_t n_rays, float* d_hit_t, uint32_t* d_hit_prim,
                                          void* cuda_stream);
+
+/*
+ * Two-level scenes: the TLAS over instances, each instance a mesh with its
+ * own BLAS, walked as marigold's scene shader walks them
+ * (marigold/assets/shaders/slang/lib/scene.slang:91-141 raytraceTlas,
+ * :143-220 raytraceBlas). The records are the ones marigold uploads for the
+ * shader (marigold/src/app/data/scene/model.rs:167-234 and
+ * geometry/mod.rs:175-199; the shader's Mesh: inverseTransform, blasRoot,
+ * vertexOffset, triangleOffset).
+ */
+typedef struct mgbvh_scene_mesh {
+    uint32_t blas_root;       /* its BLAS's root in the BLAS node array; child links are relative to it */
+    uint32_t triangle_offset; /* its first triangle in the scene triangle array */
+    uint32_t triangle_count;
+    uint32_t vertex_offset;   /* added to its triangles' vertex indices */
+} mgbvh_scene_mesh;
+
+typedef struct mgbvh_scene_instance {
+    float inverse_transform[16]; /* column-major, world space -> mesh space */
+    uint32_t mesh;               /* index into the mesh table */
+    uint32_t pad[3];
+} mgbvh_scene_instance;
+
+/* Binds a scene (device pointers, which must stay valid while tracing; the
+   mesh table is copied). The TLAS's leaves index d_instances, which are in
+   the TLAS build's permuted order (as the crate leaves the instance list);
+   each mesh's BLAS leaves index its triangles, which sit in the scene
+   triangle array in that BLAS build's permuted order, as vertex index
+   triples relative to the mesh's vertex_offset. Lens arrays (NULL = one
+   object per leaf) are node-aligned with their node arrays. Gathers the
+   triangles with their vertices. */
+MGBVH_API int mgbvh_tracer_set_scene_dev(mgbvh_tracer* tracer, const mgbvh_node* d_tlas_nodes,
+                                         uint32_t tlas_node_count, const uint32_t* d_tlas_lens,
+                                         const mgbvh_scene_instance* d_instances, uint32_t instance_count,
+                                         const mgbvh_scene_mesh* d_meshes, uint32_t mesh_count,
+                                         const mgbvh_node* d_blas_nodes, uint32_t blas_node_count,
+                                         const uint32_t* d_blas_lens, const float* d_vertices,
+                                         uint32_t vertex_stride_bytes, uint32_t vertex_count,
+                                         const uint32_t* d_triangles, uint32_t triangle_count,
+                                         void* cuda_stream);
+/* Closest hit of every world-space ray through the scene: the TLAS with the
+   world ray, each reached instance's BLAS with the ray moved into mesh space
+   by its inverse transform. Hit distances are the world ray's parameter in
+   every instance (the shader's rescaling by the mesh-space direction length,
+   scene.slang:168-169, is wrong for scaled instances and is not copied).
+   Results per ray: distance (-1 for a miss), the instance (position in
+   d_instances) and the triangle (position in the scene triangle array), both
+   0xFFFFFFFF for a miss; equal distances resolve to the lowest (instance,
+   triangle). Rays are sorted by origin cell of the TLAS root box and
+   direction bin first, as in mgbvh_trace_closest_dev. out_counts: nodes
+   visited (both levels), box tests, triangle tests. */
+MGBVH_API int mgbvh_trace_scene_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
+                                    float* d_hit_t, uint32_t* d_hit_instance, uint32_t* d_hit_triangle,
+                                    uint64_t* out_counts, double* out_seconds, void* cuda_stream);
+/* The check for mgbvh_trace_scene_dev: every ray against every triangle of
+   every instance, in mesh space, same test and tie rule. cull_by_mesh_bounds
+   != 0 skips instances whose mesh-space ray misses the mesh's BLAS root box
+   grown by a relative 1e-4 (for large scenes). */
+MGBVH_API int mgbvh_trace_scene_bruteforce_dev(mgbvh_tracer* tracer, const float* d_rays, uint32_t n_rays,
+                                               float* d_hit_t, uint32_t* d_hit_instance,
+                                               uint32_t* d_hit_triangle, int cull_by_mesh_bounds,
+                                               void* cuda_stream);
 
 /*
  * Learned split proposer (no counterpart in the reference). A small MLP,

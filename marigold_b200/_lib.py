@@ -36,6 +36,7 @@ EXPORTED = (
     "mgbvh_mlp_train_step_dev", "mgbvh_mlp_forward_dev", "mgbvh_mlp_adam_dev",
     "mgbvh_set_split_proposer", "mgbvh_set_sample_output", "mgbvh_instance_aabbs_dev",
     "mgbvh_tracer_build_wide", "mgbvh_tracer_wide_nodes", "mgbvh_trace_closest_wide_dev",
+    "mgbvh_tracer_set_scene_dev", "mgbvh_trace_scene_dev", "mgbvh_trace_scene_bruteforce_dev",
 )
 
 
@@ -173,6 +174,14 @@ def load():
         L.mgbvh_trace_closest_wide_dev.restype = ctypes.c_int
         L.mgbvh_trace_bruteforce_dev.argtypes = [P, P, u32, P, P, P]
         L.mgbvh_trace_bruteforce_dev.restype = ctypes.c_int
+        L.mgbvh_tracer_set_scene_dev.argtypes = [P, P, u32, P, P, u32, P, u32, P, u32, P, P, u32, u32, P, u32,
+                                                 P]
+        L.mgbvh_tracer_set_scene_dev.restype = ctypes.c_int
+        L.mgbvh_trace_scene_dev.argtypes = [P, P, u32, P, P, P, ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_double), P]
+        L.mgbvh_trace_scene_dev.restype = ctypes.c_int
+        L.mgbvh_trace_scene_bruteforce_dev.argtypes = [P, P, u32, P, P, P, ctypes.c_int, P]
+        L.mgbvh_trace_scene_bruteforce_dev.restype = ctypes.c_int
         L.mgbvh_build_batch_dev.argtypes = [P, ctypes.POINTER(MeshDesc), u32, ctypes.POINTER(Settings),
                                             P, u32, P, P, pu32, ctypes.POINTER(Stats)]
         L.mgbvh_build_batch_dev.restype = ctypes.c_int

@@ -15,7 +15,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmgbvh.so")
 SOURCES = ["mgbvh_build.cu", "mgbvh_trace.cu", "mgbvh_mlp.cu"]
-HEADERS = ["mgbvh_exact.cuh", "mgbvh_device.cuh", "mgbvh_mlp.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -36,7 +35,9 @@ def _stale() -> bool:
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    # every header under csrc/: a header left out of the list would not trigger a rebuild
+    headers = sorted(f for f in os.listdir(CSRC) if f.endswith((".cuh", ".h")))
+    deps = [os.path.join(CSRC, f) for f in SOURCES + headers]
     deps.append(os.path.join(HERE, "..", "include", "mgbvh.h"))
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))

@@ -322,3 +322,92 @@ def instance_aabbs_device(ctx: Context, mesh_bounds, instance_mesh, transforms, 
     vp = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
     ctx.check(ctx.L.mgbvh_instance_aabbs_dev(ctx.ptr, vp(mesh_bounds), mesh_bounds.shape[0],
                                              vp(instance_mesh), vp(transforms), n, vp(out_aabbs)))
+
+
+class Scene:
+    """A two-level scene on the device, laid out as marigold uploads it for its
+    scene shader (marigold/src/app/data/scene/model.rs:167-234,
+    geometry/mod.rs:175-199): the TLAS nodes, the instance records in the TLAS
+    build's permuted order (inverse transform + mesh index), the mesh table
+    (BLAS root, triangle offset and count, vertex offset), the BLAS nodes of
+    every mesh, the vertex positions and every mesh's triangles in its BLAS
+    build's permuted order, vertex indices relative to the mesh's vertex
+    offset.
+
+    from_batch assembles it from one batched build (build_batch_device) whose
+    descriptors were the meshes followed by the TLAS over the instances' world
+    boxes: `meshes` the (vertices [V, k], triangles [N, 3]) device tensors of
+    the BLAS meshes, `offsets`, `nodes`, `lens`, `perm` that build's outputs,
+    `instance_mesh` [I] and `transforms` [I, 16] (column-major, mesh ->
+    world) the instances in their original order. The inverse transforms are
+    computed in float64 and rounded to float32."""
+
+    def __init__(self, **tensors):
+        self.__dict__.update(tensors)
+
+    @classmethod
+    def from_batch(cls, meshes, offsets, nodes, lens, perm, instance_mesh, transforms):
+        import torch
+        m = len(meshes)
+        dev = nodes.device
+        counts = [int(t.shape[0]) for _, t in meshes]
+        tri_off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        vcounts = [int(v.shape[0]) for v, _ in meshes]
+        v_off = np.concatenate([[0], np.cumsum(vcounts)]).astype(np.int64)
+        tris, verts = [], []
+        for k, (v, t) in enumerate(meshes):
+            p = perm[tri_off[k]:tri_off[k + 1]].long()
+            tris.append(t.reshape(-1, 3)[p].to(torch.int32))
+            verts.append(v[:, :3].float())
+        mesh_tab = torch.tensor(np.stack([np.asarray(offsets[:m], np.int64), tri_off[:m],
+                                          np.asarray(counts, np.int64), v_off[:m]], 1).astype(np.uint32).view(np.int32),
+                                device=dev)
+        n_inst = int(instance_mesh.shape[0])
+        tlas_first = int(tri_off[m])
+        tlas_perm = perm[tlas_first:tlas_first + n_inst].long()
+        a = transforms.double().reshape(-1, 4, 4).transpose(1, 2)  # [instance, row, column]
+        inv = torch.linalg.inv(a).transpose(1, 2).reshape(-1, 16).float()  # back to column-major
+        rec = torch.zeros((n_inst, 20), dtype=torch.int32, device=dev)
+        rec[:, :16] = inv.view(torch.int32)
+        rec[:, 16] = instance_mesh.to(torch.int32)
+        rec = rec[tlas_perm].contiguous()
+        lo, hi = int(offsets[m]), int(offsets[m + 1])
+        return cls(tlas_nodes=nodes[lo * 8:hi * 8], tlas_count=hi - lo,
+                   tlas_lens=None if lens is None else lens[lo:hi],
+                   instances=rec, instance_count=n_inst, meshes=mesh_tab, mesh_count=m,
+                   blas_nodes=nodes[:lo * 8], blas_count=lo, blas_lens=None if lens is None else lens[:lo],
+                   vertices=torch.cat(verts).contiguous(), triangles=torch.cat(tris).contiguous(),
+                   triangle_count=int(tri_off[m]), instance_order=tlas_perm)
+
+    def bind(self, tracer, stream=None):
+        """mgbvh_tracer_set_scene_dev on `tracer` (an _lib.Tracer)."""
+        vp = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+        sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        tracer.check(tracer.L.mgbvh_tracer_set_scene_dev(
+            tracer.ptr, vp(self.tlas_nodes), self.tlas_count, vp(self.tlas_lens), vp(self.instances),
+            self.instance_count, vp(self.meshes), self.mesh_count, vp(self.blas_nodes), self.blas_count,
+            vp(self.blas_lens), vp(self.vertices), 12, int(self.vertices.shape[0]), vp(self.triangles),
+            self.triangle_count, sp))
+
+
+def trace_scene_device(tracer, rays, *, stream=None, bruteforce=False, cull=False):
+    """Closest hits of rays (float32 [n, 8] device tensor) through the scene
+    bound to `tracer`: (t float32 [n], instance int32 [n], triangle int32 [n],
+    counters or None, device seconds or None). bruteforce=True runs the
+    brute-force check instead of the traversal."""
+    import torch
+    n = int(rays.shape[0])
+    t = torch.empty(n, dtype=torch.float32, device=rays.device)
+    hi = torch.empty(n, dtype=torch.int32, device=rays.device)
+    hp = torch.empty(n, dtype=torch.int32, device=rays.device)
+    vp = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    sp = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+    if bruteforce:
+        tracer.check(tracer.L.mgbvh_trace_scene_bruteforce_dev(tracer.ptr, vp(rays), n, vp(t), vp(hi), vp(hp),
+                                                               1 if cull else 0, sp))
+        return t, hi, hp, None, None
+    counts = (ctypes.c_uint64 * 3)()
+    secs = ctypes.c_double(0)
+    tracer.check(tracer.L.mgbvh_trace_scene_dev(tracer.ptr, vp(rays), n, vp(t), vp(hi), vp(hp), counts,
+                                                ctypes.byref(secs), sp))
+    return t, hi, hp, list(counts), secs.value

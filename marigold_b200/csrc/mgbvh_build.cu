@@ -33,6 +33,7 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "mgbvh_device.cuh"
@@ -72,7 +73,7 @@ struct Task {
 
 // Split decision of one large node, read by its partition tiles.
 struct Decision {
-    uint32_t kind;  // 0 split, 1 leaf
+    uint32_t kind;  // 0 split, 1 leaf, 2 forced median (deferred to the median passes)
     uint32_t axis, split_bin, bins;
     float cmin, ext;
     uint32_t n_lt;
@@ -414,6 +415,7 @@ struct EvalArgs {
     LvlRefine* refine;
     uint32_t* rbins;
     const uint32_t* tile_hist2;  // [proposal * 17 + interval][tile]: objects in intervals 0..interval
+    Task* med;  // nodes waiting for a forced median (cap_tasks entries; count in ctr->n_med)
 };
 
 // Writes the node and its children of a decided split: the per-tile lt
@@ -585,7 +587,18 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         const uint32_t wlo = static_cast<uint32_t>(wk);
         if (wlo == kNoKey) {
             if (t.len > P.max_leaf) {
-                if (lane == 0) set_error(O.ctr, MGBVH_ERR_UNSUPPORTED, kSiteLargeMedian);
+                // no binned split and too many objects for a leaf: the forced
+                // median (bvh/src/lib.rs:527-531) runs in the median passes
+                // after this build's pipeline; the partition skips the node
+                if (lane == 0) {
+                    d.kind = 2;
+                    A.dec[w] = d;
+                    const uint32_t mi = atomicAdd(&O.ctr->n_med, 1u);
+                    if (mi < A.cap_tasks)
+                        A.med[mi] = t;
+                    else
+                        set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                }
                 return;
             }
             leaf = true;
@@ -982,9 +995,10 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_
         const uint32_t cnt = min(kTile, tlen - begin);
         const Rec* src = (t.buf ? rec1 : rec0) + tstart + begin;
         Rec* dst = t.buf ? rec0 : rec1;
-        if (d.kind == 1) {
-            for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-                O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
+        if (d.kind != 0) {  // 1: leaf; 2: forced median, partitioned by the median passes
+            if (d.kind == 1)
+                for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+                    O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
             continue;
         }
         const uint32_t axis = d.axis, split_bin = d.split_bin, nbins = d.bins, n_lt = d.n_lt;
@@ -1080,6 +1094,315 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_
             }
         }
         __syncthreads();  // wcnt/sk/sbad are rewritten by the next tile
+    }
+}
+
+// ---------------------------------------------------------------- forced median of large nodes
+//
+// median_split (bvh/src/lib.rs:444-491) on axes 0, 1 and 2 in turn over the
+// same list (:527-531), for the level-pass nodes whose binned sweeps all
+// refused (lvl_eval_kernel queues them). The waiting nodes' objects form one
+// element range, node s owning elements moff[s] .. moff[s+1] in list order.
+// Per axis:
+//   med_key_kernel      (node, centroid key) per element, position as value
+//   radix sort          stable, so equal keys stay in list order
+//   med_flag_kernel     element in lt <=> (key, position) <= the node's m-th
+//                       smallest pair, m = len / 2: the set
+//                       select_nth_unstable_by(m, total_cmp) puts first, ties
+//                       taken in list order
+//   exclusive scan      of the flags
+//   med_scatter_kernel  stable partition into the other record buffer; box
+//                       keys of both halves on this axis
+// Axis 0 moves the records buf -> buf^1, axis 1 back, axis 2 to buf^1 (the
+// children's buffer): the list ends in axis-2 order whichever axis wins, as
+// in the reference. med_finish_kernel takes the cheapest axis (first minimum
+// of total_cmp), applies the containment assertion (:637-646) to the final
+// halves and writes the node and its children.
+
+struct MedSeg {
+    uint32_t box[3][12];  // per axis: lt box keys (lo xyz, hi xyz), then gt box keys
+    uint32_t ckeys[12];   // centroid keys of the final halves: lt lo xyz, lt hi xyz, gt lo xyz, gt hi xyz
+};
+
+// Where a median node's children go (the next pipeline run starts at level 0).
+struct MedOut {
+    Task* tasks;
+    uint32_t* bins;
+    uint32_t* cbkeys;
+    uint32_t* tile_task;
+    uint32_t* tile_begin;
+    Task* medium;
+    Task* small;
+    uint32_t cap_tasks, cap_tiles, cap_medium, cap_small;
+};
+
+__device__ __forceinline__ bool child_is_leaf(uint32_t len, uint32_t depth, const Params& P) {
+    return len <= 1u || depth == P.max_depth || (len <= P.max_leaf && len < 2u * P.min_leaf);
+}
+
+// The waiting node that owns element e: the last s with moff[s] <= e.
+__device__ __forceinline__ uint32_t med_node_of(const uint32_t* __restrict__ moff, uint32_t np, uint32_t e) {
+    uint32_t lo = 0, hi = np;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (moff[mid] <= e)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void med_reset_kernel(Counters* ctr) {
+    if (threadIdx.x < 4) ctr->lvl[threadIdx.x >> 1][threadIdx.x & 1u] = 0;
+    if (threadIdx.x == 0) {
+        ctr->n_medium = 0;
+        ctr->n_small = 0;
+        ctr->n_med = 0;
+    }
+}
+
+__global__ void med_init_kernel(MedSeg* seg, uint32_t np) {
+    const uint32_t words = sizeof(MedSeg) / 4;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np * words; i += gridDim.x * blockDim.x) {
+        const uint32_t q = (i % words) % 6u;
+        reinterpret_cast<uint32_t*>(seg)[i] = q < 3 ? kKeyPosInf : kKeyNegInf;
+    }
+}
+
+__global__ void __launch_bounds__(256) med_key_kernel(const Task* __restrict__ mt, const uint32_t* __restrict__ moff,
+                                                      uint32_t np, uint32_t E, const Rec* __restrict__ rec0,
+                                                      const Rec* __restrict__ rec1, uint32_t axis,
+                                                      unsigned long long* __restrict__ keys,
+                                                      uint32_t* __restrict__ vals) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint32_t s = med_node_of(moff, np, e);
+        const uint32_t i = e - moff[s];
+        const Rec* src = ((mt[s].buf ^ (axis & 1u)) ? rec1 : rec0) + mt[s].start;
+        const float lo = reinterpret_cast<const float*>(&src[i].lo)[axis];
+        const float hi = reinterpret_cast<const float*>(&src[i].hi)[axis];
+        keys[e] = (static_cast<unsigned long long>(s) << 32) | fkey(center_of(lo, hi));
+        vals[e] = i;
+    }
+}
+
+__global__ void __launch_bounds__(256) med_flag_kernel(const Task* __restrict__ mt, const uint32_t* __restrict__ moff,
+                                                       uint32_t np, uint32_t E,
+                                                       const unsigned long long* __restrict__ keys,
+                                                       const unsigned long long* __restrict__ sorted_keys,
+                                                       const uint32_t* __restrict__ sorted_vals,
+                                                       uint32_t* __restrict__ flag) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        const uint32_t s = med_node_of(moff, np, e);
+        const uint32_t i = e - moff[s];
+        const uint32_t c = moff[s] + mt[s].len / 2u - 1u;  // the m-th smallest (key, position)
+        const uint32_t cut_key = static_cast<uint32_t>(sorted_keys[c]), cut_pos = sorted_vals[c];
+        const uint32_t k = static_cast<uint32_t>(keys[e]);
+        flag[e] = (k < cut_key || (k == cut_key && i <= cut_pos)) ? 1u : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(256) med_scatter_kernel(const Task* __restrict__ mt,
+                                                          const uint32_t* __restrict__ moff, uint32_t np,
+                                                          uint32_t E, Rec* rec0, Rec* rec1, uint32_t axis,
+                                                          const uint32_t* __restrict__ flag,
+                                                          const uint32_t* __restrict__ scan, MedSeg* seg,
+                                                          Params P, Out O) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    // whole warps step together (the reductions below take every lane)
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < E; base += nwarps * 32u) {
+        const uint32_t e = base + lane;
+        const bool valid = e < E;
+        uint32_t s = 0, bk[6], ck[3];
+        bool lt = false;
+        if (valid) {
+            s = med_node_of(moff, np, e);
+            const Task& t = mt[s];
+            const uint32_t i = e - moff[s], m = t.len / 2u;
+            const uint32_t sb = t.buf ^ (axis & 1u);
+            const Rec r = ((sb ? rec1 : rec0) + t.start)[i];
+            lt = flag[e] != 0u;
+            const uint32_t lt_before = scan[e] - scan[moff[s]];
+            const uint32_t pos = lt ? lt_before : m + (i - lt_before);
+            if (pos < t.len) {
+                ((sb ? rec0 : rec1) + t.start)[pos] = r;
+                // axis 2 leaves the final order: a leaf child's objects are placed
+                if (axis == 2u && child_is_leaf(lt ? m : t.len - m, t.depth + 1u, P))
+                    O.perm[t.start + pos] = __float_as_uint(r.lo.w);
+            } else {
+                set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteMedian);
+            }
+            bk[0] = fkey(r.lo.x);
+            bk[1] = fkey(r.lo.y);
+            bk[2] = fkey(r.lo.z);
+            bk[3] = fkey(r.hi.x);
+            bk[4] = fkey(r.hi.y);
+            bk[5] = fkey(r.hi.z);
+            ck[0] = fkey(center_of(r.lo.x, r.hi.x));
+            ck[1] = fkey(center_of(r.lo.y, r.hi.y));
+            ck[2] = fkey(center_of(r.lo.z, r.hi.z));
+        }
+        const uint32_t s0 = __shfl_sync(kFull, s, 0);
+        if (__all_sync(kFull, !valid || s == s0)) {
+            // one node under the whole warp: reduce per half, then one atomic per word
+#pragma unroll
+            for (int q = 0; q < 12; ++q) {
+                const bool mine = valid && (lt == (q < 6));
+                const bool is_min = (q % 6) < 3;
+                const uint32_t v = mine ? bk[q % 6] : (is_min ? kKeyPosInf : kKeyNegInf);
+                const uint32_t r = is_min ? __reduce_min_sync(kFull, v) : __reduce_max_sync(kFull, v);
+                if (lane == 0) {
+                    if (is_min)
+                        atomicMin(&seg[s0].box[axis][q], r);
+                    else
+                        atomicMax(&seg[s0].box[axis][q], r);
+                }
+            }
+            if (axis == 2u) {
+#pragma unroll
+                for (int q = 0; q < 12; ++q) {
+                    const bool mine = valid && (lt == (q < 6));
+                    const bool is_min = (q % 6) < 3;
+                    const uint32_t v = mine ? ck[q % 3] : (is_min ? kKeyPosInf : kKeyNegInf);
+                    const uint32_t r = is_min ? __reduce_min_sync(kFull, v) : __reduce_max_sync(kFull, v);
+                    if (lane == 0) {
+                        if (is_min)
+                            atomicMin(&seg[s0].ckeys[q], r);
+                        else
+                            atomicMax(&seg[s0].ckeys[q], r);
+                    }
+                }
+            }
+        } else if (valid) {
+            // a node boundary inside the warp: per-lane atomics
+            uint32_t* b = seg[s].box[axis] + (lt ? 0 : 6);
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                atomicMin(b + q, bk[q]);
+                atomicMax(b + 3 + q, bk[3 + q]);
+            }
+            if (axis == 2u) {
+                uint32_t* c = seg[s].ckeys + (lt ? 0 : 6);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    atomicMin(c + q, ck[q]);
+                    atomicMax(c + 3 + q, ck[q]);
+                }
+            }
+        }
+    }
+}
+
+// One warp per median node: the cheapest axis, the containment assertion,
+// the node and its two children (leaf, level-pass task, subtree CTA task or
+// warp subtree task).
+__global__ void __launch_bounds__(128) med_finish_kernel(const Task* __restrict__ mt, uint32_t np,
+                                                         const MedSeg* __restrict__ seg, MedOut M, Params P,
+                                                         Out O) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < np; s += nwarps) {
+        const Task t = mt[s];
+        const MedSeg& G = seg[s];
+        const uint32_t n = t.len, m = n / 2u;
+        const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+        uint64_t key = ~0ull;
+        if (lane < 3) {
+            float lb[6], gb[6];
+            for (int q = 0; q < 6; ++q) {
+                lb[q] = funkey(G.box[lane][q]);
+                gb[q] = funkey(G.box[lane][6 + q]);
+            }
+            key = cand_key(split_cost(surface_area6(lb), surface_area6(gb), surface_area6(nb), m, n - m), lane, 0u);
+        }
+        const uint32_t axis = (static_cast<uint32_t>(warp_min_key(key)) >> 8) & 3u;
+        float ltb[6], gtb[6];
+        for (int q = 0; q < 6; ++q) {
+            ltb[q] = funkey(G.box[axis][q]);
+            gtb[q] = funkey(G.box[axis][6 + q]);
+        }
+        // every centroid of a half inside that half's box: the corners of the
+        // half's centroid bounds inside it
+        const uint32_t* ck = G.ckeys;
+        const bool ok = box_contains(ltb, funkey(ck[0]), funkey(ck[1]), funkey(ck[2])) &&
+                        box_contains(ltb, funkey(ck[3]), funkey(ck[4]), funkey(ck[5])) &&
+                        box_contains(gtb, funkey(ck[6]), funkey(ck[7]), funkey(ck[8])) &&
+                        box_contains(gtb, funkey(ck[9]), funkey(ck[10]), funkey(ck[11]));
+        if (!ok) {
+            if (lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);
+            continue;
+        }
+        warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, n, t.pair, lane);
+        if (lane == 0) {
+            atomicMax(&O.ctr->height, t.depth);
+            atomicAdd(&O.ctr->median_splits, 1u);
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {  // [0] gt, [1] lt, as the reference pushes them
+            const uint32_t len = c == 0 ? n - m : m;
+            const uint32_t start = c == 0 ? t.start + m : t.start;
+            const uint32_t slot = c == 0 ? t.pair : t.pair + 1u;
+            const uint32_t depth = t.depth + 1u;
+            float cb[6];
+#pragma unroll
+            for (int q = 0; q < 6; ++q) cb[q] = c == 0 ? gtb[q] : ltb[q];
+            if (child_is_leaf(len, depth, P)) {
+                warp_store_node(O, t.nbase + slot, cb, start - t.tbase, len, 0u, lane);
+                if (lane == 0 && len > 1) {
+                    atomicAdd(&O.ctr->holes, 1u);
+                    if (depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+                }
+                continue;
+            }
+            Task ct;
+            for (int a = 0; a < 3; ++a) {
+                ct.lo[a] = cb[a];
+                ct.hi[a] = cb[3 + a];
+            }
+            ct.start = start;
+            ct.len = len;
+            ct.slot = slot;
+            ct.pair = c == 0 ? t.pair + 2u : t.pair + 2u * (n - m);
+            ct.depth = depth;
+            ct.buf = t.buf ^ 1u;
+            ct.tile0 = ct.ntiles = 0;
+            ct.nbase = t.nbase;
+            ct.tbase = t.tbase;
+            if (len > P.medium_max) {
+                const uint32_t nt = (len + kTile - 1) / kTile;
+                uint32_t ti = 0, t0 = 0;
+                if (lane == 0) {
+                    ti = atomicAdd(&O.ctr->lvl[0][0], 1u);
+                    t0 = atomicAdd(&O.ctr->lvl[0][1], nt);
+                }
+                ti = __shfl_sync(kFull, ti, 0);
+                t0 = __shfl_sync(kFull, t0, 0);
+                if (ti >= M.cap_tasks || t0 + nt > M.cap_tiles) {
+                    if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                    continue;
+                }
+                ct.tile0 = t0;
+                ct.ntiles = nt;
+                if (lane == 0) M.tasks[ti] = ct;
+                init_task_bins(M.bins + (size_t)ti * kBinWords, lane, 32);
+                if (lane < 6) M.cbkeys[6 * ti + lane] = ck[(c == 0 ? 6 : 0) + lane];
+                for (uint32_t i = lane; i < nt; i += 32) {
+                    M.tile_task[t0 + i] = ti;
+                    M.tile_begin[t0 + i] = i * kTile;
+                }
+            } else {
+                const bool med = len > kSmallMax;
+                uint32_t li = 0;
+                if (lane == 0) li = atomicAdd(med ? &O.ctr->n_medium : &O.ctr->n_small, 1u);
+                li = __shfl_sync(kFull, li, 0);
+                if (li >= (med ? M.cap_medium : M.cap_small)) {
+                    if (lane == 0) set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+                    continue;
+                }
+                if (lane == 0) (med ? M.medium : M.small)[li] = ct;
+            }
+        }
     }
 }
 
@@ -2199,6 +2522,9 @@ struct mgbvh_ctx {
     DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
     DevBuf in_a, in_b, out_nodes, out_lens;
     DevBuf mesh_buf, toff_buf, noff_buf, mkeys;
+    // forced medians of level-pass nodes: the waiting list, its working copy,
+    // element offsets, per-node box keys, sort keys/values, flags and scan
+    DevBuf med_list, med_work, med_off, med_seg, med_keys[2], med_vals[2], med_flag, med_scan;
     void* pin = nullptr;  // pinned staging of a batch plan
     size_t pin_bytes = 0;
     bool graph_mode = false;
@@ -2310,9 +2636,7 @@ const char* site_text(uint32_t site) {
         case kSiteIndex: return "a triangle index is past the vertex count";
         case kSiteCount: return "partition count differs from the split's count (bvh/src/lib.rs:621-634)";
         case kSiteContain: return "a centroid lies outside its child's bounds (bvh/src/lib.rs:637-646)";
-        case kSiteLargeMedian:
-            return "forced median split on a node above 1024 objects is not built (no binned split "
-                   "passed the MIN_LEAF_OBJECTS filter)";
+        case kSiteMedian: return "forced median: a half's count differs from len / 2 (bvh/src/lib.rs:621-634)";
         case kSiteCapacity: return "internal task list overflow";
         case kSiteMeshIndex: return "an instance names a mesh past mesh_count";
         default: return "device error";
@@ -2384,6 +2708,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             A.refine = LN.w ? P_<LvlRefine>(ctx->lref) : nullptr;
             A.rbins = LN.w ? P_<uint32_t>(ctx->rbins) : nullptr;
             A.tile_hist2 = LN.w ? P_<uint32_t>(ctx->tile_hist2) : nullptr;
+            A.med = P_<Task>(ctx->med_list);
             lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
             if (LN.samples) {
                 lvl_sample_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(
@@ -2487,6 +2812,115 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     return MGBVH_OK;
 }
 
+// Forced medians of level-pass nodes (the median kernels above). The nodes
+// that lvl_eval_kernel queued during the pipeline are split here, then their
+// subtrees are built by another pipeline run, which may queue further nodes;
+// until none is left. The waiting subtrees are disjoint from everything the
+// pipeline built, and their node slots follow from the closed-form numbering,
+// so building them afterwards gives the same tree. The counters in
+// ctx->h_ctr are current on entry (the caller synchronized the stream) and on
+// return.
+int run_medians(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, Rec* rec0, Rec* rec1,
+                uint32_t n_objects, uint32_t& launches) {
+    const cudaStream_t sm = ctx->stream;
+    Counters* d_ctr = O.ctr;
+    // chunks streamed to the host during the pipeline miss the waiting
+    // subtrees: let them land, then the caller copies the whole array
+    if (ctx->streamed) {
+        MG_CUDA(cudaStreamSynchronize(ctx->cstream));
+        ctx->streamed = false;
+    }
+    struct Restore {  // the level-count hint and streaming belong to the main pipeline run
+        mgbvh_ctx* c;
+        uint32_t hint, slots;
+        ~Restore() {
+            c->levels_hint = hint;
+            c->stream_slots = slots;
+        }
+    } restore{ctx, ctx->levels_hint, ctx->stream_slots};
+    ctx->stream_slots = 0;
+    const int grid = ctx->sm_count * 8;
+    int rc;
+    while (!ctx->h_ctr->error && ctx->h_ctr->n_med) {
+        const uint32_t np = ctx->h_ctr->n_med;
+        if (np > C.tasks) return fail(ctx, MGBVH_ERR_CAPACITY, "internal task list overflow");
+        std::vector<Task> ht(np);
+        MG_CUDA(cudaMemcpyAsync(ht.data(), ctx->med_list.p, sizeof(Task) * np, cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        std::vector<uint32_t> off(np + 1);
+        uint64_t E = 0;
+        for (uint32_t i = 0; i < np; ++i) {
+            off[i] = static_cast<uint32_t>(E);
+            E += ht[i].len;
+        }
+        if (E > n_objects) return fail(ctx, MGBVH_ERR_ASSERT, "forced median: waiting nodes overlap");
+        off[np] = static_cast<uint32_t>(E);
+        if ((rc = ensure(ctx, ctx->med_work, sizeof(Task) * np)) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->med_off, 4ull * (np + 1))) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->med_seg, sizeof(MedSeg) * np)) != MGBVH_OK) return rc;
+        for (int i = 0; i < 2; ++i) {
+            if ((rc = ensure(ctx, ctx->med_keys[i], 8 * E)) != MGBVH_OK) return rc;
+            if ((rc = ensure(ctx, ctx->med_vals[i], 4 * E)) != MGBVH_OK) return rc;
+        }
+        if ((rc = ensure(ctx, ctx->med_flag, 4 * E)) != MGBVH_OK) return rc;
+        if ((rc = ensure(ctx, ctx->med_scan, 4 * E)) != MGBVH_OK) return rc;
+        const Task* mt = P_<Task>(ctx->med_work);
+        const uint32_t* moff = P_<uint32_t>(ctx->med_off);
+        MedSeg* seg = P_<MedSeg>(ctx->med_seg);
+        unsigned long long* k0 = P_<unsigned long long>(ctx->med_keys[0]);
+        unsigned long long* k1 = P_<unsigned long long>(ctx->med_keys[1]);
+        uint32_t* v0 = P_<uint32_t>(ctx->med_vals[0]);
+        uint32_t* v1 = P_<uint32_t>(ctx->med_vals[1]);
+        uint32_t* flag = P_<uint32_t>(ctx->med_flag);
+        uint32_t* scan = P_<uint32_t>(ctx->med_scan);
+        const uint32_t e32 = static_cast<uint32_t>(E);
+        MG_CUDA(cudaMemcpyAsync(ctx->med_off.p, off.data(), 4ull * (np + 1), cudaMemcpyHostToDevice, sm));
+        MG_CUDA(cudaMemcpyAsync(ctx->med_work.p, ctx->med_list.p, sizeof(Task) * np, cudaMemcpyDeviceToDevice, sm));
+        med_reset_kernel<<<1, 32, 0, sm>>>(d_ctr);
+        med_init_kernel<<<std::min<uint32_t>((np * 48u + 255u) / 256u, 1024u), 256, 0, sm>>>(seg, np);
+        const int end_bit = 32 + (np > 1 ? 32 - __builtin_clz(np - 1) : 0);
+        const int eg = (int)std::min<uint64_t>((E + 255) / 256, (uint64_t)grid);
+        for (uint32_t axis = 0; axis < 3; ++axis) {
+            med_key_kernel<<<eg, 256, 0, sm>>>(mt, moff, np, e32, rec0, rec1, axis, k0, v0);
+            size_t tb = 0, ts = 0;
+            MG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, (int)e32, 0, end_bit, sm));
+            MG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, ts, flag, scan, (int)e32, sm));
+            if ((rc = ensure(ctx, ctx->cub_tmp, std::max(tb, ts))) != MGBVH_OK) return rc;
+            tb = ts = ctx->cub_tmp.bytes;
+            MG_CUDA(cub::DeviceRadixSort::SortPairs(ctx->cub_tmp.p, tb, k0, k1, v0, v1, (int)e32, 0, end_bit, sm));
+            med_flag_kernel<<<eg, 256, 0, sm>>>(mt, moff, np, e32, k0, k1, v1, flag);
+            MG_CUDA(cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, ts, flag, scan, (int)e32, sm));
+            med_scatter_kernel<<<eg, 256, 0, sm>>>(mt, moff, np, e32, rec0, rec1, axis, flag, scan, seg, P, O);
+            launches += 5;
+        }
+        MedOut M;
+        M.tasks = P_<Task>(ctx->tasks[0]);
+        M.bins = P_<uint32_t>(ctx->bins[0]);
+        M.cbkeys = P_<uint32_t>(ctx->cbkeys[0]);
+        M.tile_task = P_<uint32_t>(ctx->tile_task[0]);
+        M.tile_begin = P_<uint32_t>(ctx->tile_begin[0]);
+        M.medium = P_<Task>(ctx->medium);
+        M.small = P_<Task>(ctx->small);
+        M.cap_tasks = C.tasks;
+        M.cap_tiles = C.tiles;
+        M.cap_medium = C.medium;
+        M.cap_small = C.small;
+        med_finish_kernel<<<std::min<uint32_t>((np + 3) / 4, 1024u), 128, 0, sm>>>(mt, np, seg, M, P, O);
+        launches += 3;
+        MG_CUDA(cudaGetLastError());
+        MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+        if (ctx->h_ctr->error) break;
+        uint32_t levels = 0;
+        if ((rc = run_pipeline(ctx, C, P, O, rec0, rec1, ctx->h_ctr->lvl[0][0] > 0, 0, launches, levels)) !=
+            MGBVH_OK)
+            return rc;
+        MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+    }
+    return MGBVH_OK;
+}
+
 // Runs a build whose inputs are device-resident. Outputs go to device memory:
 // d_nodes (capacity cap), d_lens (nullable), d_perm. Returns status.
 int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_node* d_nodes,
@@ -2511,6 +2945,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     ENS(ctx->tile_hist, 4ull * 96 * C.tiles);  // [axis][bin][tile]
     ENS(ctx->tile_lt, 4ull * C.tiles);
     ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
+    ENS(ctx->med_list, sizeof(Task) * (size_t)C.tasks);
     ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
     ENS(ctx->small, sizeof(Task) * (size_t)C.small);
     ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
@@ -2591,13 +3026,19 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     MG_CUDA(cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(Counters), cudaMemcpyDeviceToHost, sm));
     MG_CUDA(cudaStreamSynchronize(sm));
-    const Counters hc = *ctx->h_ctr;
-    if (optimistic && hc.lvl[levels & 1u][0] != 0) {
+    if (optimistic && ctx->h_ctr->lvl[levels & 1u][0] != 0) {
         // the tree needs more level passes than the hint: build again, reading
         // the task count after every batch of levels
         ctx->levels_hint = 0;
         return run_build(ctx, in, st, d_nodes, cap, d_lens, d_perm, out_count, stats);
     }
+    if (!ctx->h_ctr->error && ctx->h_ctr->n_med) {
+        // level-pass nodes that need the forced median
+        if ((rc = run_medians(ctx, C, P, O, rec0, rec1, n, launches)) != MGBVH_OK) return rc;
+        MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+        MG_CUDA(cudaStreamSynchronize(sm));
+    }
+    const Counters hc = *ctx->h_ctr;
     if (hc.error) {
         return fail(ctx, (int)hc.error, site_text(hc.error_site));
     }
@@ -2893,6 +3334,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     ENS(ctx->tile_hist, 4ull * 96 * C.tiles);
     ENS(ctx->tile_lt, 4ull * C.tiles);
     ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
+    ENS(ctx->med_list, sizeof(Task) * (size_t)C.tasks);
     ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
     ENS(ctx->small, sizeof(Task) * (size_t)C.small);
     ENS(ctx->nodes, sizeof(mgbvh_node) * (size_t)C.nodes);
@@ -2959,14 +3401,16 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     uint32_t launches = 0, levels = 0;
     bool done = false;
     bool from_graph = false;
+    bool had_medians = false;
     if (ctx->graph_mode && same_signature(ctx, sig)) {
         MG_CUDA(cudaEventRecord(ctx->ev0, sm));
         MG_CUDA(cudaGraphLaunch(ctx->graph_exec, sm));
         MG_CUDA(cudaEventRecord(ctx->ev1, sm));
         MG_CUDA(cudaStreamSynchronize(sm));
         const Counters& hc = *ctx->h_ctr;
-        // the spare level must have found nothing to do
-        if (!hc.error && hc.lvl[ctx->graph_levels & 1u][0] == 0) {
+        // the spare level must have found nothing to do, and no node may wait
+        // for a forced median (the graph holds no median passes)
+        if (!hc.error && hc.lvl[ctx->graph_levels & 1u][0] == 0 && hc.n_med == 0) {
             done = true;
             from_graph = true;
             launches = ctx->graph_launches;
@@ -2978,6 +3422,23 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
                                 cap >= B.slots)) != MGBVH_OK)
             return rc;
         MG_CUDA(cudaStreamSynchronize(sm));
+        if (!ctx->h_ctr->error && ctx->h_ctr->n_med) {
+            // level-pass nodes that need the forced median
+            had_medians = true;
+            const bool dir = cap >= B.slots;
+            Out O;
+            O.nodes = dir ? d_nodes : P_<mgbvh_node>(ctx->nodes);
+            O.lens = (dir && d_lens) ? d_lens : P_<uint32_t>(ctx->lens);
+            O.used = P_<uint8_t>(ctx->used);
+            O.perm = d_perm;
+            O.ctr = P_<Counters>(ctx->ctr);
+            O.node_cap = C.nodes;
+            if ((rc = run_medians(ctx, C, params_of(ctx, st), O, P_<Rec>(ctx->rec[0]), P_<Rec>(ctx->rec[1]), n,
+                                  launches)) != MGBVH_OK)
+                return rc;
+            MG_CUDA(cudaEventRecord(ctx->ev1, sm));
+            MG_CUDA(cudaStreamSynchronize(sm));
+        }
     }
     const Counters hc = *ctx->h_ctr;
     if (hc.error) return fail(ctx, (int)hc.error, site_text(hc.error_site));
@@ -3032,7 +3493,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     }
     MG_CUDA(cudaStreamSynchronize(sm));
     // capture a graph for the next build of this mesh set
-    if (ctx->graph_mode && !from_graph && hc.holes == 0 && cap >= B.slots) {
+    if (ctx->graph_mode && !from_graph && !had_medians && hc.holes == 0 && cap >= B.slots) {
         if (ctx->graph_exec) {
             cudaGraphExecDestroy(ctx->graph_exec);
             ctx->graph_exec = nullptr;
@@ -3283,7 +3744,9 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->used, &ctx->newidx, &ctx->widened, &ctx->perm, &ctx->ctr, &ctx->cub_tmp, &ctx->in_a,
                      &ctx->in_b, &ctx->out_nodes, &ctx->out_lens, &ctx->mesh_buf,
                      &ctx->toff_buf, &ctx->noff_buf, &ctx->mkeys, &ctx->learn_wt, &ctx->lref,
-                     &ctx->rbins, &ctx->tile_hist2};
+                     &ctx->rbins, &ctx->tile_hist2, &ctx->med_list, &ctx->med_work, &ctx->med_off,
+                     &ctx->med_seg, &ctx->med_keys[0], &ctx->med_keys[1], &ctx->med_vals[0],
+                     &ctx->med_vals[1], &ctx->med_flag, &ctx->med_scan};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
@@ -3519,15 +3982,11 @@ double mgbvh_sah_cost(const mgbvh_node* nodes, const uint32_t* lens, uint32_t co
 }
 
 
-// Allocation-free build (see include/mgbvh.h). Per-device set-up, done by the
-// first call on each device: the scratch array's device address and the
-// medium kernel's shared-memory limit.
-namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
-int g_noalloc_sms[64] = {};
-}  // namespace
-
+// Allocation-free build (see include/mgbvh.h). Every call looks up, for the
+// current device and context, the scratch array's device address
+// (cudaGetSymbolAddress allocates nothing), the medium kernel's shared-memory
+// limit and the SM count: nothing is cached, so a call after a device reset
+// never launches on an address of a context that is gone.
 int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_settings* settings,
                               mgbvh_node* d_out_nodes, uint32_t node_capacity,
                               uint32_t* out_node_count, uint32_t* d_out_lens, uint32_t* d_out_perm,
@@ -3540,26 +3999,15 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
     if (count > kNoAllocMax) return MGBVH_ERR_TOO_LARGE;
     if (!d_aabbs || !d_out_nodes || !d_out_perm) return MGBVH_ERR_INVALID_ARG;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return MGBVH_ERR_NO_DEVICE;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return MGBVH_ERR_NO_DEVICE;
     void* addr = nullptr;
     int sms = 0;
-    {
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_addr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return MGBVH_ERR_CUDA;
-            if (cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(MediumSmem)) != cudaSuccess)
-                return MGBVH_ERR_CUDA;
-            int n_sm = 0;
-            if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-                return MGBVH_ERR_CUDA;
-            g_noalloc_addr[dev] = p;
-            g_noalloc_sms[dev] = n_sm;
-        }
-        addr = g_noalloc_addr[dev];
-        sms = g_noalloc_sms[dev];
-    }
+    if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return MGBVH_ERR_CUDA;
+    if (cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(MediumSmem)) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
+        return MGBVH_ERR_CUDA;
     NoAllocScratch* S = reinterpret_cast<NoAllocScratch*>(addr);
     const cudaStream_t sm = reinterpret_cast<cudaStream_t>(cuda_stream);
     const mgbvh_settings* st = settings;

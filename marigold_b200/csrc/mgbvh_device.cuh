@@ -59,7 +59,7 @@ struct Counters {
     uint32_t n_small;
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
     uint32_t learned;        // nodes where a proposal of the split network replaced the binned split
-    uint32_t pad_;
+    uint32_t n_med;          // level-pass nodes waiting for a forced median split (the median passes)
     // streamed output (slot chunks): subtrees of 33..medium_max objects per
     // chunk, their placement cursors and sorted ranges; subtrees of <= 32
     // objects selected so far, the sorted range of each chunk's, and the CTAs
@@ -77,7 +77,7 @@ enum ErrorSite : uint32_t {
     kSiteIndex = 1,        // a triangle index past the vertex count
     kSiteCount = 2,        // partition count differs from the split's count
     kSiteContain = 3,      // a centroid outside its child's bounds
-    kSiteLargeMedian = 4,  // forced median on a node above the CTA size with distinct keys
+    kSiteMedian = 4,       // forced median of a level-pass node: counts of its halves differ
     kSiteCapacity = 5,
     kSiteMeshIndex = 6,  // an instance names a mesh past the mesh count
 };

@@ -33,6 +33,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/mgbvh.h"
 
@@ -906,6 +907,292 @@ __global__ void ray_key_kernel(const float4* __restrict__ rays, uint32_t n, cons
     }
 }
 
+// ---------------------------------------------------------------- two-level scenes
+//
+// The reference's scene traversal (scene.slang:91-141 raytraceTlas, :143-220
+// raytraceBlas): the TLAS is walked with the world ray; at a TLAS leaf the
+// ray moves into the instance's mesh space through its inverse transform
+// (:161-164) and that mesh's BLAS is walked from its root (:172), on the same
+// stack. The hit distance stays the world ray's parameter: the mesh-space ray
+// o' = M o, d' = M d (d' not normalized) reaches M p at the same t as the
+// world ray reaches p, so distances compare across instances as they are
+// (the shader's rescaling by |d'|, :168-169, is wrong for scaled instances
+// and is not copied). Equal distances resolve to the lowest (instance,
+// triangle) pair, and TLAS boxes are tested grown by a relative 1e-5 (they
+// come from f32 corner transforms, which can round a hair inside the exact
+// transformed mesh), so the traversal finds exactly the brute-force hits.
+
+struct SceneMesh {  // mgbvh_scene_mesh
+    uint32_t blas_root, tri_offset, tri_count, vertex_offset;
+};
+
+struct SceneInst {  // mgbvh_scene_instance
+    float m[16];  // column-major world -> mesh
+    uint32_t mesh, pad[3];
+};
+
+constexpr int kSceneStack = 96;  // a TLAS path and a BLAS path of up to 47 levels each
+
+// Column-major M * (x, y, z, w), each component ((c0 x + c1 y) + c2 z) + c3 w
+// with every product and sum rounded (glam's f32 Mat4 * Vec4 order).
+__device__ __forceinline__ void xform(const float* m, float x, float y, float z, float w, float& ox, float& oy,
+                                      float& oz) {
+    ox = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[0], x), __fmul_rn(m[4], y)), __fmul_rn(m[8], z)),
+                   __fmul_rn(m[12], w));
+    oy = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[1], x), __fmul_rn(m[5], y)), __fmul_rn(m[9], z)),
+                   __fmul_rn(m[13], w));
+    oz = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(m[2], x), __fmul_rn(m[6], y)), __fmul_rn(m[10], z)),
+                   __fmul_rn(m[14], w));
+}
+
+__device__ __forceinline__ float4 grow_lo(float4 v) {
+    return make_float4(v.x - fabsf(v.x) * 1e-5f - 1e-30f, v.y - fabsf(v.y) * 1e-5f - 1e-30f,
+                       v.z - fabsf(v.z) * 1e-5f - 1e-30f, v.w);
+}
+__device__ __forceinline__ float4 grow_hi(float4 v) {
+    return make_float4(v.x + fabsf(v.x) * 1e-5f + 1e-30f, v.y + fabsf(v.y) * 1e-5f + 1e-30f,
+                       v.z + fabsf(v.z) * 1e-5f + 1e-30f, v.w);
+}
+
+// (t, instance, triangle) strictly before the current best.
+__device__ __forceinline__ bool scene_better(float tt, uint32_t inst, uint32_t tri, float best, uint32_t bi,
+                                             uint32_t bp) {
+    return tt < best || (tt == best && (inst < bi || (inst == bi && tri < bp)));
+}
+
+template <bool kTlasLens, bool kBlasLens>
+__global__ void __launch_bounds__(128) trace_scene_kernel(
+    const float4* __restrict__ tlas, const uint32_t* __restrict__ tlas_lens, const SceneInst* __restrict__ inst,
+    uint32_t n_inst, const SceneMesh* __restrict__ meshes, uint32_t n_meshes, const float4* __restrict__ blas,
+    const uint32_t* __restrict__ blas_lens, const TriRec* __restrict__ tris, const float4* __restrict__ rays,
+    uint32_t n_rays, float* __restrict__ hit_t, uint32_t* __restrict__ hit_inst, uint32_t* __restrict__ hit_tri,
+    Counts* counts, int* err, const uint32_t* __restrict__ order) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c_nodes = 0, c_boxes = 0, c_tris = 0;
+    if (j < n_rays) {
+        const uint32_t i = order ? order[j] : j;
+        const float4 o = rays[2 * i], d = rays[2 * i + 1];
+        const float ix = __fdiv_rn(1.0f, d.x), iy = __fdiv_rn(1.0f, d.y), iz = __fdiv_rn(1.0f, d.z);
+        float best = __int_as_float(0x7F800000);
+        uint32_t bi = kNoHit, bp = kNoHit;
+        uint32_t stack[kSceneStack];
+        int sp = 0;
+        c_boxes++;
+        if (box_entry(o.x, o.y, o.z, ix, iy, iz, grow_lo(tlas[0]), grow_hi(tlas[1]), best) <= best) stack[sp++] = 0;
+        while (sp > 0) {
+            const uint32_t ni = stack[--sp];
+            c_nodes++;
+            const float4 nhi = tlas[2 * ni + 1];
+            const uint32_t child = __float_as_uint(nhi.w);
+            if (child != 0) {
+                c_boxes += 2;
+                const float da = box_entry(o.x, o.y, o.z, ix, iy, iz, grow_lo(tlas[2 * child]),
+                                           grow_hi(tlas[2 * child + 1]), best);
+                const float db = box_entry(o.x, o.y, o.z, ix, iy, iz, grow_lo(tlas[2 * child + 2]),
+                                           grow_hi(tlas[2 * child + 3]), best);
+                const bool pa = da <= best, pb = db <= best;
+                if (sp + 2 > kSceneStack) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                if (pa && pb) {
+                    const bool a_first = da < db;
+                    stack[sp++] = a_first ? child + 1 : child;
+                    stack[sp++] = a_first ? child : child + 1;
+                } else if (pa || pb) {
+                    stack[sp++] = pa ? child : child + 1;
+                }
+                continue;
+            }
+            const uint32_t start = __float_as_uint(tlas[2 * ni].w);
+            const uint32_t len = kTlasLens ? tlas_lens[ni] : 1u;
+            for (uint32_t k = start; k < start + len; ++k) {
+                if (k >= n_inst || inst[k].mesh >= n_meshes) {
+                    atomicExch(err, 2);
+                    continue;
+                }
+                const SceneInst& I = inst[k];
+                const SceneMesh M = meshes[I.mesh];
+                if (M.tri_count == 0) continue;  // an empty mesh: no BLAS
+                float lox, loy, loz, ldx, ldy, ldz;
+                xform(I.m, o.x, o.y, o.z, 1.0f, lox, loy, loz);
+                xform(I.m, d.x, d.y, d.z, 0.0f, ldx, ldy, ldz);
+                const float lix = __fdiv_rn(1.0f, ldx), liy = __fdiv_rn(1.0f, ldy), liz = __fdiv_rn(1.0f, ldz);
+                const float4* bn = blas + 2 * (size_t)M.blas_root;
+                const uint32_t* bl = kBlasLens ? blas_lens + M.blas_root : nullptr;
+                // the mesh's BLAS on the same stack, from its root (scene.slang:171-173)
+                const int base = sp;
+                if (sp + 1 > kSceneStack) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                stack[sp++] = 0;
+                while (sp > base) {
+                    const uint32_t bi_ = stack[--sp];
+                    c_nodes++;
+                    const uint32_t bchild = __float_as_uint(bn[2 * bi_ + 1].w);
+                    if (bchild != 0) {
+                        c_boxes += 2;
+                        const float da = box_entry(lox, loy, loz, lix, liy, liz, bn[2 * bchild], bn[2 * bchild + 1], best);
+                        const float db =
+                            box_entry(lox, loy, loz, lix, liy, liz, bn[2 * bchild + 2], bn[2 * bchild + 3], best);
+                        const bool pa = da <= best, pb = db <= best;
+                        if (sp + 2 > kSceneStack) {
+                            atomicExch(err, 1);
+                            sp = base;
+                            break;
+                        }
+                        if (pa && pb) {
+                            const bool a_first = da < db;
+                            stack[sp++] = a_first ? bchild + 1 : bchild;
+                            stack[sp++] = a_first ? bchild : bchild + 1;
+                        } else if (pa || pb) {
+                            stack[sp++] = pa ? bchild : bchild + 1;
+                        }
+                    } else {
+                        const uint32_t s0 = __float_as_uint(bn[2 * bi_].w);
+                        const uint32_t n0 = kBlasLens ? bl[bi_] : 1u;
+                        for (uint32_t q = s0; q < s0 + n0 && q < M.tri_count; ++q) {
+                            const uint32_t tri = M.tri_offset + q;
+                            c_tris++;
+                            const float tt = intersect_tri(lox, loy, loz, ldx, ldy, ldz, tris[tri]);
+                            if (tt >= 0.0f && scene_better(tt, k, tri, best, bi, bp)) {
+                                best = tt;
+                                bi = k;
+                                bp = tri;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        hit_t[i] = bp == kNoHit ? -1.0f : best;
+        hit_inst[i] = bi;
+        hit_tri[i] = bp;
+    }
+    if (counts) {
+        unsigned long long a = c_nodes, b = c_boxes, c = c_tris;
+        for (int off = 16; off > 0; off >>= 1) {
+            a += __shfl_down_sync(kFull, a, off);
+            b += __shfl_down_sync(kFull, b, off);
+            c += __shfl_down_sync(kFull, c, off);
+        }
+        if ((threadIdx.x & 31u) == 0) {
+            atomicAdd(&counts->nodes, a);
+            atomicAdd(&counts->boxes, b);
+            atomicAdd(&counts->tris, c);
+        }
+    }
+}
+
+// Brute force over a scene: one CTA per ray; for every instance the ray in
+// mesh space, then every triangle of the mesh (threads split the triangles).
+// cull != 0 skips an instance whose mesh-space ray misses the mesh's BLAS
+// root box grown by a relative 1e-4 (a filter far wider than any rounding;
+// it keeps large scenes affordable).
+constexpr int kBruteThreads = 256;
+
+__global__ void __launch_bounds__(kBruteThreads) brute_scene_kernel(
+    const SceneInst* __restrict__ inst, uint32_t n_inst, const SceneMesh* __restrict__ meshes, uint32_t n_meshes,
+    const float4* __restrict__ blas, const TriRec* __restrict__ tris, const float4* __restrict__ rays,
+    uint32_t n_rays, float* __restrict__ hit_t, uint32_t* __restrict__ hit_inst, uint32_t* __restrict__ hit_tri,
+    int cull) {
+    __shared__ float st[kBruteThreads];
+    __shared__ uint32_t si[kBruteThreads], sp[kBruteThreads];
+    for (uint32_t r = blockIdx.x; r < n_rays; r += gridDim.x) {
+        const float4 o = rays[2 * r], d = rays[2 * r + 1];
+        float best = __int_as_float(0x7F800000);
+        uint32_t bi = kNoHit, bp = kNoHit;
+        for (uint32_t k = 0; k < n_inst; ++k) {
+            const SceneInst& I = inst[k];
+            if (I.mesh >= n_meshes) continue;
+            const SceneMesh M = meshes[I.mesh];
+            if (M.tri_count == 0) continue;
+            float lox, loy, loz, ldx, ldy, ldz;
+            xform(I.m, o.x, o.y, o.z, 1.0f, lox, loy, loz);
+            xform(I.m, d.x, d.y, d.z, 0.0f, ldx, ldy, ldz);
+            if (cull) {
+                float4 lo = blas[2 * (size_t)M.blas_root], hi = blas[2 * (size_t)M.blas_root + 1];
+                const float gx = (fabsf(lo.x) + fabsf(hi.x)) * 1e-4f + 1e-30f;
+                const float gy = (fabsf(lo.y) + fabsf(hi.y)) * 1e-4f + 1e-30f;
+                const float gz = (fabsf(lo.z) + fabsf(hi.z)) * 1e-4f + 1e-30f;
+                lo = make_float4(lo.x - gx, lo.y - gy, lo.z - gz, 0.f);
+                hi = make_float4(hi.x + gx, hi.y + gy, hi.z + gz, 0.f);
+                const float lix = __fdiv_rn(1.0f, ldx), liy = __fdiv_rn(1.0f, ldy), liz = __fdiv_rn(1.0f, ldz);
+                if (!(box_entry(lox, loy, loz, lix, liy, liz, lo, hi, __int_as_float(0x7F800000)) >= 0.0f))
+                    continue;  // block-uniform
+            }
+            for (uint32_t q = threadIdx.x; q < M.tri_count; q += blockDim.x) {
+                const uint32_t tri = M.tri_offset + q;
+                const float tt = intersect_tri(lox, loy, loz, ldx, ldy, ldz, tris[tri]);
+                if (tt >= 0.0f && scene_better(tt, k, tri, best, bi, bp)) {
+                    best = tt;
+                    bi = k;
+                    bp = tri;
+                }
+            }
+        }
+        st[threadIdx.x] = best;
+        si[threadIdx.x] = bi;
+        sp[threadIdx.x] = bp;
+        __syncthreads();
+        for (int s = kBruteThreads / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < (uint32_t)s) {
+                const uint32_t o2 = threadIdx.x + s;
+                if (sp[o2] != kNoHit &&
+                    (sp[threadIdx.x] == kNoHit || scene_better(st[o2], si[o2], sp[o2], st[threadIdx.x],
+                                                               si[threadIdx.x], sp[threadIdx.x]))) {
+                    st[threadIdx.x] = st[o2];
+                    si[threadIdx.x] = si[o2];
+                    sp[threadIdx.x] = sp[o2];
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            hit_t[r] = sp[0] == kNoHit ? -1.0f : st[0];
+            hit_inst[r] = si[0];
+            hit_tri[r] = sp[0];
+        }
+        __syncthreads();
+    }
+}
+
+// The scene's triangles with their vertices, mesh by mesh (blockIdx.y):
+// TriRec k holds triangle k of the scene array (indices relative to its
+// mesh's vertex offset), id = k.
+__global__ void gather_scene_kernel(const float* __restrict__ verts, uint32_t stride_floats, uint32_t nverts,
+                                    const uint32_t* __restrict__ tris, uint32_t n_tris,
+                                    const SceneMesh* __restrict__ meshes, TriRec* __restrict__ out, int* err) {
+    const SceneMesh M = meshes[blockIdx.y];
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < M.tri_count; q += gridDim.x * blockDim.x) {
+        const uint32_t k = M.tri_offset + q;
+        if (k >= n_tris) {
+            atomicExch(err, 2);
+            continue;
+        }
+        uint32_t v[3];
+        bool bad = false;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            v[c] = tris[3 * (size_t)k + c] + M.vertex_offset;
+            bad |= v[c] >= nverts || v[c] < M.vertex_offset;
+        }
+        if (bad) {
+            atomicExch(err, 2);
+            continue;
+        }
+        const float* a = verts + (size_t)v[0] * stride_floats;
+        const float* b = verts + (size_t)v[1] * stride_floats;
+        const float* c = verts + (size_t)v[2] * stride_floats;
+        TriRec r;
+        r.a = make_float4(a[0], a[1], a[2], __uint_as_float(k));
+        r.b = make_float4(b[0], b[1], b[2], 0.0f);
+        r.c = make_float4(c[0], c[1], c[2], 0.0f);
+        out[k] = r;
+    }
+}
+
 }  // namespace mgbvh_trace
 
 using namespace mgbvh_trace;
@@ -937,6 +1224,18 @@ struct mgbvh_tracer {
     size_t ray_cap = 0;
     void* sort_tmp = nullptr;
     size_t sort_tmp_bytes = 0;
+    // a two-level scene (mgbvh_tracer_set_scene_dev): the caller's TLAS,
+    // instances and BLAS nodes (kept as pointers), the mesh table (copied)
+    bool scene = false;
+    const mgbvh_node* tlas = nullptr;
+    const uint32_t* tlas_lens = nullptr;
+    const SceneInst* inst = nullptr;
+    uint32_t n_inst = 0;
+    SceneMesh* meshes = nullptr;
+    size_t meshes_cap = 0;
+    uint32_t n_meshes = 0;
+    const mgbvh_node* blas = nullptr;
+    const uint32_t* blas_lens = nullptr;
 };
 
 namespace {
@@ -973,9 +1272,10 @@ int ensure_order_buffers(mgbvh_tracer* t, uint32_t n) {
 // Enqueues the tracing order of the rays on stream sm: keys (ray_key_kernel
 // mode), then a radix sort of (key, ray index); returns the sorted ray
 // indices, or nullptr (rays traced as given).
-const uint32_t* ray_order(mgbvh_tracer* t, const float4* rays, uint32_t n, cudaStream_t sm, uint32_t mode) {
+const uint32_t* ray_order(mgbvh_tracer* t, const float4* rays, uint32_t n, cudaStream_t sm, uint32_t mode,
+                          const mgbvh_node* root = nullptr) {
     if (mode == 0) return nullptr;
-    ray_key_kernel<<<1184, 256, 0, sm>>>(rays, n, reinterpret_cast<const float4*>(t->nodes), mode,
+    ray_key_kernel<<<1184, 256, 0, sm>>>(rays, n, reinterpret_cast<const float4*>(root ? root : t->nodes), mode,
                                          t->rkey[0], t->ridx[0]);
     cub::DoubleBuffer<uint32_t> kb(t->rkey[0], t->rkey[1]), vb(t->ridx[0], t->ridx[1]);
     size_t bytes = t->sort_tmp_bytes;
@@ -1030,6 +1330,7 @@ void mgbvh_tracer_destroy(mgbvh_tracer* t) {
         if (t->ridx[k]) cudaFree(t->ridx[k]);
     }
     if (t->sort_tmp) cudaFree(t->sort_tmp);
+    if (t->meshes) cudaFree(t->meshes);
     if (t->ev0) cudaEventDestroy(t->ev0);
     if (t->ev1) cudaEventDestroy(t->ev1);
     delete t;
@@ -1067,6 +1368,7 @@ int mgbvh_tracer_set_blas_dev(mgbvh_tracer* t, const mgbvh_node* d_nodes, uint32
     t->node_count = node_count;
     t->n_tris = triangle_count;
     t->wide_count = 0;  // a wide BVH of an earlier tree no longer applies
+    t->scene = false;
     return MGBVH_OK;
 }
 
@@ -1242,6 +1544,150 @@ int mgbvh_trace_bruteforce_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_
     brute_kernel<<<(n_rays + 255) / 256, 256, 0, sm>>>(t->tris, t->n_tris,
                                                         reinterpret_cast<const float4*>(d_rays), n_rays,
                                                         d_hit_t, d_hit_prim);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    return trace_check(cudaStreamSynchronize(sm));
+}
+
+int mgbvh_tracer_set_scene_dev(mgbvh_tracer* t, const mgbvh_node* d_tlas_nodes, uint32_t tlas_node_count,
+                               const uint32_t* d_tlas_lens, const mgbvh_scene_instance* d_instances,
+                               uint32_t instance_count, const mgbvh_scene_mesh* d_meshes, uint32_t mesh_count,
+                               const mgbvh_node* d_blas_nodes, uint32_t blas_node_count,
+                               const uint32_t* d_blas_lens, const float* d_vertices, uint32_t vertex_stride_bytes,
+                               uint32_t vertex_count, const uint32_t* d_triangles, uint32_t triangle_count,
+                               void* stream) {
+    static_assert(sizeof(mgbvh_scene_mesh) == sizeof(SceneMesh), "mesh record layout");
+    static_assert(sizeof(mgbvh_scene_instance) == sizeof(SceneInst), "instance record layout");
+    if (!t || !d_tlas_nodes || tlas_node_count == 0 || !d_instances || instance_count == 0 || !d_meshes ||
+        mesh_count == 0 || mesh_count > 65535 || !d_blas_nodes || blas_node_count == 0 || !d_vertices ||
+        !d_triangles || triangle_count == 0 || vertex_stride_bytes < 12 || vertex_stride_bytes % 4)
+        return MGBVH_ERR_INVALID_ARG;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    // the mesh table: checked on the host, copied into the tracer
+    std::vector<mgbvh_scene_mesh> hm(mesh_count);
+    if (cudaMemcpyAsync(hm.data(), d_meshes, sizeof(mgbvh_scene_mesh) * mesh_count, cudaMemcpyDeviceToHost, sm) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    uint32_t max_count = 0;
+    for (const mgbvh_scene_mesh& m : hm) {
+        if (m.triangle_count == 0) continue;  // an empty mesh has no BLAS; its instances hit nothing
+        if ((uint64_t)m.triangle_offset + m.triangle_count > triangle_count || m.blas_root >= blas_node_count)
+            return MGBVH_ERR_INVALID_ARG;
+        max_count = std::max(max_count, m.triangle_count);
+    }
+    const size_t need = sizeof(TriRec) * (size_t)triangle_count;
+    if (t->tris_cap < need) {
+        if (t->tris) cudaFree(t->tris);
+        t->tris = nullptr;
+        t->tris_cap = 0;
+        if (cudaMalloc(&t->tris, need) != cudaSuccess) return MGBVH_ERR_CUDA;
+        t->tris_cap = need;
+    }
+    if (t->meshes_cap < mesh_count) {
+        if (t->meshes) cudaFree(t->meshes);
+        t->meshes = nullptr;
+        t->meshes_cap = 0;
+        if (cudaMalloc(&t->meshes, sizeof(SceneMesh) * mesh_count) != cudaSuccess) return MGBVH_ERR_CUDA;
+        t->meshes_cap = mesh_count;
+    }
+    if (cudaMemcpyAsync(t->meshes, hm.data(), sizeof(SceneMesh) * mesh_count, cudaMemcpyHostToDevice, sm) !=
+            cudaSuccess ||
+        cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    const dim3 grid(std::max(1u, std::min((max_count + 255) / 256, 64u)), mesh_count);
+    gather_scene_kernel<<<grid, 256, 0, sm>>>(d_vertices, vertex_stride_bytes / 4, vertex_count, d_triangles,
+                                              triangle_count, t->meshes, t->tris, t->d_err);
+    int herr = 0;
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (herr) return MGBVH_ERR_INVALID_ARG;
+    t->scene = true;
+    t->tlas = d_tlas_nodes;
+    t->tlas_lens = d_tlas_lens;
+    t->inst = reinterpret_cast<const SceneInst*>(d_instances);
+    t->n_inst = instance_count;
+    t->n_meshes = mesh_count;
+    t->blas = d_blas_nodes;
+    t->blas_lens = d_blas_lens;
+    t->n_tris = triangle_count;
+    // the one-level traversal and the wide tree no longer apply
+    t->nodes = nullptr;
+    t->lens = nullptr;
+    t->node_count = 0;
+    t->wide_count = 0;
+    return MGBVH_OK;
+}
+
+int mgbvh_trace_scene_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_rays, float* d_hit_t,
+                          uint32_t* d_hit_instance, uint32_t* d_hit_triangle, uint64_t* out_counts,
+                          double* out_seconds, void* stream) {
+    if (!t || !t->scene || (n_rays && (!d_rays || !d_hit_t || !d_hit_instance || !d_hit_triangle)))
+        return MGBVH_ERR_INVALID_ARG;
+    if (n_rays == 0) return MGBVH_OK;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(t->d_counts, 0, sizeof(Counts), sm) != cudaSuccess ||
+        cudaMemsetAsync(t->d_err, 0, sizeof(int), sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (int rc = ensure_order_buffers(t, n_rays)) return rc;
+    cudaEventRecord(t->ev0, sm);
+    const float4* rays = reinterpret_cast<const float4*>(d_rays);
+    const uint32_t* order = ray_order(t, rays, n_rays, sm, MGBVH_RAY_SORT_BINARY, t->tlas);
+    Counts* cnt = out_counts ? t->d_counts : nullptr;
+    const uint32_t grid = (n_rays + 127) / 128;
+    const float4* tl = reinterpret_cast<const float4*>(t->tlas);
+    const float4* bl = reinterpret_cast<const float4*>(t->blas);
+    auto launch = [&](auto kern) {
+        kern<<<grid, 128, 0, sm>>>(tl, t->tlas_lens, t->inst, t->n_inst, t->meshes, t->n_meshes, bl, t->blas_lens,
+                                   t->tris, rays, n_rays, d_hit_t, d_hit_instance, d_hit_triangle, cnt, t->d_err,
+                                   order);
+    };
+    if (t->tlas_lens && t->blas_lens)
+        launch(trace_scene_kernel<true, true>);
+    else if (t->tlas_lens)
+        launch(trace_scene_kernel<true, false>);
+    else if (t->blas_lens)
+        launch(trace_scene_kernel<false, true>);
+    else
+        launch(trace_scene_kernel<false, false>);
+    cudaEventRecord(t->ev1, sm);
+    if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
+    Counts hc;
+    int herr = 0;
+    if (cudaMemcpyAsync(&hc, t->d_counts, sizeof(Counts), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaMemcpyAsync(&herr, t->d_err, sizeof(int), cudaMemcpyDeviceToHost, sm) != cudaSuccess ||
+        cudaStreamSynchronize(sm) != cudaSuccess)
+        return MGBVH_ERR_CUDA;
+    if (herr == 1) return MGBVH_ERR_CAPACITY;  // traversal stack would have overflowed
+    if (herr) return MGBVH_ERR_INVALID_ARG;    // a TLAS leaf names an instance or mesh past the tables
+    if (out_counts) {
+        out_counts[0] = hc.nodes;
+        out_counts[1] = hc.boxes;
+        out_counts[2] = hc.tris;
+    }
+    if (out_seconds) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, t->ev0, t->ev1);
+        *out_seconds = ms * 1e-3;
+    }
+    return MGBVH_OK;
+}
+
+int mgbvh_trace_scene_bruteforce_dev(mgbvh_tracer* t, const float* d_rays, uint32_t n_rays, float* d_hit_t,
+                                     uint32_t* d_hit_instance, uint32_t* d_hit_triangle, int cull_by_mesh_bounds,
+                                     void* stream) {
+    if (!t || !t->scene || (n_rays && (!d_rays || !d_hit_t || !d_hit_instance || !d_hit_triangle)))
+        return MGBVH_ERR_INVALID_ARG;
+    if (n_rays == 0) return MGBVH_OK;
+    if (cudaSetDevice(t->device) != cudaSuccess) return MGBVH_ERR_CUDA;
+    const cudaStream_t sm = reinterpret_cast<cudaStream_t>(stream);
+    brute_scene_kernel<<<std::min<uint32_t>(n_rays, 148u * 8u), kBruteThreads, 0, sm>>>(
+        t->inst, t->n_inst, t->meshes, t->n_meshes, reinterpret_cast<const float4*>(t->blas), t->tris,
+        reinterpret_cast<const float4*>(d_rays), n_rays, d_hit_t, d_hit_instance, d_hit_triangle,
+        cull_by_mesh_bounds);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;
     return trace_check(cudaStreamSynchronize(sm));
 }

@@ -62,6 +62,11 @@ constexpr float kInf = std::numeric_limits<float>::infinity();
 // thresholds that split different object sets (the only place where list
 // order, not the object set, picks the split).
 thread_local uint32_t g_tie_events = 0;
+// Nodes of the last build on this thread whose split was one of several
+// equal-cost splits over different object sets on the winning axis, chosen by
+// list order: the nodes where the reference's unstable partitions
+// (partition_in_place, select_nth_unstable_by) could make its tree differ.
+thread_local uint32_t g_order_dependent = 0;
 
 // glam's SSE2 Vec3A::min/max are _mm_min_ps/_mm_max_ps: a < b ? a : b.
 inline float vmin(float a, float b) { return a < b ? a : b; }
@@ -130,6 +135,9 @@ struct Split {
     int axis;
     float threshold;
     uint32_t index;
+    // len < 8 adaptive split whose axis holds another threshold of the same
+    // cost over a different object set: list order picked this one
+    bool order_dep = false;
 };
 
 struct Node {
@@ -192,7 +200,7 @@ struct Builder {
     // node samples for the learned split proposer (features + full-sweep label)
     std::vector<float>* samples = nullptr;
     uint32_t sample_min_n = 33;
-    uint32_t median_splits = 0, tie_events = 0, depth_capped = 0, learned_splits = 0;
+    uint32_t median_splits = 0, tie_events = 0, depth_capped = 0, learned_splits = 0, order_dependent = 0;
     int error = 0;
 
     Builder(const Acc& a, uint32_t mn, uint32_t mx, uint32_t md, Knobs kn)
@@ -307,6 +315,7 @@ struct Builder {
                         float c = center(list[j], axis);
                         if (c >= lo && c < hi) {
                             tie_events++;
+                            out.order_dep = true;
                             break;
                         }
                     }
@@ -688,6 +697,7 @@ struct Builder {
             if (!select_split(self.bounds, s, n, sp)) continue;  // :576-579
             // :583 (leaf_cost, :251-253); a NaN cost compares false and splits
             if (self.len <= MAX && sp.cost >= kObjectCost * static_cast<float>(self.len)) continue;
+            if (sp.order_dep) order_dependent++;
             if (k.learn_max_n && !k.full_sweep && n > 32 && n <= k.learn_max_n && sp.kind == kIndex &&
                 (k.bins ? k.bins : std::clamp<uint32_t>(n, 16, 32)) == 32)
                 learned_refine(self.bounds, s, n, sp);
@@ -798,7 +808,36 @@ int run_build(const Acc& acc, uint32_t n, const float* root_bounds, uint32_t MIN
         st->feasible = feasible;
     }
     g_tie_events = b.tie_events;
+    g_order_dependent = b.order_dependent;
     return feasible ? MGBVH_OK : MGBVH_WARN_INFEASIBLE;
+}
+
+// Moller-Trumbore as marigold/assets/shaders/slang/lib/scene.slang:19-89
+// evaluates it (|det| < 1e-6 and t < 1e-6 reject), every product and sum as
+// written; returns t or -1 (miss).
+float moller_trumbore(float ox, float oy, float oz, float dx, float dy, float dz, const float* a, const float* b,
+                      const float* c) {
+    auto dot3 = [](float ax, float ay, float az, float bx, float by, float bz) {
+        float d = ax * bx;
+        d = d + ay * by;
+        d = d + az * bz;
+        return d;
+    };
+    const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
+    const float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
+    const float hx = dy * e2z - dz * e2y, hy = dz * e2x - dx * e2z, hz = dx * e2y - dy * e2x;
+    const float det = dot3(hx, hy, hz, e1x, e1y, e1z);
+    if (std::fabs(det) < 1e-6f) return -1.0f;
+    const float f = 1.0f / det;
+    const float sx = ox - a[0], sy = oy - a[1], sz = oz - a[2];
+    const float u = f * dot3(sx, sy, sz, hx, hy, hz);
+    if (u < 0.0f || u > 1.0f) return -1.0f;
+    const float qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
+    const float v = f * dot3(dx, dy, dz, qx, qy, qz);
+    if (v < 0.0f || u + v > 1.0f) return -1.0f;
+    const float t = f * dot3(e2x, e2y, e2z, qx, qy, qz);
+    if (t < 1e-6f) return -1.0f;
+    return t;
 }
 
 }  // namespace
@@ -853,6 +892,7 @@ int oracle_build(const float* verts, uint32_t vertex_stride_bytes, const uint32_
 }
 
 uint32_t oracle_last_tie_events(void) { return g_tie_events; }
+uint32_t oracle_last_order_dependent(void) { return g_order_dependent; }
 
 // Node samples of a plain (reference-profile) build over triangles: 30 floats
 // per node with at least min_n objects (24 features, label as u32 bits, gain
@@ -928,35 +968,16 @@ uint32_t oracle_instance_aabbs(const float* mesh_bounds, uint32_t mesh_count, co
 void oracle_trace_bruteforce(const float* verts, uint32_t stride_floats, const uint32_t* tris,
                              uint32_t n, const float* rays, uint32_t n_rays, float* out_t,
                              uint32_t* out_prim) {
-    auto dot3 = [](float ax, float ay, float az, float bx, float by, float bz) {
-        float d = ax * bx;
-        d = d + ay * by;
-        d = d + az * bz;
-        return d;
-    };
     for (uint32_t r = 0; r < n_rays; ++r) {
         const float* R = rays + 8 * (size_t)r;
-        const float ox = R[0], oy = R[1], oz = R[2], dx = R[4], dy = R[5], dz = R[6];
         float best = std::numeric_limits<float>::infinity();
         uint32_t best_prim = 0xFFFFFFFFu;
         for (uint32_t p = 0; p < n; ++p) {
             const float* a = verts + (size_t)tris[3 * (size_t)p] * stride_floats;
             const float* b = verts + (size_t)tris[3 * (size_t)p + 1] * stride_floats;
             const float* c = verts + (size_t)tris[3 * (size_t)p + 2] * stride_floats;
-            const float e1x = b[0] - a[0], e1y = b[1] - a[1], e1z = b[2] - a[2];
-            const float e2x = c[0] - a[0], e2y = c[1] - a[1], e2z = c[2] - a[2];
-            const float hx = dy * e2z - dz * e2y, hy = dz * e2x - dx * e2z, hz = dx * e2y - dy * e2x;
-            const float det = dot3(hx, hy, hz, e1x, e1y, e1z);
-            if (std::fabs(det) < 1e-6f) continue;
-            const float f = 1.0f / det;
-            const float sx = ox - a[0], sy = oy - a[1], sz = oz - a[2];
-            const float u = f * dot3(sx, sy, sz, hx, hy, hz);
-            if (u < 0.0f || u > 1.0f) continue;
-            const float qx = sy * e1z - sz * e1y, qy = sz * e1x - sx * e1z, qz = sx * e1y - sy * e1x;
-            const float v = f * dot3(dx, dy, dz, qx, qy, qz);
-            if (v < 0.0f || u + v > 1.0f) continue;
-            const float t = f * dot3(e2x, e2y, e2z, qx, qy, qz);
-            if (t < 1e-6f) continue;
+            const float t = moller_trumbore(R[0], R[1], R[2], R[4], R[5], R[6], a, b, c);
+            if (t < 0.0f) continue;
             if (t < best || (t == best && p < best_prim)) {
                 best = t;
                 best_prim = p;
@@ -964,6 +985,64 @@ void oracle_trace_bruteforce(const float* verts, uint32_t stride_floats, const u
         }
         out_t[r] = best_prim == 0xFFFFFFFFu ? -1.0f : best;
         out_prim[r] = best_prim;
+    }
+}
+
+// Closest hit of each world-space ray in a two-level scene, by brute force
+// (the checker of the two-level traversal; marigold's scene shader,
+// scene.slang:91-220, walks the same scene through its TLAS): for every
+// instance the ray moves into mesh space through the instance's column-major
+// inverse transform, each component ((c0 x + c1 y) + c2 z) + c3 w rounded
+// after every product and sum, and meets every triangle of the instance's
+// mesh. The hit distance is the ray parameter, the same in both spaces; equal
+// distances resolve to the lowest (instance, triangle). meshes: 4 u32 per
+// mesh (BLAS root, unused here; triangle offset; triangle count; vertex
+// offset); instances: 20 words each (16 floats of the inverse transform, the
+// mesh index, 3 unused); tris: vertex index triples relative to the mesh's
+// vertex offset.
+void oracle_trace_scene_bruteforce(const float* verts, uint32_t stride_floats, const uint32_t* tris,
+                                   const uint32_t* meshes, uint32_t n_meshes, const uint32_t* instances,
+                                   uint32_t n_inst, const float* rays, uint32_t n_rays, float* out_t,
+                                   uint32_t* out_inst, uint32_t* out_tri) {
+    auto xform = [](const float* m, float x, float y, float z, float w, float* o) {
+        for (int r = 0; r < 3; ++r) {
+            float s = m[r] * x;
+            s = s + m[4 + r] * y;
+            s = s + m[8 + r] * z;
+            s = s + m[12 + r] * w;
+            o[r] = s;
+        }
+    };
+    for (uint32_t r = 0; r < n_rays; ++r) {
+        const float* R = rays + 8 * (size_t)r;
+        float best = std::numeric_limits<float>::infinity();
+        uint32_t bi = 0xFFFFFFFFu, bp = 0xFFFFFFFFu;
+        for (uint32_t k = 0; k < n_inst; ++k) {
+            const uint32_t* I = instances + 20 * (size_t)k;
+            if (I[16] >= n_meshes) continue;
+            float m[16];
+            std::memcpy(m, I, sizeof(m));
+            const uint32_t* M = meshes + 4 * (size_t)I[16];
+            float o[3], d[3];
+            xform(m, R[0], R[1], R[2], 1.0f, o);
+            xform(m, R[4], R[5], R[6], 0.0f, d);
+            for (uint32_t q = 0; q < M[2]; ++q) {
+                const uint32_t p = M[1] + q;
+                const float* a = verts + (size_t)(tris[3 * (size_t)p] + M[3]) * stride_floats;
+                const float* b = verts + (size_t)(tris[3 * (size_t)p + 1] + M[3]) * stride_floats;
+                const float* c = verts + (size_t)(tris[3 * (size_t)p + 2] + M[3]) * stride_floats;
+                const float t = moller_trumbore(o[0], o[1], o[2], d[0], d[1], d[2], a, b, c);
+                if (t < 0.0f) continue;
+                if (t < best || (t == best && (k < bi || (k == bi && p < bp)))) {
+                    best = t;
+                    bi = k;
+                    bp = p;
+                }
+            }
+        }
+        out_t[r] = bp == 0xFFFFFFFFu ? -1.0f : best;
+        out_inst[r] = bi;
+        out_tri[r] = bp;
     }
 }
 

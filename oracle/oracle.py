@@ -89,8 +89,11 @@ def lib():
                                        ctypes.POINTER(u32), ctypes.POINTER(Stats)]
             L.oracle_build.restype = ctypes.c_int
             L.oracle_last_tie_events.restype = u32
+            L.oracle_last_order_dependent.restype = u32
             L.oracle_trace_bruteforce.argtypes = [P, u32, P, u32, P, u32, P, P]
             L.oracle_trace_bruteforce.restype = None
+            L.oracle_trace_scene_bruteforce.argtypes = [P, u32, P, P, u32, P, u32, P, u32, P, P, P]
+            L.oracle_trace_scene_bruteforce.restype = None
             L.oracle_sample_nodes.argtypes = [P, u32, P, u32, u32, P, u32]
             L.oracle_instance_aabbs.argtypes = [P, u32, P, P, u32, P]
             L.oracle_instance_aabbs.restype = u32
@@ -147,6 +150,7 @@ def build(vertices=None, triangles=None, aabbs=None, *, vertex_stride_bytes=32,
         "perm": perm[:n].copy(),
         "stats": st.as_dict(),
         "tie_events": L.oracle_last_tie_events(),
+        "order_dependent": L.oracle_last_order_dependent(),
     }
 
 
@@ -161,6 +165,28 @@ def trace_bruteforce(vertices, triangles, rays):
     L.oracle_trace_bruteforce(_ptr(v), v.shape[1], _ptr(t), t.shape[0], _ptr(r), r.shape[0],
                               _ptr(out_t), _ptr(out_p))
     return out_t, out_p
+
+
+def trace_scene_bruteforce(vertices, triangles, meshes, instances, rays):
+    """Closest hit of each world-space ray in a two-level scene, every
+    triangle of every instance tested in mesh space (CPU). vertices float32
+    [V, k]; triangles uint32 [T, 3] relative to each mesh's vertex offset;
+    meshes uint32 [M, 4] (BLAS root, triangle offset, count, vertex offset);
+    instances [I, 20] words (inverse transform, mesh, pad). Returns (t,
+    instance, triangle)."""
+    L = lib()
+    v = np.ascontiguousarray(vertices, dtype=np.float32)
+    t = np.ascontiguousarray(triangles, dtype=np.uint32)
+    m = np.ascontiguousarray(meshes).view(np.uint32)
+    ins = np.ascontiguousarray(instances).view(np.uint32)
+    r = np.ascontiguousarray(rays, dtype=np.float32)
+    n = r.shape[0]
+    out_t = np.zeros(n, np.float32)
+    out_i = np.zeros(n, np.uint32)
+    out_p = np.zeros(n, np.uint32)
+    L.oracle_trace_scene_bruteforce(_ptr(v), v.shape[1], _ptr(t), _ptr(m), m.shape[0], _ptr(ins), ins.shape[0],
+                                    _ptr(r), n, _ptr(out_t), _ptr(out_i), _ptr(out_p))
+    return out_t, out_i, out_p
 
 
 SAMPLE_WIDTH = 30  # 24 features, label, gain, n, plain cost, full-sweep cost, start

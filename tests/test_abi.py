@@ -48,6 +48,20 @@ def test_struct_layouts_match_header(tmp_path):
     assert got[0] == 32 == NODE_DTYPE.itemsize
 
 
+def test_scene_record_layouts(tmp_path):
+    # the two-level scene records: 16-byte mesh table rows, 80-byte instances
+    # (marigold_b200.bvh.Scene writes them as int32 [M, 4] and [I, 20])
+    src = tmp_path / "sc.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "mgbvh.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu\\n", sizeof(mgbvh_scene_mesh), sizeof(mgbvh_scene_instance), '
+        'offsetof(mgbvh_scene_mesh, vertex_offset), offsetof(mgbvh_scene_instance, mesh));return 0;}\n')
+    exe = tmp_path / "sc"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got == [16, 80, 12, 64]
+
+
 def test_default_settings_are_the_reference_profile():
     s = _lib.Settings()
     _lib.load().mgbvh_default_settings(ctypes.byref(s))

@@ -35,18 +35,13 @@ KNOWN = [
     [unit_box(0), unit_box(2), unit_box(4), unit_box(6)],
     [unit_box(0)] * 4,
     [unit_box(0)] * 40,      # forced medians through the medium-node path
-    [unit_box(0)] * 1030,    # coincident centroids in a node above the CTA size
+    [unit_box(0)] * 1030,    # coincident centroids in a node above the CTA size: level-pass medians
 ]
 
 
 @pytest.mark.parametrize("case", range(len(KNOWN)))
 def test_known_answer_cases(oracle, gpu_ctx, case):
     boxes = np.array(KNOWN[case], np.float32)
-    if case == 6:
-        g = gpu_build(gpu_ctx, aabbs=boxes)
-        # a forced median above 1024 objects is reported, not silently built
-        assert g["status"] == -6, g
-        return
     both(oracle, gpu_ctx, aabbs=boxes)
 
 
@@ -188,3 +183,30 @@ def test_level_hint_across_meshes(oracle):
             assert compare_exact(g["nodes"], g["lens"], g["perm"], o["nodes"], o["lens"], o["perm"]) is None
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("key", ["config1_reference", "config1_bins16_adaptive_off", "config2_reference",
+                                 "config2_adaptive_steps16"])
+def test_output_hashes_equal_the_committed_oracle_hashes(gpu_ctx, key):
+    # tests/golden/oracle_hashes.json holds the oracle's bytes for these
+    # workloads (tests/golden/make_oracle_hashes.py); no oracle run here
+    import hashlib
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "oracle_hashes.json")))[key]
+    v, t = synth.config1_mesh() if g["mesh"] == "config1" else synth.config2_mesh()
+    r = gpu_build(gpu_ctx, vertices=v, triangles=t, root_bounds=synth.mesh_bounds(v), **g["knobs"])
+    assert r["status"] == 0 and r["nodes"].shape[0] == g["nodes"]
+    h = hashlib.sha256()
+    for a in (r["nodes"], r["lens"], r["perm"]):
+        h.update(np.ascontiguousarray(a, dtype="<u4").tobytes())
+    assert h.hexdigest() == g["sha256"]
+
+
+@pytest.mark.parametrize("name", ["adaptive_8", "adaptive_16", "binned_33", "binned_64"])
+def test_worked_root_splits(oracle, gpu_ctx, name):
+    from tests.test_oracle_pins import CASES, line_boxes
+    boxes = line_boxes(CASES[name][0])
+    both(oracle, gpu_ctx, aabbs=boxes)
+    # the same lines with 16 bins and 4 fixed adaptive steps
+    both(oracle, gpu_ctx, aabbs=boxes, bins=16, adaptive_steps=4)

@@ -70,3 +70,42 @@ def test_two_calls_in_a_row_match_the_allocating_build():
 def test_rejects_more_than_the_limit():
     got = noalloc_build(boxes(_lib.NOALLOC_MAX_OBJECTS + 1, 3))
     assert got["status"] == _lib.ERR_TOO_LARGE
+
+
+@pytest.mark.parametrize("n", [1, 2, 32, 33, 1024])
+def test_sizes_against_the_oracle(oracle, n):
+    """n = 1: the root is a leaf; 2 and 32: one warp subtree; 33: the
+    smallest subtree-CTA build; 1024: the limit. Each equals the oracle and
+    the allocating build, in both leaf-size profiles."""
+    ctx = _lib.Context(0)
+    for kw in ({}, dict(min_leaf=2, max_leaf=4)):
+        aabbs = boxes(n, 40 + n)
+        got = noalloc_build(aabbs, **kw)
+        want = oracle.build(aabbs=aabbs, **kw)
+        assert got["status"] == want["status"] >= 0, (n, kw, got["status"], want["status"])
+        msg = compare_exact(got["nodes"], got["lens"], got["perm"], want["nodes"], want["lens"], want["perm"])
+        assert msg is None, (n, kw, msg)
+        alloc = gpu_build(ctx, aabbs=aabbs, **kw)
+        msg = compare_exact(got["nodes"], got["lens"], got["perm"], alloc["nodes"], alloc["lens"], alloc["perm"])
+        assert msg is None, (n, kw, msg)
+    ctx.close()
+
+
+def test_capacity_too_small():
+    import torch
+    L = _lib.load()
+    aabbs = boxes(500, 7)
+    n = aabbs.shape[0]
+    cap = 2 * n - 2  # one node short of the tree
+    d_aabbs = torch.from_numpy(aabbs).cuda()
+    d_nodes = torch.zeros(cap * 8, dtype=torch.int32, device="cuda")
+    d_perm = torch.zeros(n, dtype=torch.int32, device="cuda")
+    count = ctypes.c_uint32(12345)
+    torch.cuda.synchronize()
+    rc = L.mgbvh_build_aabbs_noalloc(ctypes.c_void_p(d_aabbs.data_ptr()), n, ctypes.byref(settings()),
+                                     ctypes.c_void_p(d_nodes.data_ptr()), cap, ctypes.byref(count), None,
+                                     ctypes.c_void_p(d_perm.data_ptr()), None)
+    assert rc == _lib.ERR_CAPACITY and count.value == 0
+    # the next call on the shared scratch is unaffected
+    got = noalloc_build(aabbs)
+    assert got["status"] == 0 and got["nodes"].shape[0] == 2 * n - 1
