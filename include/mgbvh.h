@@ -242,6 +242,32 @@ MGBVH_API int mgbvh_set_graph_capture(mgbvh_ctx* ctx, int enable);
    smaller ones to the per-subtree kernels. */
 MGBVH_API int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max);
 
+/* How mgbvh_build_batch_dev builds (no counterpart in the reference, whose
+   marigold/src/app/data/scene/model.rs:77-95 builds one BLAS per rayon
+   worker and then the TLAS; the trees are the same either way):
+     MGBVH_BATCH_LEVELS  level passes over every mesh's nodes above
+                         medium_max, then one launch for the subtrees of
+                         33..medium_max objects and one for those of <= 32
+                         (the default);
+     MGBVH_BATCH_QUEUE   one persistent launch: resident CTAs take node
+                         tasks of every mesh and the TLAS from device-side
+                         queues (one CTA splits a node above medium_max or
+                         builds a subtree of 33..medium_max objects; its
+                         warps build subtrees of <= 32) and push the
+                         children. Plain builds of meshes up to 4,194,304
+                         objects; others take the level passes. Forced medians
+                         of nodes above medium_max run after the launch.
+   Every wait of the persistent launch is bounded (2 s by default): when one
+   runs out the launch ends and the build returns MGBVH_ERR_TIMEOUT. */
+#define MGBVH_BATCH_LEVELS 0
+#define MGBVH_BATCH_QUEUE 1
+MGBVH_API int mgbvh_set_batch_mode(mgbvh_ctx* ctx, int mode);
+/* The persistent launch's wait bound in microseconds (0: 2 s), and, for
+   tests of that bound, a number of tasks counted as pending that never
+   arrive (0 in normal use): with held_tasks > 0 every wait runs out and the
+   build returns MGBVH_ERR_TIMEOUT. */
+MGBVH_API int mgbvh_set_queue_limits(mgbvh_ctx* ctx, uint32_t wait_microseconds, uint32_t held_tasks);
+
 /* World AABBs of instances for the TLAS, computed on the GPU as marigold's
    scene upload computes them on the host (marigold/src/app/data/scene/
    model.rs:191-234): the 8 corners of each instance's mesh bounds through its

@@ -37,7 +37,10 @@ EXPORTED = (
     "mgbvh_set_split_proposer", "mgbvh_set_sample_output", "mgbvh_instance_aabbs_dev",
     "mgbvh_tracer_build_wide", "mgbvh_tracer_wide_nodes", "mgbvh_trace_closest_wide_dev",
     "mgbvh_tracer_set_scene_dev", "mgbvh_trace_scene_dev", "mgbvh_trace_scene_bruteforce_dev",
+    "mgbvh_set_batch_mode", "mgbvh_set_queue_limits",
 )
+BATCH_LEVELS = 0
+BATCH_QUEUE = 1
 
 
 class Node(ctypes.Structure):
@@ -202,6 +205,10 @@ def load():
         L.mgbvh_instance_aabbs_dev.restype = ctypes.c_int
         L.mgbvh_set_tuning.argtypes = [P, u32]
         L.mgbvh_set_tuning.restype = ctypes.c_int
+        L.mgbvh_set_batch_mode.argtypes = [P, ctypes.c_int]
+        L.mgbvh_set_batch_mode.restype = ctypes.c_int
+        L.mgbvh_set_queue_limits.argtypes = [P, u32, u32]
+        L.mgbvh_set_queue_limits.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]
         L.mgbvh_sah_cost.restype = ctypes.c_double
         _lib = L
@@ -235,6 +242,14 @@ class Context:
 
     def set_tuning(self, medium_max: int):
         self.check(self.L.mgbvh_set_tuning(self.ptr, medium_max))
+
+    def set_batch_mode(self, queue: bool):
+        """Batched builds by one persistent launch over device-side task
+        queues (True) or by level passes and subtree launches (False)."""
+        self.check(self.L.mgbvh_set_batch_mode(self.ptr, BATCH_QUEUE if queue else BATCH_LEVELS))
+
+    def set_queue_limits(self, wait_us: int = 0, held_tasks: int = 0):
+        self.check(self.L.mgbvh_set_queue_limits(self.ptr, wait_us, held_tasks))
 
     def set_graph_capture(self, on: bool):
         self.check(self.L.mgbvh_set_graph_capture(self.ptr, 1 if on else 0))

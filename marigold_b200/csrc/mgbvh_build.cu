@@ -60,6 +60,24 @@ struct Rec {
     float4 hi;  // max xyz, 0
 };
 
+// A record read through L2 only. Within one launch of the persistent batched
+// build, records are rewritten by other CTAs (other SMs), whose writes an
+// SM's L1 does not see: reads of such data bypass L1.
+__device__ __forceinline__ Rec ldcg_rec(const Rec* p) {
+    Rec r;
+    r.lo = __ldcg(&p->lo);
+    r.hi = __ldcg(&p->hi);
+    return r;
+}
+
+template <bool kCoherent>
+__device__ __forceinline__ Rec load_rec(const Rec* p) {
+    if constexpr (kCoherent)
+        return ldcg_rec(p);
+    else
+        return *p;
+}
+
 // A node waiting to be split (large, medium or small list entry). 64 bytes.
 struct Task {
     float lo[3];
@@ -71,9 +89,20 @@ struct Task {
     uint32_t nbase, tbase;  // node-slot and record offsets of the object's mesh (batched builds)
 };
 
+// A task read through L2 only (see ldcg_rec).
+__device__ __forceinline__ Task ldcg_task(const Task* p) {
+    static_assert(sizeof(Task) == 64, "task layout");
+    Task t;
+    const uint4* q = reinterpret_cast<const uint4*>(p);
+    uint4* d = reinterpret_cast<uint4*>(&t);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) d[k] = __ldcg(q + k);
+    return t;
+}
+
 // Split decision of one large node, read by its partition tiles.
 struct Decision {
-    uint32_t kind;  // 0 split, 1 leaf, 2 forced median (deferred to the median passes)
+    uint32_t kind;  // 0 split, 1 leaf (or a forced median deferred to the median passes)
     uint32_t axis, split_bin, bins;
     float cmin, ext;
     uint32_t n_lt;
@@ -589,9 +618,11 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
             if (t.len > P.max_leaf) {
                 // no binned split and too many objects for a leaf: the forced
                 // median (bvh/src/lib.rs:527-531) runs in the median passes
-                // after this build's pipeline; the partition skips the node
+                // after this build's pipeline. The partition treats the node
+                // as a leaf: it only copies the ids into the permutation, which
+                // the leaves of the node's subtree overwrite later.
                 if (lane == 0) {
-                    d.kind = 2;
+                    d.kind = 1;
                     A.dec[w] = d;
                     const uint32_t mi = atomicAdd(&O.ctr->n_med, 1u);
                     if (mi < A.cap_tasks)
@@ -995,10 +1026,9 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_
         const uint32_t cnt = min(kTile, tlen - begin);
         const Rec* src = (t.buf ? rec1 : rec0) + tstart + begin;
         Rec* dst = t.buf ? rec0 : rec1;
-        if (d.kind != 0) {  // 1: leaf; 2: forced median, partitioned by the median passes
-            if (d.kind == 1)
-                for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
-                    O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
+        if (d.kind == 1) {
+            for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
+                O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
             continue;
         }
         const uint32_t axis = d.axis, split_bin = d.split_bin, nbins = d.bins, n_lt = d.n_lt;
@@ -1706,11 +1736,17 @@ __global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, __
     t[i] = src >= 0 ? w[src] : __float2bfloat16_rn(0.0f);
 }
 
+// The persistent batched build's queues (defined with its kernel below).
+struct QueueArgs;
+__device__ void queue_push_small(const QueueArgs& Q, const Task& t, Counters* ctr);
+
 // One CTA builds the subtree of one medium node (33..1024 objects).
-template <bool kLearn, class MS>
+// kQueue: subtrees of <= 32 objects go to the persistent build's small
+// queue (QA) instead of the small list.
+template <bool kLearn, class MS, bool kQueue = false>
 __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec* rec1,
                                             Task* small, uint32_t cap_small, const Params& P,
-                                            const Out& O, const Learn& LN) {
+                                            const Out& O, const Learn& LN, const QueueArgs* QA = nullptr) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     Rec* src = (t.buf ? rec1 : rec0) + t.start;
     const uint32_t base = t.start;
@@ -1720,7 +1756,7 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
     if (threadIdx.x < 2) S.list_n[threadIdx.x] = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) {
-        const Rec r = src[i];
+        const Rec r = load_rec<kQueue>(src + i);
         S.rlo[i] = r.lo;
         S.rhi[i] = r.hi;
         S.idx[0][i] = static_cast<uint16_t>(i);
@@ -1971,6 +2007,29 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                         rr.hi = S.rhi[r];
                         src[cs + lane] = rr;
                     }
+                    if constexpr (kQueue) {
+                        // the records reach memory before the task is marked ready
+                        __threadfence();
+                        __syncwarp();
+                        if (lane == 0) {
+                            Task st;
+                            for (int a = 0; a < 3; ++a) {
+                                st.lo[a] = cbx[a];
+                                st.hi[a] = cbx[3 + a];
+                            }
+                            st.start = base + cs;
+                            st.len = len;
+                            st.slot = slot;
+                            st.pair = pair;
+                            st.depth = cdepth;
+                            st.buf = t.buf;
+                            st.tile0 = st.ntiles = 0;
+                            st.nbase = t.nbase;
+                            st.tbase = t.tbase;
+                            queue_push_small(*QA, st, O.ctr);
+                        }
+                        continue;
+                    }
                     uint32_t si = 0;
                     if (lane == 0) si = atomicAdd(&O.ctr->n_small, 1u);
                     si = __shfl_sync(kFull, si, 0);
@@ -2157,6 +2216,462 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
         else
             warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase,
                                b, P, O, xchg[wib]);
+    }
+}
+
+// ---------------------------------------------------------------- persistent batched build
+//
+// A batch of meshes (every BLAS and the TLAS) built by one persistent launch
+// that takes node tasks from device-side queues, in place of the level
+// passes and the subtree launches. One CTA of kMediumThreads threads per
+// resident slot loops: pop a task, build it, push its children.
+//   main queue   nodes above 32 objects. Above medium_max the CTA bins the
+//                node (3 x 32 bins in shared memory), warp 0 picks the split,
+//                the CTA partitions the records stably into the other buffer
+//                and pushes the children; at or below medium_max it builds
+//                the whole subtree in shared memory (medium_task), pushing its
+//                subtrees of <= 32 objects to the small queue.
+//   small queue  subtrees of <= 32 objects (the small list, ctr->n_small as
+//                its tail), taken four at a time, one per warp.
+// A push counts the task as pending, writes it, fences and then marks it
+// ready; a finished task is uncounted after its children were pushed, so
+// pending reaches 0 only when the whole batch is built, and every CTA then
+// leaves. Every wait (an empty queue while tasks are pending, a claimed slot
+// not yet marked ready) is bounded by a deadline on the global timer; when
+// one runs out the CTA records the time-out, raises abort and leaves, and so
+// do all others at their next poll: the launch ends with MGBVH_ERR_TIMEOUT.
+// Nodes that need the forced median are queued for the median passes, which
+// run after the launch as in the level-pass build.
+
+constexpr uint32_t kQueueMaxMesh = 1u << 22;  // largest mesh the persistent build takes (objects)
+#ifndef MGBVH_QUEUE_MIN_BLOCKS
+#define MGBVH_QUEUE_MIN_BLOCKS 4  // persistent CTAs per SM the register budget must allow (tuning knob)
+#endif
+
+struct QueueState {
+    uint32_t head, tail;  // main queue: next entry to pop, next entry to reserve
+    uint32_t shead;       // small queue: next entry to pop (its tail is ctr->n_small)
+    uint32_t pending;     // tasks pushed and not yet finished
+    uint32_t abort;       // an error or a time-out: every CTA leaves
+    uint32_t timeouts;    // waits that ran out
+    uint32_t pad[2];
+};
+
+struct QueueArgs {
+    Task* q;           // main queue entries
+    uint32_t* qready;  // 1 once entry i is written
+    uint32_t* qcb;     // centroid bound keys of entry i (6; level-pass-size nodes)
+    uint32_t qcap;
+    Task* small;       // small queue (the small list)
+    uint32_t* sready;
+    uint32_t scap;
+    QueueState* st;
+    Task* med;         // nodes waiting for the forced median (count in ctr->n_med)
+    uint32_t med_cap;
+    unsigned long long wait_ns;  // longest wait before a time-out
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t vload(const uint32_t* p) { return *reinterpret_cast<const volatile uint32_t*>(p); }
+
+__device__ __forceinline__ void queue_abort(const QueueArgs& Q) { atomicExch(&Q.st->abort, 1u); }
+
+// Waits until *flag is 1; false if the deadline passed or the build aborted.
+__device__ __forceinline__ bool wait_ready(const QueueArgs& Q, const uint32_t* flag) {
+    const unsigned long long t0 = global_ns();
+    uint32_t ns = 32;
+    while (vload(flag) == 0u) {
+        if (vload(&Q.st->abort)) return false;
+        if (global_ns() - t0 > Q.wait_ns) {
+            atomicAdd(&Q.st->timeouts, 1u);
+            queue_abort(Q);
+            return false;
+        }
+        __nanosleep(ns);
+        ns = min(ns * 2u, 1024u);
+    }
+    __threadfence();  // the entry (and the records it names) before the flag
+    return true;
+}
+
+// One thread: push a node task of more than 32 objects (cb: its centroid
+// bound keys when it is above medium_max).
+__device__ void queue_push_main(const QueueArgs& Q, const Task& t, const uint32_t* cb, Counters* ctr) {
+    atomicAdd(&Q.st->pending, 1u);
+    const uint32_t i = atomicAdd(&Q.st->tail, 1u);
+    if (i >= Q.qcap) {
+        set_error(ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+        queue_abort(Q);
+        return;
+    }
+    Q.q[i] = t;
+    if (cb)
+        for (int k = 0; k < 6; ++k) Q.qcb[6 * i + k] = cb[k];
+    __threadfence();
+    atomicExch(&Q.qready[i], 1u);
+}
+
+// One thread: push a subtree of <= 32 objects.
+__device__ void queue_push_small(const QueueArgs& Q, const Task& t, Counters* ctr) {
+    atomicAdd(&Q.st->pending, 1u);
+    const uint32_t i = atomicAdd(&ctr->n_small, 1u);
+    if (i >= Q.scap) {
+        set_error(ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+        queue_abort(Q);
+        return;
+    }
+    Q.small[i] = t;
+    __threadfence();
+    atomicExch(&Q.sready[i], 1u);
+}
+
+// Thread 0: the next task (kind 1: main entry idx; kind 2: small entries idx
+// .. idx + count - 1) or none (kind 0: the batch is done, or aborted).
+struct Popped {
+    uint32_t kind, idx, count;
+};
+
+__device__ Popped queue_pop(const QueueArgs& Q, Counters* ctr) {
+    Popped p{0u, 0u, 0u};
+    const unsigned long long t0 = global_ns();
+    uint32_t ns = 32;
+    for (;;) {
+        if (vload(&Q.st->abort)) return p;
+        const uint32_t h = vload(&Q.st->head), tl = min(vload(&Q.st->tail), Q.qcap);
+        if (h < tl) {
+            if (atomicCAS(&Q.st->head, h, h + 1u) == h) {
+                if (!wait_ready(Q, Q.qready + h)) return p;
+                p.kind = 1;
+                p.idx = h;
+                return p;
+            }
+            continue;
+        }
+        const uint32_t sh = vload(&Q.st->shead), stl = min(vload(&ctr->n_small), Q.scap);
+        if (sh < stl) {
+            const uint32_t n = min(stl - sh, (uint32_t)kMediumWarps);
+            if (atomicCAS(&Q.st->shead, sh, sh + n) == sh) {
+                for (uint32_t k = 0; k < n; ++k)
+                    if (!wait_ready(Q, Q.sready + sh + k)) return p;
+                p.kind = 2;
+                p.idx = sh;
+                p.count = n;
+                return p;
+            }
+            continue;
+        }
+        if (vload(&Q.st->pending) == 0u) return p;  // every task finished: the batch is built
+        if (global_ns() - t0 > Q.wait_ns) {
+            atomicAdd(&Q.st->timeouts, 1u);
+            queue_abort(Q);
+            return p;
+        }
+        __nanosleep(ns);
+        ns = min(ns * 2u, 1024u);
+    }
+}
+
+struct LargeSmem {
+    uint32_t bins[kBinWords];
+    uint32_t wlt[kMediumWarps], wn[kMediumWarps];
+    uint32_t keys[12];
+    uint32_t kind, axis, split_bin, n_lt;  // kind: 0 split, 1 leaf, 2 forced median
+    float ltb[6], gtb[6];
+    int bad;
+};
+
+// One CTA: a node above medium_max objects (records in buffer t.buf, its
+// centroid bound keys cbk), as lvl_bin + lvl_eval + lvl_part do for a level.
+__device__ void queue_large_task(const QueueArgs& Q, LargeSmem& L, const Task& t, const uint32_t* cbk, Rec* rec0,
+                                 Rec* rec1, const Params& P, const Out& O) {
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+    Rec* dst = (t.buf ? rec0 : rec1) + t.start;
+    const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    const uint32_t n = t.len, B = P.bins ? P.bins : 32u;
+    float cmn[3], ext[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        cmn[a] = funkey(__ldcg(cbk + a));
+        ext[a] = __fsub_rn(funkey(__ldcg(cbk + 3 + a)), cmn[a]);
+    }
+    const bool leaf0 = t.depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf);
+    if (!leaf0) {
+        init_task_bins(L.bins, tid, blockDim.x);
+        __syncthreads();
+        for (uint32_t i = tid; i < n; i += blockDim.x) {
+            const Rec r = ldcg_rec(src + i);
+            const float l[3] = {r.lo.x, r.lo.y, r.lo.z}, h[3] = {r.hi.x, r.hi.y, r.hi.z};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (ext[a] == 0.0f) continue;  // block-uniform
+                uint32_t* w = L.bins + (a * 32 + bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B)) * 7;
+                atomicAdd(w, 1u);
+                atomicMin(w + 1, fkey(l[0]));
+                atomicMin(w + 2, fkey(l[1]));
+                atomicMin(w + 3, fkey(l[2]));
+                atomicMax(w + 4, fkey(h[0]));
+                atomicMax(w + 5, fkey(h[1]));
+                atomicMax(w + 6, fkey(h[2]));
+            }
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        uint32_t kind = 1;
+        if (!leaf0) {
+            uint32_t cnt[3];
+            float box[3][6];
+            bool axis_ok[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const uint32_t* bw = L.bins + (a * 32 + lane) * 7;
+                cnt[a] = bw[0];
+                for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
+                axis_ok[a] = !(ext[a] == 0.0f);
+            }
+            Cand best;
+            binned_candidates(cnt, box, axis_ok, B, n, surface_area6(nb), P, lane, best);
+            const uint64_t wk = warp_min_key(best.key);
+            const uint32_t wlo = static_cast<uint32_t>(wk);
+            if (wlo == kNoKey) {
+                kind = n > P.max_leaf ? 2u : 1u;
+            } else {
+                const uint32_t sb = wlo & 0xFFu;
+                Cand win = best;
+                shfl_cand(win, sb);
+                kind = (n <= P.max_leaf && funkey(static_cast<uint32_t>(wk >> 32)) >= leaf_cost(n)) ? 1u : 0u;
+                if (lane == 0) {
+                    L.axis = (wlo >> 8) & 3u;
+                    L.split_bin = sb;
+                    L.n_lt = win.n_lt;
+                    for (int i = 0; i < 6; ++i) {
+                        L.ltb[i] = win.lt[i];
+                        L.gtb[i] = win.gt[i];
+                    }
+                }
+            }
+        }
+        if (lane == 0) {
+            L.kind = kind;
+            L.bad = 0;
+        }
+        if (lane < 12) L.keys[lane] = ((lane % 6) < 3) ? kKeyPosInf : kKeyNegInf;
+    }
+    __syncthreads();
+    const uint32_t kind = L.kind;
+    if (kind == 2) {  // the forced median: after the launch, by the median passes
+        if (tid == 0) {
+            const uint32_t mi = atomicAdd(&O.ctr->n_med, 1u);
+            if (mi < Q.med_cap)
+                Q.med[mi] = t;
+            else
+                set_error(O.ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
+        }
+        return;
+    }
+    if (kind == 1) {  // a leaf of all n objects, in list order
+        if (warp == 0) warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, n, 0u, lane);
+        for (uint32_t i = tid; i < n; i += blockDim.x) O.perm[t.start + i] = __float_as_uint(__ldcg(&src[i].lo).w);
+        if (tid == 0) {
+            atomicAdd(&O.ctr->holes, 1u);
+            if (t.depth == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+        }
+        return;
+    }
+    // stable partition: chunks of 4 records per thread; warp w holds records
+    // w*128 .. w*128+127 of the chunk, 32 at a time
+    const uint32_t axis = L.axis, split_bin = L.split_bin, n_lt = L.n_lt;
+    const float cmin = sel3(cmn, axis), ex = sel3(ext, axis);
+    const uint32_t n_gt = n - n_lt;
+    const uint32_t d1 = t.depth + 1u;
+    const bool leaf_lt = n_lt <= 1u || d1 == P.max_depth || (n_lt <= P.max_leaf && n_lt < 2u * P.min_leaf);
+    const bool leaf_gt = n_gt <= 1u || d1 == P.max_depth || (n_gt <= P.max_leaf && n_gt < 2u * P.min_leaf);
+    const uint32_t below = (1u << lane) - 1u;
+    float ltb[6], gtb[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        ltb[i] = L.ltb[i];
+        gtb[i] = L.gtb[i];
+    }
+    uint32_t k[12];
+    init_key12(k);
+    bool bad = false;
+    uint32_t run_lt = 0, run_gt = 0;
+    constexpr uint32_t kPer = 4, kChunk = kMediumThreads * kPer;
+    for (uint32_t base = 0; base < n; base += kChunk) {
+        Rec r[kPer];
+        uint32_t bal[kPer], vm[kPer];
+        uint32_t lw = 0, nw = 0;
+#pragma unroll
+        for (uint32_t g = 0; g < kPer; ++g) {
+            const uint32_t i = base + warp * (32u * kPer) + g * 32u + lane;
+            bool pred = false;
+            if (i < n) {
+                r[g] = ldcg_rec(src + i);
+                // selects, not a run-time index into r (which would put it in local memory)
+                const float la = axis == 0 ? r[g].lo.x : (axis == 1 ? r[g].lo.y : r[g].lo.z);
+                const float ha = axis == 0 ? r[g].hi.x : (axis == 1 ? r[g].hi.y : r[g].hi.z);
+                pred = bin_of(center_of(la, ha), cmin, ex, B) < split_bin;
+            }
+            bal[g] = __ballot_sync(kFull, pred);
+            vm[g] = __ballot_sync(kFull, i < n);
+            lw += __popc(bal[g]);
+            nw += __popc(vm[g]);
+        }
+        if (lane == 0) {
+            L.wlt[warp] = lw;
+            L.wn[warp] = nw;
+        }
+        __syncthreads();
+        uint32_t lt_before = 0, gt_before = 0, lt_tot = 0, n_tot = 0;
+#pragma unroll
+        for (uint32_t q = 0; q < kMediumWarps; ++q) {
+            const uint32_t a = L.wlt[q], b = L.wn[q];
+            lt_before += q < warp ? a : 0u;
+            gt_before += q < warp ? b - a : 0u;
+            lt_tot += a;
+            n_tot += b;
+        }
+        uint32_t lt_run = run_lt + lt_before, gt_run = run_gt + gt_before;
+#pragma unroll
+        for (uint32_t g = 0; g < kPer; ++g) {
+            const bool valid = (vm[g] >> lane) & 1u;
+            if (valid) {
+                const bool pred = (bal[g] >> lane) & 1u;
+                const uint32_t dest = pred ? lt_run + __popc(bal[g] & below)
+                                           : n_lt + gt_run + __popc(vm[g] & ~bal[g] & below);
+                if (dest < n) {
+                    dst[dest] = r[g];
+                    if (pred ? leaf_lt : leaf_gt) O.perm[t.start + dest] = __float_as_uint(r[g].lo.w);
+                } else {
+                    bad = true;
+                }
+                const float c[3] = {center_of(r[g].lo.x, r[g].hi.x), center_of(r[g].lo.y, r[g].hi.y),
+                                    center_of(r[g].lo.z, r[g].hi.z)};
+                bad |= !box_contains2(ltb, gtb, pred, c[0], c[1], c[2]);
+                grow_keys12(k, pred, c);
+            }
+            lt_run += __popc(bal[g]);
+            gt_run += __popc(vm[g] & ~bal[g]);
+        }
+        run_lt += lt_tot;
+        run_gt += n_tot - lt_tot;
+        __syncthreads();  // wlt/wn are rewritten by the next chunk
+    }
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+        const bool is_min = (q % 6) < 3;
+        const uint32_t v = is_min ? __reduce_min_sync(kFull, k[q]) : __reduce_max_sync(kFull, k[q]);
+        if (lane == 0) {
+            if (is_min)
+                atomicMin(&L.keys[q], v);
+            else
+                atomicMax(&L.keys[q], v);
+        }
+    }
+    if (__any_sync(kFull, bad) && lane == 0) L.bad = 1;
+    __threadfence();  // the records and leaf entries before the children are pushed
+    __syncthreads();
+    if (warp != 0) return;
+    if (run_lt != n_lt || L.bad) {
+        if (lane == 0) set_error(O.ctr, MGBVH_ERR_ASSERT, run_lt != n_lt ? kSiteCount : kSiteContain);
+        return;
+    }
+    warp_store_node(O, t.nbase + t.slot, nb, t.start - t.tbase, n, t.pair, lane);
+    if (lane == 0) atomicMax(&O.ctr->height, t.depth);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {  // [0] gt, [1] lt, as the reference pushes them
+        const uint32_t len = c == 0 ? n_gt : n_lt;
+        const uint32_t start = c == 0 ? t.start + n_lt : t.start;
+        const uint32_t slot = c == 0 ? t.pair : t.pair + 1u;
+        float cb[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) cb[i] = c == 0 ? gtb[i] : ltb[i];
+        if (c == 0 ? leaf_gt : leaf_lt) {
+            warp_store_node(O, t.nbase + slot, cb, start - t.tbase, len, 0u, lane);
+            if (lane == 0 && len > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (d1 == P.max_depth) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+            continue;
+        }
+        if (lane == 0) {
+            Task ct;
+            for (int a = 0; a < 3; ++a) {
+                ct.lo[a] = cb[a];
+                ct.hi[a] = cb[3 + a];
+            }
+            ct.start = start;
+            ct.len = len;
+            ct.slot = slot;
+            ct.pair = c == 0 ? t.pair + 2u : t.pair + 2u * n_gt;
+            ct.depth = d1;
+            ct.buf = t.buf ^ 1u;
+            ct.tile0 = ct.ntiles = 0;
+            ct.nbase = t.nbase;
+            ct.tbase = t.tbase;
+            if (len <= kSmallMax)
+                queue_push_small(Q, ct, O.ctr);
+            else
+                queue_push_main(Q, ct, len > P.medium_max ? L.keys + (c == 0 ? 6 : 0) : nullptr, O.ctr);
+        }
+    }
+}
+
+template <uint32_t kCap, bool kLevels>
+__global__ void __launch_bounds__(kMediumThreads, MGBVH_QUEUE_MIN_BLOCKS) queue_build_kernel(QueueArgs Q, Rec* rec0, Rec* rec1, Params P,
+                                                                      Out O) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
+    LargeSmem& L = *reinterpret_cast<LargeSmem*>(smem_raw);  // the same space: one task at a time
+    __shared__ Popped pop;
+    __shared__ XRec xchg[kMediumWarps][32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) pop = queue_pop(Q, O.ctr);
+        __syncthreads();
+        const Popped p = pop;
+        if (p.kind == 0) break;
+        if (p.kind == 1) {
+            const Task t = ldcg_task(Q.q + p.idx);
+            if (t.len > P.medium_max)
+                queue_large_task(Q, L, t, Q.qcb + 6 * p.idx, rec0, rec1, P, O);
+            else
+                medium_task<false, MediumSmemT<kCap>, true>(S, t, rec0, rec1, Q.small, Q.scap, P, O,
+                                                            Learn{nullptr, 0, nullptr, 0, nullptr}, &Q);
+        } else if (warp < p.count) {
+            const Task t = ldcg_task(Q.small + p.idx + warp);
+            const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+            float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+            uint32_t id = 0;
+            if (lane < t.len) {
+                const Rec r = ldcg_rec(src + lane);
+                lo[0] = r.lo.x;
+                lo[1] = r.lo.y;
+                lo[2] = r.lo.z;
+                id = __float_as_uint(r.lo.w);
+                hi[0] = r.hi.x;
+                hi[1] = r.hi.y;
+                hi[2] = r.hi.z;
+            }
+            const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+            if constexpr (kLevels)
+                warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b,
+                                          P, O, xchg[warp]);
+            else
+                warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b, P,
+                                   O, xchg[warp]);
+        }
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) atomicSub(&Q.st->pending, p.kind == 1 ? 1u : p.count);
     }
 }
 
@@ -2397,6 +2912,49 @@ __global__ void init_roots_kernel(const DevMesh* __restrict__ meshes, uint32_t n
     }
 }
 
+// The batch's roots into the queues: main entries (with centroid bound keys)
+// and small entries, ready flags set; leaf roots finished here.
+__global__ void queue_roots_kernel(const DevMesh* __restrict__ meshes, uint32_t nm, const uint32_t* __restrict__ mkeys,
+                                   QueueArgs Q, Out O, uint32_t max_depth, uint32_t medium_max, uint32_t hold) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    if (blockIdx.x == 0 && threadIdx.x == 0 && hold) atomicAdd(&Q.st->pending, hold);
+    for (uint32_t m = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; m < nm; m += nwarps) {
+        const DevMesh& M = meshes[m];
+        if (M.cls > 3) continue;  // empty mesh: nothing to build
+        float b[6];
+        for (int i = 0; i < 6; ++i) b[i] = M.has_bounds ? M.bounds[i] : funkey(mkeys[12 * m + i]);
+        if (M.cls == 0) {
+            warp_store_node(O, M.nbase, b, 0u, M.n, 0u, lane);
+            for (uint32_t i = lane; i < M.n; i += 32) O.perm[M.tbase + i] = i;
+            if (lane == 0 && M.n > 1) {
+                atomicAdd(&O.ctr->holes, 1u);
+                if (max_depth == 0) atomicAdd(&O.ctr->depth_capped, 1u);
+            }
+            continue;
+        }
+        if (lane != 0) continue;
+        Task t;
+        for (int a = 0; a < 3; ++a) {
+            t.lo[a] = b[a];
+            t.hi[a] = b[3 + a];
+        }
+        t.start = M.tbase;
+        t.len = M.n;
+        t.slot = 0;
+        t.pair = 1;
+        t.depth = 0;
+        t.buf = 0;
+        t.tile0 = t.ntiles = 0;
+        t.nbase = M.nbase;
+        t.tbase = M.tbase;
+        if (M.cls == 1)
+            queue_push_small(Q, t, O.ctr);
+        else
+            queue_push_main(Q, t, M.n > medium_max ? mkeys + 12 * m + 6 : nullptr, O.ctr);
+    }
+}
+
 // Compaction of a batch: slot s of mesh m moves to newidx[s] and its child
 // link (local) to newidx[nbase_m + child] - newidx[nbase_m].
 __global__ void compact_batch_kernel(const mgbvh_node* __restrict__ src, const uint32_t* __restrict__ lens,
@@ -2525,6 +3083,15 @@ struct mgbvh_ctx {
     // forced medians of level-pass nodes: the waiting list, its working copy,
     // element offsets, per-node box keys, sort keys/values, flags and scan
     DevBuf med_list, med_work, med_off, med_seg, med_keys[2], med_vals[2], med_flag, med_scan;
+    // persistent batched build (mgbvh_set_batch_mode): main queue entries, their
+    // ready flags and centroid keys, small-queue ready flags, queue state
+    bool batch_queue = false;
+    DevBuf q, qready, qcb, sready, qstate;
+    void* h_qstate = nullptr;  // pinned QueueState of the last launch
+    int queue_ctas[2] = {0, 0};  // resident CTAs of the 512- and 1024-record instances
+    unsigned long long queue_wait_ns = 2000000000ull;
+    uint32_t queue_hold = 0;
+    uint32_t qcap = 0;  // main queue entries of the current batch
     void* pin = nullptr;  // pinned staging of a batch plan
     size_t pin_bytes = 0;
     bool graph_mode = false;
@@ -3242,12 +3809,34 @@ Params params_of(const mgbvh_ctx* ctx, const mgbvh_settings* st) {
     return P;
 }
 
+// Queue capacities of the persistent build for n objects over nm meshes:
+// every pushed task is a distinct node of at least 2 objects whose tasks form
+// a binary tree, so at most n - 1 + nm of them; the small queue holds
+// disjoint subtrees (the small list's bound).
+QueueArgs queue_args(mgbvh_ctx* ctx, const Caps& C) {
+    QueueArgs Q;
+    Q.q = P_<Task>(ctx->q);
+    Q.qready = P_<uint32_t>(ctx->qready);
+    Q.qcb = P_<uint32_t>(ctx->qcb);
+    Q.qcap = ctx->qcap;
+    Q.small = P_<Task>(ctx->small);
+    Q.sready = P_<uint32_t>(ctx->sready);
+    Q.scap = C.small;
+    Q.st = P_<QueueState>(ctx->qstate);
+    Q.med = P_<Task>(ctx->med_list);
+    Q.med_cap = C.tasks;
+    Q.wait_ns = ctx->queue_wait_ns;
+    return Q;
+}
+
 // Device work of a batch on the context's stream. fixed_levels == 0: eager
 // (reads level counts back); > 0: capture form, which also copies the slot
 // array to the caller's outputs and the counters to pinned host memory.
+// queue: the persistent build (one launch over device-side task queues) in
+// place of the level passes and subtree launches.
 int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh_settings* st,
                   uint32_t fixed_levels, mgbvh_node* d_nodes, uint32_t* d_lens, uint32_t* d_perm,
-                  uint32_t& launches, uint32_t& levels, bool direct) {
+                  uint32_t& launches, uint32_t& levels, bool direct, bool queue) {
     const cudaStream_t sm = ctx->stream;
     const uint32_t nm = B.nm, n = B.n;
     const Params P = params_of(ctx, st);
@@ -3281,16 +3870,49 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
         P_<uint32_t>(ctx->mkeys), nm);
     prep_batch_kernel<<<(int)std::min<uint32_t>((n + 255) / 256, 148u * 8u), 256, 0, sm>>>(
         dmesh, P_<uint32_t>(ctx->toff_buf), nm, n, rec0, P_<uint32_t>(ctx->mkeys), d_ctr);
-    init_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
-        dmesh, nm, P_<uint32_t>(ctx->mkeys), P_<Task>(ctx->tasks[0]), P_<uint32_t>(ctx->bins[0]),
-        P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]), P_<uint32_t>(ctx->tile_begin[0]),
-        P_<Task>(ctx->medium), P_<Task>(ctx->small), O, st->max_depth);
-    MG_CUDA(cudaGetLastError());
-    if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
-    launches = 3;
     levels = 0;
-    int rc = run_pipeline(ctx, C, P, O, rec0, rec1, B.n_large > 0, fixed_levels, launches, levels);
-    if (rc != MGBVH_OK) return rc;
+    if (queue) {
+        // the persistent build: roots into the queues, then one launch
+        QueueArgs Q = queue_args(ctx, C);
+        MG_CUDA(cudaMemsetAsync(ctx->qstate.p, 0, sizeof(QueueState), sm));
+        MG_CUDA(cudaMemsetAsync(ctx->qready.p, 0, 4ull * Q.qcap, sm));
+        MG_CUDA(cudaMemsetAsync(ctx->sready.p, 0, 4ull * Q.scap, sm));
+        // queue_hold: tasks counted as pending that never arrive (the test of
+        // the bounded waits: the launch must end with a time-out)
+        queue_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
+            dmesh, nm, P_<uint32_t>(ctx->mkeys), Q, O, st->max_depth, P.medium_max, ctx->queue_hold);
+        MG_CUDA(cudaGetLastError());
+        if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+        const bool small_cap = P.medium_max <= kMediumSmallCap;
+        const bool lv = P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax;
+        const size_t smem = small_cap ? sizeof(MediumSmemSmall) : sizeof(MediumSmem);
+        const int grid = small_cap ? ctx->queue_ctas[0] : ctx->queue_ctas[1];
+        if (small_cap && lv)
+            queue_build_kernel<kMediumSmallCap, true><<<grid, kMediumThreads, smem, sm>>>(Q, rec0, rec1, P, O);
+        else if (small_cap)
+            queue_build_kernel<kMediumSmallCap, false><<<grid, kMediumThreads, smem, sm>>>(Q, rec0, rec1, P, O);
+        else if (lv)
+            queue_build_kernel<kMediumMax, true><<<grid, kMediumThreads, smem, sm>>>(Q, rec0, rec1, P, O);
+        else
+            queue_build_kernel<kMediumMax, false><<<grid, kMediumThreads, smem, sm>>>(Q, rec0, rec1, P, O);
+        MG_CUDA(cudaGetLastError());
+        if (!fixed_levels) {
+            MG_CUDA(cudaEventRecord(ctx->evp[1], sm));
+            MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
+        }
+        launches = 4;
+        MG_CUDA(cudaMemcpyAsync(ctx->h_qstate, ctx->qstate.p, sizeof(QueueState), cudaMemcpyDeviceToHost, sm));
+    } else {
+        init_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
+            dmesh, nm, P_<uint32_t>(ctx->mkeys), P_<Task>(ctx->tasks[0]), P_<uint32_t>(ctx->bins[0]),
+            P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]), P_<uint32_t>(ctx->tile_begin[0]),
+            P_<Task>(ctx->medium), P_<Task>(ctx->small), O, st->max_depth);
+        MG_CUDA(cudaGetLastError());
+        if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
+        launches = 3;
+        int rc = run_pipeline(ctx, C, P, O, rec0, rec1, B.n_large > 0, fixed_levels, launches, levels);
+        if (rc != MGBVH_OK) return rc;
+    }
     if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->ev1, sm));
     if (fixed_levels && !direct) {
         MG_CUDA(cudaMemcpyAsync(d_nodes, ctx->nodes.p, sizeof(mgbvh_node) * (size_t)B.slots,
@@ -3350,6 +3972,21 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         ENS(ctx->rbins, 4ull * kRBinWords * C.tasks);
         ENS(ctx->tile_hist2, 4ull * 34 * C.tiles);
     }
+    // the persistent build: plain builds (the learned form and sample output
+    // run in the level passes) of meshes up to kQueueMaxMesh objects (one CTA
+    // splits a node, so a larger root would lengthen the launch's critical path)
+    uint32_t max_mesh = 0;
+    for (const DevMesh& M : B.hm) max_mesh = std::max(max_mesh, M.n);
+    const bool use_queue = ctx->batch_queue && !ctx->learn_w && !ctx->learn_samples && max_mesh <= kQueueMaxMesh;
+    const uint32_t qcap = 2u * (n / (kSmallMax + 1)) + nm + 8u;
+    if (use_queue) {
+        ENS(ctx->q, sizeof(Task) * (size_t)qcap);
+        ENS(ctx->qready, 4ull * qcap);
+        ENS(ctx->qcb, 24ull * qcap);
+        ENS(ctx->sready, 4ull * C.small);
+        ENS(ctx->qstate, sizeof(QueueState));
+    }
+    ctx->qcap = qcap;
 #undef ENS
     if (B.n_large > C.tasks || B.tiles > C.tiles || B.n_medium > C.medium || B.n_small > C.small)
         return fail(ctx, MGBVH_ERR_CAPACITY, "batch root lists exceed their capacity");
@@ -3372,10 +4009,12 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         unsigned char* pin = static_cast<unsigned char*>(ctx->pin);
         Counters init;
         std::memset(&init, 0, sizeof(init));
-        init.lvl[0][0] = B.n_large;
-        init.lvl[0][1] = B.tiles;
-        init.n_medium = B.n_medium;
-        init.n_small = B.n_small;
+        if (!use_queue) {  // the persistent build pushes its roots itself
+            init.lvl[0][0] = B.n_large;
+            init.lvl[0][1] = B.tiles;
+            init.n_medium = B.n_medium;
+            init.n_small = B.n_small;
+        }
         std::memcpy(pin, &init, sizeof(init));
         std::memcpy(pin + sizeof(Counters), B.hm.data(), sizeof(DevMesh) * (size_t)nm);
         uint32_t* t = reinterpret_cast<uint32_t*>(pin + sizeof(Counters) + sizeof(DevMesh) * (size_t)nm);
@@ -3397,6 +4036,9 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         put(&d_perm, sizeof(d_perm));
         put(&cap, 4);
         put(&ctx->stream, sizeof(ctx->stream));
+        put(&use_queue, sizeof(use_queue));
+        put(&ctx->queue_hold, 4);
+        put(&ctx->queue_wait_ns, sizeof(ctx->queue_wait_ns));
     }
     uint32_t launches = 0, levels = 0;
     bool done = false;
@@ -3417,11 +4059,18 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
             levels = ctx->graph_levels;
         }
     }
+    auto queue_timed_out = [&]() {
+        return use_queue && static_cast<const QueueState*>(ctx->h_qstate)->timeouts != 0;
+    };
+    if (done && queue_timed_out()) done = false;
     if (!done) {
         if ((rc = enqueue_batch(ctx, B, C, st, 0, d_nodes, d_lens, d_perm, launches, levels,
-                                cap >= B.slots)) != MGBVH_OK)
+                                cap >= B.slots, use_queue)) != MGBVH_OK)
             return rc;
         MG_CUDA(cudaStreamSynchronize(sm));
+        if (queue_timed_out())
+            return fail(ctx, MGBVH_ERR_TIMEOUT,
+                        "a wait of the persistent batched build ran out (no task arrived within the wait limit)");
         if (!ctx->h_ctr->error && ctx->h_ctr->n_med) {
             // level-pass nodes that need the forced median
             had_medians = true;
@@ -3506,7 +4155,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         if (cudaStreamBeginCapture(sm, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             cudaGetLastError();
         } else {
-        const int erc = enqueue_batch(ctx, B, C, st, fixed, d_nodes, d_lens, d_perm, gl, glev, true);
+        const int erc = enqueue_batch(ctx, B, C, st, fixed, d_nodes, d_lens, d_perm, gl, glev, true, use_queue);
         const cudaError_t ce = cudaStreamEndCapture(sm, &g);
         if (erc == MGBVH_OK && ce == cudaSuccess && g) {
             if (cudaGraphInstantiate(&ctx->graph_exec, g, 0) == cudaSuccess) {
@@ -3746,9 +4395,11 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->toff_buf, &ctx->noff_buf, &ctx->mkeys, &ctx->learn_wt, &ctx->lref,
                      &ctx->rbins, &ctx->tile_hist2, &ctx->med_list, &ctx->med_work, &ctx->med_off,
                      &ctx->med_seg, &ctx->med_keys[0], &ctx->med_keys[1], &ctx->med_vals[0],
-                     &ctx->med_vals[1], &ctx->med_flag, &ctx->med_scan};
+                     &ctx->med_vals[1], &ctx->med_flag, &ctx->med_scan, &ctx->q, &ctx->qready,
+                     &ctx->qcb, &ctx->sready, &ctx->qstate};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
+    if (ctx->h_qstate) cudaFreeHost(ctx->h_qstate);
     if (ctx->h_ctr) cudaFreeHost(ctx->h_ctr);
     if (ctx->h_init) cudaFreeHost(ctx->h_init);
     if (ctx->pin) cudaFreeHost(ctx->pin);
@@ -3909,6 +4560,48 @@ int mgbvh_set_tuning(mgbvh_ctx* ctx, uint32_t medium_max) {
     if (medium_max < kSmallMax + 1 || medium_max > kMediumMax)
         return fail(ctx, MGBVH_ERR_UNSUPPORTED, "medium_max must be 33..1024");
     ctx->medium_max = medium_max;
+    return MGBVH_OK;
+}
+
+int mgbvh_set_batch_mode(mgbvh_ctx* ctx, int mode) {
+    int rc = check_ctx(ctx);
+    if (rc) return rc;
+    if (mode != MGBVH_BATCH_LEVELS && mode != MGBVH_BATCH_QUEUE)
+        return fail(ctx, MGBVH_ERR_INVALID_ARG, "batch mode must be MGBVH_BATCH_LEVELS or MGBVH_BATCH_QUEUE");
+    if (mode == MGBVH_BATCH_QUEUE && !ctx->queue_ctas[0]) {
+        // shared-memory limits and resident CTAs of the persistent kernel's instances
+        const int s_small = (int)sizeof(MediumSmemSmall), s_big = (int)sizeof(MediumSmem);
+        MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumSmallCap, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, s_small));
+        MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumSmallCap, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, s_small));
+        MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumMax, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, s_big));
+        MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumMax, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, s_big));
+        int o[4] = {0, 0, 0, 0};
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[0], queue_build_kernel<kMediumSmallCap, true>,
+                                                              kMediumThreads, s_small));
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[1], queue_build_kernel<kMediumSmallCap, false>,
+                                                              kMediumThreads, s_small));
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[2], queue_build_kernel<kMediumMax, true>,
+                                                              kMediumThreads, s_big));
+        MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o[3], queue_build_kernel<kMediumMax, false>,
+                                                              kMediumThreads, s_big));
+        if (!ctx->h_qstate) MG_CUDA(cudaMallocHost(&ctx->h_qstate, sizeof(QueueState)));
+        std::memset(ctx->h_qstate, 0, sizeof(QueueState));
+        // a grid no larger than what is resident at once: every CTA polls
+        ctx->queue_ctas[0] = ctx->sm_count * std::max(1, std::min(o[0], o[1]));
+        ctx->queue_ctas[1] = ctx->sm_count * std::max(1, std::min(o[2], o[3]));
+    }
+    ctx->batch_queue = mode == MGBVH_BATCH_QUEUE;
+    return MGBVH_OK;
+}
+
+int mgbvh_set_queue_limits(mgbvh_ctx* ctx, uint32_t wait_microseconds, uint32_t held_tasks) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    ctx->queue_wait_ns = wait_microseconds ? 1000ull * wait_microseconds : 2000000000ull;
+    ctx->queue_hold = held_tasks;
     return MGBVH_OK;
 }
 
