@@ -58,6 +58,8 @@ def parse_args():
                    help="icosphere: the headline build; mixed: 16.8M-triangle scene + 8M rays")
     p.add_argument("--mixed-scale", type=int, default=1,
                    help="divide the mixed scene and its ray count by this factor")
+    p.add_argument("--batch-mode", default="both", choices=["levels", "queue", "both"],
+                   help="batched workload: level passes, the persistent queue launch, or both (the faster leads)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-e2e", action="store_true", help="skip the host-pointer (e2e) leg")
     p.add_argument("--profile-steps", type=int, default=None, help=argparse.SUPPRESS)
@@ -286,8 +288,7 @@ def run_ours(args):
     settings = BvhSettings(name="bench", bounds=bounds, max_depth=32)
     ctx = _lib.Context(local)
     from marigold_b200 import autotune
-    medium_max = autotune.choice("icosphere_l8", "medium_max", 1024)  # speed only; same tree
-    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
+    tuned = autotune.apply(ctx, "icosphere_l8")  # switch-over and block size: speed only, same tree
     dv = torch.from_numpy(v).cuda()
     dt = torch.from_numpy(t.view(np.int32)).cuda()
     cap = 2 * n - 1
@@ -436,7 +437,8 @@ def run_ours(args):
         "config": {"workload": WORKLOAD, "triangles": n, "vertices": int(v.shape[0]),
                    "min_leaf": 1, "max_leaf": 1, "max_depth": 32, "bins": 32,
                    "adaptive_max_n": 32, "parallelism": f"replicas x{world}",
-                   "l2": "flushed before every step (256 MiB write, outside the timed interval)"},
+                   "l2": "flushed before every step (256 MiB write, outside the timed interval)",
+                   "tuning": tuned},
         "e2e": {"value": round(whole_job_rate(n, world, e2e_step), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": round(e2e_step, 4)},
@@ -630,7 +632,10 @@ def run_batched(args):
     of the mesh bounds), all 513 trees in one batched build. A step computes
     the instance boxes on the GPU from the meshes' bounds and the instances'
     f32 transforms, then builds all trees; the first build runs eagerly and
-    captures a CUDA graph, timed builds replay the graph."""
+    captures a CUDA graph, timed builds replay the graph. Both batch modes are
+    timed (level passes + subtree launches; one persistent launch over
+    device-side task queues), their trees compared, and the faster one leads
+    the line. Then closest-hit rays through the built two-level scene."""
     import torch
     from marigold_b200 import BvhSettings, _lib, autotune, build_batch_device, synth
     torch.cuda.set_device(0)
@@ -638,10 +643,9 @@ def run_batched(args):
     meshes, bounds, inst = synth.batched_scene()
     ids, xf = synth.scene_instances(3, len(meshes), inst.shape[0])
     gen_s = time.perf_counter() - t0
-    medium_max = autotune.choice("batched_scene", "medium_max", 1024)
-    bins = autotune.choice("batched_scene", "bins", 0)
     ctx = _lib.Context(0)
-    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
+    tuned = autotune.apply(ctx, "batched_scene")
+    medium_max, bins = tuned["medium_max"], tuned["bins"]
     ctx.check(ctx.L.mgbvh_set_graph_capture(ctx.ptr, 1))
     descs = [{"vertices": torch.from_numpy(v).cuda(), "triangles": torch.from_numpy(t.view(np.int32)).cuda(),
               "bounds": b} for (v, t), b in zip(meshes, bounds)]
@@ -660,25 +664,41 @@ def run_batched(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
     settings = BvhSettings(bins=bins)
-    times, replays, eager_ms = [], 0, None
-    offs = None
-    with ClockSampler(0) as clocks:
-        for k in range(max(args.warmup, 2) + args.steps):
-            flush.fill_(k & 0xFF)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            ctx.set_stream(stream.cuda_stream)
-            instance_aabbs_device(ctx, d_bounds, d_ids, d_xf, d_inst)
-            offs, rc, st = build_batch_device(ctx, settings, descs, nodes, perm, out_lens=lens,
-                                              stream=stream)
-            e1.record(stream)
-            stream.synchronize()
-            if k == 0:
-                eager_ms = e0.elapsed_time(e1)
-            if k >= max(args.warmup, 2):
-                times.append(e0.elapsed_time(e1))
-                replays += st["graph_replay"]
+    modes = {}
+    trees = {}
+    for mode in (["levels", "queue"] if args.batch_mode == "both" else [args.batch_mode]):
+        ctx.set_batch_mode(mode == "queue")
+        times, replays, eager_ms = [], 0, None
+        offs = None
+        with ClockSampler(0) as clocks:
+            for k in range(max(args.warmup, 2) + args.steps):
+                flush.fill_(k & 0xFF)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                ctx.set_stream(stream.cuda_stream)
+                instance_aabbs_device(ctx, d_bounds, d_ids, d_xf, d_inst)
+                offs, rc, st = build_batch_device(ctx, settings, descs, nodes, perm, out_lens=lens,
+                                                  stream=stream)
+                e1.record(stream)
+                stream.synchronize()
+                if k == 0:
+                    eager_ms = e0.elapsed_time(e1)
+                if k >= max(args.warmup, 2):
+                    times.append(e0.elapsed_time(e1))
+                    replays += st["graph_replay"]
+        mms = float(np.mean(times))
+        modes[mode] = {"value": round(total / (mms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms_per_step": round(mms, 3),
+                       "eager_first_build_ms": round(eager_ms, 3), "graph_replays": replays,
+                       "kernel_launches": st["kernel_launches"], "clocks": clocks.summary()}
+        trees[mode] = (offs, nodes.cpu().numpy().copy(), lens.cpu().numpy().copy(), perm.cpu().numpy().copy())
+    if len(trees) == 2:
+        a, b = trees["levels"], trees["queue"]
+        modes["same_trees"] = bool(a[0] == b[0] and all(np.array_equal(x, y) for x, y in zip(a[1:], b[1:])))
+    best = min((m for m in modes if m in ("levels", "queue")), key=lambda m: modes[m]["ms_per_step"])
+    times = [modes[best]["ms_per_step"]]
+    replays, eager_ms = modes[best]["graph_replays"], modes[best]["eager_first_build_ms"]
+    clocks_best = modes[best]["clocks"]
     from marigold_b200.bvh import NODE_DTYPE, sah_cost
     nh = nodes.cpu().numpy().view(NODE_DTYPE)
     lh = lens.cpu().numpy().view(np.uint32)
@@ -721,11 +741,11 @@ def run_batched(args):
                   "traversal": "two-level: TLAS with the world ray, each instance's BLAS in mesh space "
                                "(scene.slang:91-220); one thread per ray, rays sorted"},
         "value": round(total / (ms * 1e-3) / 1e6, 2), "unit": "Mtri/s", "ms_per_step": round(ms, 3),
-        "clocks": clocks.summary(),
+        "clocks": clocks_best, "batch_mode": best, "modes": modes,
         "eager_first_build_ms": round(eager_ms, 3), "graph_replays": replays, "steps": args.steps,
         "config": {"meshes": len(meshes), "triangles": n_tris, "instances": int(inst.shape[0]),
                    "trees": len(meshes) + 1, "nodes": int(offs[-1]), "medium_max": medium_max,
-                   "bins": bins or "reference (32)", "tuning": "marigold_b200/tuning.json"},
+                   "bins": bins or "reference (32)", "tuning": dict(tuned, table="marigold_b200/tuning.json")},
         "sah": {"blas_sum": round(sah_blas, 3), "tlas": round(sah_tlas, 3)},
         "instance_boxes": "computed on the GPU in every step (mgbvh_instance_aabbs_dev); equal to the "
                           "host restatement: " + str(bool(np.array_equal(d_inst.cpu().numpy().view(np.uint32),

@@ -267,6 +267,12 @@ MGBVH_API int mgbvh_set_batch_mode(mgbvh_ctx* ctx, int mode);
    arrive (0 in normal use): with held_tasks > 0 every wait runs out and the
    build returns MGBVH_ERR_TIMEOUT. */
 MGBVH_API int mgbvh_set_queue_limits(mgbvh_ctx* ctx, uint32_t wait_microseconds, uint32_t held_tasks);
+/* Launch shapes of a context, speed only (the trees do not change): threads
+   per CTA of the kernel that builds subtrees of <= 32 objects, one warp each
+   (64, 128 or 256; 0: 256), and persistent CTAs per SM of the
+   MGBVH_BATCH_QUEUE launch (0: as many as fit). The autotuner
+   (marigold_b200/autotune.py) picks them per workload. */
+MGBVH_API int mgbvh_set_launch_shape(mgbvh_ctx* ctx, uint32_t small_threads, uint32_t queue_ctas_per_sm);
 
 /* World AABBs of instances for the TLAS, computed on the GPU as marigold's
    scene upload computes them on the host (marigold/src/app/data/scene/

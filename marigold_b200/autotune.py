@@ -1,14 +1,21 @@
 """Autotuner of the builder's per-workload choices; writes tuning.json.
 
-Two knobs are tuned per workload:
+Knobs tuned per workload:
   * medium_max — the size at which nodes leave the level passes for the
-    per-subtree kernels (33..1024). Every phase computes the same split
-    decisions, so this knob changes speed only, never the tree: the fastest
-    value is always taken.
+    per-subtree kernels (33..1024): the level-to-subtree switch-over.
+  * small_threads — the block size of the kernel that builds subtrees of
+    <= 32 objects, one warp each (64, 128 or 256 threads per CTA).
+  * batch_mode and queue_ctas_per_sm (batched workloads) — level passes and
+    subtree launches, or one persistent launch over device-side task queues
+    with a given number of resident CTAs per SM.
   * bins — the binned-sweep bin count. The reference profile (bins = 0,
     32 bins) is what the crate builds; other counts change the tree. A
     non-reference count is chosen only for workloads that allow it, and only
     when its total SAH cost is within 1% of the reference profile's.
+Every knob but bins changes speed only, never the tree (each phase and
+mode computes the same split decisions): the fastest value is taken, the
+knobs one after another (switch-over, block size, batch mode, persistent
+CTAs per SM, bins), each at the best values found before it.
 
 Each candidate is timed as the median of several builds (CUDA events on the
 build stream, inputs resident on the device, L2 flushed before each build).
@@ -28,7 +35,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.json")
 
 MEDIUM_MAX = (64, 128, 256, 512, 1024)
+SMALL_THREADS = (64, 128, 256)
+QUEUE_CTAS = (1, 2, 3)
 BINS = (0, 8, 16, 24)
+DEFAULTS = {"medium_max": 1024, "small_threads": 256, "batch_mode": "levels", "queue_ctas_per_sm": 0, "bins": 0}
 
 
 def load_table() -> dict:
@@ -39,8 +49,20 @@ def load_table() -> dict:
         return {}
 
 
-def choice(workload: str, key: str, default):
-    return load_table().get(workload, {}).get("choice", {}).get(key, default)
+def choice(workload: str, key: str, default=None):
+    d = DEFAULTS.get(key) if default is None else default
+    return load_table().get(workload, {}).get("choice", {}).get(key, d)
+
+
+def apply(ctx, workload: str) -> dict:
+    """Sets the speed knobs tuning.json holds for `workload` on a context;
+    returns the choices (bins included, which the caller passes in its
+    settings)."""
+    c = {k: choice(workload, k) for k in DEFAULTS}
+    ctx.set_tuning(int(c["medium_max"]))
+    ctx.set_launch_shape(int(c["small_threads"]), int(c["queue_ctas_per_sm"]))
+    ctx.set_batch_mode(c["batch_mode"] == "queue")
+    return c
 
 
 def _workloads():
@@ -48,25 +70,27 @@ def _workloads():
 
     def icosphere():
         v, t = synth.config2_mesh()
-        return [{"v": v, "t": t, "bounds": synth.mesh_bounds(v)}], False
+        return [{"v": v, "t": t, "bounds": synth.mesh_bounds(v)}], False, False
 
     def batched():
         meshes, bounds, inst = synth.batched_scene()
         ms = [{"v": v, "t": t, "bounds": b} for (v, t), b in zip(meshes, bounds)]
         ms.append({"aabbs": inst})
-        return ms, True
+        return ms, True, True
 
     def mixed():
         v, t = synth.mixed_scene()
-        return [{"v": v, "t": t, "bounds": None}], False
+        return [{"v": v, "t": t, "bounds": None}], False, False
 
     return {"icosphere_l8": icosphere, "batched_scene": batched, "mixed_scene": mixed}
 
 
-def _measure(ctx, meshes, medium_max, bins, reps=5):
+def _measure(ctx, meshes, knobs, reps=5):
     import torch
     from . import BvhSettings, build_batch_device
-    ctx.check(ctx.L.mgbvh_set_tuning(ctx.ptr, medium_max))
+    ctx.set_tuning(knobs["medium_max"])
+    ctx.set_launch_shape(knobs["small_threads"], knobs["queue_ctas_per_sm"])
+    ctx.set_batch_mode(knobs["batch_mode"] == "queue")
     descs = []
     for m in meshes:
         if "aabbs" in m:
@@ -86,7 +110,7 @@ def _measure(ctx, meshes, medium_max, bins, reps=5):
         flush.fill_(k & 0xFF)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        offs, rc, st = build_batch_device(ctx, BvhSettings(bins=bins), descs, nodes, perm,
+        offs, rc, st = build_batch_device(ctx, BvhSettings(bins=knobs["bins"]), descs, nodes, perm,
                                           out_lens=lens, stream=stream)
         e1.record(stream)
         torch.cuda.synchronize()
@@ -106,7 +130,7 @@ def tune(names):
     table = load_table()
     ctx = _lib.Context(0)
     for name in names:
-        meshes, bins_free = _workloads()[name]()
+        meshes, bins_free, batched = _workloads()[name]()
         for m in meshes:
             if "aabbs" in m:
                 m["dev_aabbs"] = torch.from_numpy(m["aabbs"]).cuda()
@@ -116,27 +140,43 @@ def tune(names):
                 m["dev_t"] = torch.from_numpy(m["t"].view(np.int32)).cuda()
                 m["n"] = m["t"].shape[0]
         rows = []
-        for mm in MEDIUM_MAX:
-            ms, sah = _measure(ctx, meshes, mm, 0)
-            rows.append({"medium_max": mm, "bins": 0, "ms": round(ms, 4), "sah": sah})
+        best = dict(DEFAULTS)
+
+        def trial(**change):
+            k = dict(best, **change)
+            ms, sah = _measure(ctx, meshes, k)
+            rows.append(dict(k, ms=round(ms, 4), sah=sah))
             print(name, rows[-1], file=sys.stderr, flush=True)
-        best_ref = min((r for r in rows if r["bins"] == 0), key=lambda r: r["ms"])
-        ref_sah = best_ref["sah"]
-        chosen = dict(best_ref)
+            return rows[-1]
+
+        def pick(key, values):
+            cands = [trial(**{key: v}) for v in values]
+            top = min(cands, key=lambda r: r["ms"])
+            best[key] = top[key]
+            return top
+
+        pick("medium_max", MEDIUM_MAX)
+        pick("small_threads", SMALL_THREADS)
+        if batched:
+            pick("batch_mode", ("levels", "queue"))
+            if best["batch_mode"] == "queue":
+                pick("queue_ctas_per_sm", QUEUE_CTAS + (0,))
+        ref = min((r for r in rows if r["bins"] == 0), key=lambda r: r["ms"])
+        ref_sah = ref["sah"]
+        chosen_ms = ref["ms"]
         if bins_free:
             for b in BINS[1:]:
-                ms, sah = _measure(ctx, meshes, best_ref["medium_max"], b)
-                rows.append({"medium_max": best_ref["medium_max"], "bins": b, "ms": round(ms, 4),
-                             "sah": sah})
-                print(name, rows[-1], file=sys.stderr, flush=True)
-                if sah <= 1.01 * ref_sah and ms < chosen["ms"]:
-                    chosen = dict(rows[-1])
+                r = trial(bins=b)
+                if r["sah"] <= 1.01 * ref_sah and r["ms"] < chosen_ms:
+                    best["bins"] = b
+                    chosen_ms = r["ms"]
         table[name] = {
-            "choice": {"medium_max": chosen["medium_max"], "bins": chosen["bins"]},
+            "choice": dict(best),
             "reference_profile_sah": ref_sah,
             "candidates": rows,
-            "rule": ("fastest medium_max (tree unchanged); bins other than the reference "
-                     "profile only where allowed and within 1% of its SAH")
+            "rule": ("knobs that leave the tree unchanged (medium_max, small_threads, batch_mode, "
+                     "queue_ctas_per_sm): the fastest, one knob after another; bins other than the "
+                     "reference profile only where allowed and within 1% of its SAH")
                     + ("" if bins_free else "; bins fixed to the reference profile"),
             "measured": time.strftime("%Y-%m-%d"),
         }

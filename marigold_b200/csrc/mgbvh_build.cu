@@ -2194,7 +2194,8 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t w0 = range ? range[0] : 0u;
     const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
-    for (uint32_t w = w0 + blockIdx.x * 8 + wib; w < n_tasks; w += gridDim.x * 8) {
+    const uint32_t wpb = blockDim.x >> 5;  // warps per CTA (64..256 threads)
+    for (uint32_t w = w0 + blockIdx.x * wpb + wib; w < n_tasks; w += gridDim.x * wpb) {
         const Task t = tasks[w];
         const Rec* src = (t.buf ? rec1 : rec0) + t.start;
         float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
@@ -3092,6 +3093,10 @@ struct mgbvh_ctx {
     unsigned long long queue_wait_ns = 2000000000ull;
     uint32_t queue_hold = 0;
     uint32_t qcap = 0;  // main queue entries of the current batch
+    // launch shapes (mgbvh_set_launch_shape; speed only): threads per CTA of
+    // the warp-subtree kernel, persistent CTAs per SM (0: as many as fit)
+    uint32_t small_threads = 256;
+    uint32_t queue_per_sm = 0;
     void* pin = nullptr;  // pinned staging of a batch plan
     size_t pin_bytes = 0;
     bool graph_mode = false;
@@ -3332,6 +3337,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
         // small subtrees: count read on the device; grid sized for full occupancy
         auto small = (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax) ? small_kernel<true>
                                                                               : small_kernel<false>;
+        // as many warps as 8 CTAs of 256 threads per SM, whatever the CTA size
+        const int small_grid = ctx->sm_count * (2048 / (int)ctx->small_threads);
         if (ctx->stream_slots && ctx->h_nodes_out) {
             // streamed output: the subtrees of both kinds run chunk by chunk
             // of node slots (the chunk of their children pair): chunk c's
@@ -3351,7 +3358,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 medium(P_<Task>(ctx->medium2), d_ctr->mrange + c);
                 small_select_kernel<<<ctx->sm_count, 256, 0, sm>>>(P_<Task>(ctx->small), P_<Task>(ctx->small2),
                                                                    C.small, O, c, S);
-                small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small2), rec0, rec1, P, O,
+                small<<<small_grid, ctx->small_threads, 0, sm>>>(P_<Task>(ctx->small2), rec0, rec1, P, O,
                                                          d_ctr->srange + c);
                 launches += 3;
                 MG_CUDA(cudaEventRecord(ctx->evs[c], sm));
@@ -3369,7 +3376,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             medium(P_<Task>(ctx->medium), nullptr);
             launches++;
             if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
-            small<<<ctx->sm_count * 8, 256, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
+            small<<<small_grid, ctx->small_threads, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
             launches++;
         }
         MG_CUDA(cudaGetLastError());
@@ -3886,7 +3893,8 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
         const bool small_cap = P.medium_max <= kMediumSmallCap;
         const bool lv = P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax;
         const size_t smem = small_cap ? sizeof(MediumSmemSmall) : sizeof(MediumSmem);
-        const int grid = small_cap ? ctx->queue_ctas[0] : ctx->queue_ctas[1];
+        int grid = small_cap ? ctx->queue_ctas[0] : ctx->queue_ctas[1];
+        if (ctx->queue_per_sm) grid = std::min(grid, ctx->sm_count * (int)ctx->queue_per_sm);
         if (small_cap && lv)
             queue_build_kernel<kMediumSmallCap, true><<<grid, kMediumThreads, smem, sm>>>(Q, rec0, rec1, P, O);
         else if (small_cap)
@@ -4039,6 +4047,8 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         put(&use_queue, sizeof(use_queue));
         put(&ctx->queue_hold, 4);
         put(&ctx->queue_wait_ns, sizeof(ctx->queue_wait_ns));
+        put(&ctx->small_threads, 4);
+        put(&ctx->queue_per_sm, 4);
     }
     uint32_t launches = 0, levels = 0;
     bool done = false;
@@ -4595,6 +4605,16 @@ int mgbvh_set_batch_mode(mgbvh_ctx* ctx, int mode) {
         ctx->queue_ctas[1] = ctx->sm_count * std::max(1, std::min(o[2], o[3]));
     }
     ctx->batch_queue = mode == MGBVH_BATCH_QUEUE;
+    return MGBVH_OK;
+}
+
+int mgbvh_set_launch_shape(mgbvh_ctx* ctx, uint32_t small_threads, uint32_t queue_ctas_per_sm) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (small_threads == 0) small_threads = 256;
+    if (small_threads != 64 && small_threads != 128 && small_threads != 256)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "small_threads must be 64, 128 or 256");
+    ctx->small_threads = small_threads;
+    ctx->queue_per_sm = queue_ctas_per_sm;
     return MGBVH_OK;
 }
 
