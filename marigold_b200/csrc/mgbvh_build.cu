@@ -337,6 +337,11 @@ constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 #ifndef MGBVH_BIN_MIN_BLOCKS
 #define MGBVH_BIN_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
 #endif
+#ifndef MGBVH_BIN_BATCH
+#define MGBVH_BIN_BATCH 8  // records a thread loads before binning them (tuning knob; divides 8)
+#endif
+constexpr uint32_t kBinBatch = MGBVH_BIN_BATCH;
+static_assert(kRecsPerThread % kBinBatch == 0, "the bin batch divides the records per thread");
 #ifndef MGBVH_PART_UNROLL
 #define MGBVH_PART_UNROLL 1  // records in flight per lane in the scatter pass (tuning knob; 1 / 2 / 4: 681 / 676 / 680 Mtri/s)
 #endif
@@ -365,32 +370,36 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_ke
             cmn[a] = funkey(cbkeys[6 * ti + a]);
             ext[a] = __fsub_rn(funkey(cbkeys[6 * ti + 3 + a]), cmn[a]);
         }
-        float4 rl[kRecsPerThread], rh[kRecsPerThread];
+        // records loaded kBinBatch at a time, then binned
 #pragma unroll
-        for (uint32_t k = 0; k < kRecsPerThread; ++k) {
-            const uint32_t i = threadIdx.x + k * kTileThreads;
-            if (i < cnt) {
-                rl[k] = src[i].lo;
-                rh[k] = src[i].hi;
+        for (uint32_t k0 = 0; k0 < kRecsPerThread; k0 += kBinBatch) {
+            float4 rl[kBinBatch], rh[kBinBatch];
+#pragma unroll
+            for (uint32_t k = 0; k < kBinBatch; ++k) {
+                const uint32_t i = threadIdx.x + (k0 + k) * kTileThreads;
+                if (i < cnt) {
+                    rl[k] = src[i].lo;
+                    rh[k] = src[i].hi;
+                }
             }
-        }
-        __syncthreads();
+            if (k0 == 0) __syncthreads();  // the tile's bins are initialized
 #pragma unroll
-        for (uint32_t k = 0; k < kRecsPerThread; ++k) {
-            if (threadIdx.x + k * kTileThreads >= cnt) break;
-            const float l[3] = {rl[k].x, rl[k].y, rl[k].z}, h[3] = {rh[k].x, rh[k].y, rh[k].z};
+            for (uint32_t k = 0; k < kBinBatch; ++k) {
+                if (threadIdx.x + (k0 + k) * kTileThreads >= cnt) break;
+                const float l[3] = {rl[k].x, rl[k].y, rl[k].z}, h[3] = {rh[k].x, rh[k].y, rh[k].z};
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (ext[a] == 0.0f) continue;  // block-uniform
-                const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
-                uint32_t* w = sb + (a * 32 + b) * 7;
-                atomicAdd(w, 1u);
-                atomicMin(w + 1, fkey(l[0]));
-                atomicMin(w + 2, fkey(l[1]));
-                atomicMin(w + 3, fkey(l[2]));
-                atomicMax(w + 4, fkey(h[0]));
-                atomicMax(w + 5, fkey(h[1]));
-                atomicMax(w + 6, fkey(h[2]));
+                for (int a = 0; a < 3; ++a) {
+                    if (ext[a] == 0.0f) continue;  // block-uniform
+                    const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
+                    uint32_t* w = sb + (a * 32 + b) * 7;
+                    atomicAdd(w, 1u);
+                    atomicMin(w + 1, fkey(l[0]));
+                    atomicMin(w + 2, fkey(l[1]));
+                    atomicMin(w + 3, fkey(l[2]));
+                    atomicMax(w + 4, fkey(h[0]));
+                    atomicMax(w + 5, fkey(h[1]));
+                    atomicMax(w + 6, fkey(h[2]));
+                }
             }
         }
         __syncthreads();
