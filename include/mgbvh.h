@@ -483,6 +483,12 @@ MGBVH_API int mgbvh_mlp_adam_dev(float* d_master, void* d_weights_bf16, const fl
    is positive. The trees then differ from the reference's (the plain split
    is replaced only by an exactly cheaper one). No reference counterpart. */
 MGBVH_API int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gate);
+/* The learned form's cost knobs (no reference counterpart): with the gate on,
+   proposals are scored only where the refine logit exceeds refine_threshold
+   (default 0); nodes of fewer than min_objects objects (default 0) take the
+   plain split without running the network. Higher values build faster and
+   close less of the gap to the full sweep. */
+MGBVH_API int mgbvh_set_proposer_gate(mgbvh_ctx* ctx, float refine_threshold, uint32_t min_objects);
 /* Builds on this context also write one training sample (30 floats: 24
    features, label bits, gain, n, plain cost, full-sweep cost, node start) per
    binned node of 33..8192 objects to d_samples (device, capacity samples) and

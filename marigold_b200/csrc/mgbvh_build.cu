@@ -335,10 +335,10 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
 constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 
 #ifndef MGBVH_BIN_MIN_BLOCKS
-#define MGBVH_BIN_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
+#define MGBVH_BIN_MIN_BLOCKS 4  // CTAs per SM the register budget must allow (tuning knob; 1 / 3 / 4 with batches of 8 / 4 / 4: 682 / 691 / 692 Mtri/s)
 #endif
 #ifndef MGBVH_BIN_BATCH
-#define MGBVH_BIN_BATCH 8  // records a thread loads before binning them (tuning knob; divides 8)
+#define MGBVH_BIN_BATCH 4  // records a thread loads before binning them (tuning knob; divides 8)
 #endif
 constexpr uint32_t kBinBatch = MGBVH_BIN_BATCH;
 static_assert(kRecsPerThread % kBinBatch == 0, "the bin batch divides the records per thread");
@@ -450,6 +450,8 @@ struct EvalArgs {
     // per-task pending proposals, their interval bins and per-tile counts
     const __nv_bfloat16* lw;
     int lgate;
+    float lgate_thr;  // refine-logit threshold of the gate
+    uint32_t lmin_n;  // smallest node that runs the network
     LvlRefine* refine;
     uint32_t* rbins;
     const uint32_t* tile_hist2;  // [proposal * 17 + interval][tile]: objects in intervals 0..interval
@@ -671,7 +673,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         d.ltb[i] = win.lt[i];
         d.gtb[i] = win.gt[i];
     }
-    if (A.lw && B == 32u) {
+    if (A.lw && B == 32u && t.len >= A.lmin_n) {
         // the learned form: run the network; with proposals to score, the
         // decision waits for the refine pass (lvl_eval2_kernel)
         const float cb[6] = {cmn[0], cmn[1], cmn[2], funkey(A.cbkeys[6 * w + 3]),
@@ -681,7 +683,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         int top0 = 0, top1 = 0;
         float refine = 0.0f;
         mgbvh_mlp::warp_forward_t(f, A.lw, lane, top0, top1, refine);
-        const bool on = !A.lgate || refine > 0.0f;
+        const bool on = !A.lgate || refine > A.lgate_thr;
         if (lane == 0) {
             LvlRefine R;
             R.on = on ? 1u : 0u;
@@ -1567,8 +1569,16 @@ __device__ __forceinline__ void warp_reduce_keys12(uint32_t* k) {
 //  * with LN.w: run the network, score 16 thresholds inside each of its two
 //    best (axis, bucket) proposals exactly (one per lane), and replace the
 //    plain split when the best of them costs strictly less.
+#ifndef MGBVH_LEARNED_NODE_INLINE
+#define MGBVH_LEARNED_NODE_INLINE 0  // 1: inline the learned form's node code into the subtree CTA (tuning knob)
+#endif
+#if MGBVH_LEARNED_NODE_INLINE
+#define MGBVH_LEARNED_NODE_ATTR __forceinline__
+#else
+#define MGBVH_LEARNED_NODE_ATTR __noinline__
+#endif
 template <class MS>
-__device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Params& P,
+__device__ MGBVH_LEARNED_NODE_ATTR void learned_node(const MS& S, const Learn& LN, const Params& P,
                                           const MNode& nd, uint32_t ib, uint32_t base, uint32_t s,
                                           uint32_t n, uint32_t depth, uint32_t tbase,
                                           const uint32_t* cnt, const float* ext,
@@ -1630,11 +1640,11 @@ __device__ __noinline__ void learned_node(const MS& S, const Learn& LN, const Pa
             write_sample(LN, f, bk, ba, bthr, ba < 3 ? sel3(nd.cb, ba) : 0.0f, ba < 3 ? sel3(ext, ba) : 0.0f,
                          plain_ck, n, base + s - tbase);
     }
-    if (LN.w) {
+    if (LN.w && n >= LN.min_n) {
         int top0 = 0, top1 = 0;
         float refine = 0.0f;
         mgbvh_mlp::warp_forward_t(f, LN.w, lane, top0, top1, refine);
-        if (!LN.gate || refine > 0.0f) {
+        if (!LN.gate || refine > LN.gate_thr) {
             // Interval bins (the warp's bin area is free once the binned
             // candidates are in registers): every object goes to the interval
             // of its centroid among each proposal's 16 thresholds; lane
@@ -3117,6 +3127,8 @@ struct mgbvh_ctx {
     const void* learn_w = nullptr;
     DevBuf learn_wt, lref, rbins, tile_hist2;  // level-pass refine state (learned form)
     int learn_gate = 1;
+    float learn_gate_thr = 0.0f;  // mgbvh_set_proposer_gate
+    uint32_t learn_min_n = 0;
     float* learn_samples = nullptr;
     uint32_t learn_cap = 0;
     uint32_t* learn_count = nullptr;
@@ -3249,6 +3261,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     Learn LN;
     LN.w = static_cast<const __nv_bfloat16*>(ctx->learn_w);
     LN.gate = ctx->learn_gate;
+    LN.gate_thr = ctx->learn_gate_thr;
+    LN.min_n = ctx->learn_min_n;
     LN.samples = ctx->learn_samples;
     LN.cap = ctx->learn_cap;
     LN.count = ctx->learn_count;
@@ -3286,6 +3300,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             A.cap_small = C.small;
             A.lw = LN.w;
             A.lgate = LN.gate;
+            A.lgate_thr = LN.gate_thr;
+            A.lmin_n = LN.min_n;
             A.refine = LN.w ? P_<LvlRefine>(ctx->lref) : nullptr;
             A.rbins = LN.w ? P_<uint32_t>(ctx->rbins) : nullptr;
             A.tile_hist2 = LN.w ? P_<uint32_t>(ctx->tile_hist2) : nullptr;
@@ -4545,6 +4561,19 @@ int mgbvh_set_split_proposer(mgbvh_ctx* ctx, const void* d_weights_bf16, int gat
     MG_CUDA(cudaGetLastError());
     MG_CUDA(cudaStreamSynchronize(ctx->stream));  // the caller's buffer may go after this
     ctx->learn_w = ctx->learn_wt.p;
+    return MGBVH_OK;
+}
+
+int mgbvh_set_proposer_gate(mgbvh_ctx* ctx, float refine_threshold, uint32_t min_objects) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (!(refine_threshold == refine_threshold)) return fail(ctx, MGBVH_ERR_INVALID_ARG, "refine_threshold is NaN");
+    if (ctx->graph_exec) {  // a captured graph holds the old gate
+        cudaGraphExecDestroy(ctx->graph_exec);
+        ctx->graph_exec = nullptr;
+        ctx->graph_sig.clear();
+    }
+    ctx->learn_gate_thr = refine_threshold;
+    ctx->learn_min_n = min_objects;
     return MGBVH_OK;
 }
 

@@ -17,10 +17,12 @@ namespace mgbvh {
 // Learned-form switches of one build.
 struct Learn {
     const __nv_bfloat16* w;  // network parameters; NULL: no proposals
-    int gate;                // 1: refine only where the refine logit is > 0
+    int gate;                // 1: refine only where the refine logit is > gate_thr
     float* samples;          // training-sample output (kSampleWidth floats each); NULL: none
     uint32_t cap;            // sample capacity
     uint32_t* count;         // samples written (device counter)
+    float gate_thr;          // refine-logit threshold of the gate
+    uint32_t min_n;          // nodes of fewer objects take the plain split without the network
 };
 
 constexpr int kSampleWidth = 30;  // 24 features, label bits, gain, n, plain cost, full cost, start

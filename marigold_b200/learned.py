@@ -38,15 +38,26 @@ def _vp(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-def training_mesh(k: int, seed: int):
-    """Mesh k of a training stream: alternately random small triangles
-    (65,536 / 262,144 / 1,048,576) and noisy icospheres (levels 6 / 7 / 8),
-    each with its own seed."""
+TRAINING_KINDS = ("random", "icosphere", "mixed")
+
+
+def training_mesh(k: int, seed: int, kinds=TRAINING_KINDS):
+    """Mesh k of a training stream, cycling through `kinds`, each mesh with
+    its own seed: random small triangles (65,536 / 262,144 / 1,048,576),
+    noisy icospheres (levels 6 / 7 / 8), and small mixed scenes (Gaussian
+    blobs, a ground grid and long thin triangles, about 0.23M / 0.92M / 1.8M
+    triangles: the large mixed scene's generator at reduced sizes)."""
     from . import synth
     s = seed + 7919 * k
-    if k % 2 == 0:
-        return synth.random_triangles([65536, 262144, 1048576][(k // 2) % 3], seed=s)
-    return synth.noisy_icosphere([6, 7, 8][(k // 2) % 3], seed=s)
+    kind = kinds[k % len(kinds)]
+    size = (k // len(kinds)) % 3
+    if kind == "random":
+        return synth.random_triangles([65536, 262144, 1048576][size], seed=s)
+    if kind == "icosphere":
+        return synth.noisy_icosphere([6, 7, 8][size], seed=s)
+    blob, grid, thin = [(131072, (128, 128), 65536), (524288, (256, 256), 262144),
+                        (1048576, (512, 256), 524288)][size]
+    return synth.mixed_scene(seed=s, n_blob=blob, grid=grid, n_thin=thin)
 
 
 # held-out evaluation meshes (seeds never drawn by training_mesh's streams):

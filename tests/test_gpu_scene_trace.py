@@ -21,6 +21,10 @@ def make_scene(seed=5, n_meshes=10, n_inst=60, lo=20, hi=3000, **kw):
     import torch
     meshes, bounds, _ = synth.batched_scene(seed=seed, n_meshes=n_meshes, n_instances=1, lo=lo, hi=hi)
     ids, xf = synth.scene_instances(seed + 1, n_meshes, n_inst)
+    # translations shrunk from [-100, 100]^3 to [-3, 3]^3: instances of unit-size
+    # meshes crowd together, so most rays meet some of them (and overlap)
+    xf = xf.copy()
+    xf[:, 12:15] *= np.float32(0.03)
     boxes = synth.instance_aabbs(bounds, ids, xf)
     dmeshes = [(torch.from_numpy(v).cuda(), torch.from_numpy(t.view(np.int32)).cuda()) for v, t in meshes]
     descs = [{"vertices": v, "triangles": t, "bounds": b} for (v, t), b in zip(dmeshes, bounds)]
