@@ -1479,6 +1479,26 @@ using MediumSmem = MediumSmemT<kMediumMax>;
 constexpr uint32_t kMediumSmallCap = 512;  // the instance for medium_max <= 512 (more CTAs per SM)
 using MediumSmemSmall = MediumSmemT<kMediumSmallCap>;
 
+// A subtree of <= 32 objects split off inside a subtree CTA of the persistent
+// build: its objects are idx[ob][cs .. cs + len) of the CTA's records, built
+// by the CTA's warps once the CTA's own nodes are done (the range is the
+// subtree's alone, so later partitions leave it as it is).
+struct SmallRef {
+    float b[6];
+    uint32_t slot, pair, depth;
+    uint16_t cs;
+    uint8_t len, ob;
+};
+
+// The persistent build's subtree CTA: the records, lists and bins of a
+// subtree CTA, plus the list of its subtrees of <= 32 objects (at most
+// kCap / 2: disjoint subtrees of at least 2 objects).
+template <uint32_t kCap>
+struct MediumSmemQ : MediumSmemT<kCap> {
+    SmallRef sref[kCap / 2];
+    uint32_t sref_n;
+};
+
 template <class MS>
 __device__ __forceinline__ void medium_load_warp_records(const MS& S, uint32_t ib, uint32_t s,
                                                          uint32_t n, uint32_t lane, float* lo,
@@ -1755,17 +1775,14 @@ __global__ void transpose_weights_kernel(const __nv_bfloat16* __restrict__ w, __
     t[i] = src >= 0 ? w[src] : __float2bfloat16_rn(0.0f);
 }
 
-// The persistent batched build's queues (defined with its kernel below).
-struct QueueArgs;
-__device__ void queue_push_small(const QueueArgs& Q, const Task& t, Counters* ctr);
-
 // One CTA builds the subtree of one medium node (33..1024 objects).
-// kQueue: subtrees of <= 32 objects go to the persistent build's small
-// queue (QA) instead of the small list.
-template <bool kLearn, class MS, bool kQueue = false>
+// kQueue (the persistent batched build): records are read through L2 only,
+// and each subtree of <= 32 objects is built at once by the warp that split
+// it off, from shared memory, instead of going to the small list.
+template <bool kLearn, class MS, bool kQueue = false, bool kSmallLevels = true>
 __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec* rec1,
                                             Task* small, uint32_t cap_small, const Params& P,
-                                            const Out& O, const Learn& LN, const QueueArgs* QA = nullptr) {
+                                            const Out& O, const Learn& LN) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     Rec* src = (t.buf ? rec1 : rec0) + t.start;
     const uint32_t base = t.start;
@@ -1773,6 +1790,9 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
     init_key12(k);
     if (threadIdx.x < 12) S.rootk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
     if (threadIdx.x < 2) S.list_n[threadIdx.x] = 0;
+    if constexpr (kQueue) {
+        if (threadIdx.x == 0) S.sref_n = 0;
+    }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < t.len; i += blockDim.x) {
         const Rec r = load_rec<kQueue>(src + i);
@@ -2017,6 +2037,24 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                         S.list_x[cur ^ 1u][li2].ib = ob;
                     }
                 } else {
+                    if constexpr (kQueue) {
+                        // the persistent build: listed, and built from shared memory
+                        // once the CTA's own nodes are done
+                        uint32_t ri = 0;
+                        if (lane == 0) ri = atomicAdd(&S.sref_n, 1u);
+                        ri = __shfl_sync(kFull, ri, 0);
+                        if (lane == 0) {
+                            SmallRef& q = S.sref[ri];
+                            for (int i = 0; i < 6; ++i) q.b[i] = cbx[i];
+                            q.slot = slot;
+                            q.pair = pair;
+                            q.depth = cdepth;
+                            q.cs = static_cast<uint16_t>(cs);
+                            q.len = static_cast<uint8_t>(len);
+                            q.ob = static_cast<uint8_t>(ob);
+                        }
+                        continue;
+                    }
                     // subtree of <= 32 objects: write its records back to this task's
                     // range of the record buffer and queue it for small_kernel
                     if (lane < len) {
@@ -2025,29 +2063,6 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
                         rr.lo = S.rlo[r];
                         rr.hi = S.rhi[r];
                         src[cs + lane] = rr;
-                    }
-                    if constexpr (kQueue) {
-                        // the records reach memory before the task is marked ready
-                        __threadfence();
-                        __syncwarp();
-                        if (lane == 0) {
-                            Task st;
-                            for (int a = 0; a < 3; ++a) {
-                                st.lo[a] = cbx[a];
-                                st.hi[a] = cbx[3 + a];
-                            }
-                            st.start = base + cs;
-                            st.len = len;
-                            st.slot = slot;
-                            st.pair = pair;
-                            st.depth = cdepth;
-                            st.buf = t.buf;
-                            st.tile0 = st.ntiles = 0;
-                            st.nbase = t.nbase;
-                            st.tbase = t.tbase;
-                            queue_push_small(*QA, st, O.ctr);
-                        }
-                        continue;
                     }
                     uint32_t si = 0;
                     if (lane == 0) si = atomicAdd(&O.ctr->n_small, 1u);
@@ -2079,6 +2094,33 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
     if (lane == 0) {
         if (any_split) atomicMax(&O.ctr->height, hmax);
         if (n_median) atomicAdd(&O.ctr->median_splits, n_median);
+    }
+    if constexpr (kQueue) {
+        // the subtrees of <= 32 objects, one warp each (the loop above ends
+        // after a barrier, so the list is complete)
+        const uint32_t ns = S.sref_n;
+        for (uint32_t i = warp; i < ns; i += kMediumWarps) {
+            const SmallRef q = S.sref[i];
+            float slo[3] = {0.f, 0.f, 0.f}, shi[3] = {0.f, 0.f, 0.f};
+            uint32_t sid = 0;
+            if (lane < q.len) {
+                const uint32_t r = S.idx[q.ob][q.cs + lane];
+                const float4 a = S.rlo[r], b = S.rhi[r];
+                slo[0] = a.x;
+                slo[1] = a.y;
+                slo[2] = a.z;
+                sid = __float_as_uint(a.w);
+                shi[0] = b.x;
+                shi[1] = b.y;
+                shi[2] = b.z;
+            }
+            if constexpr (kSmallLevels)
+                warp_build_subtree_levels(slo, shi, sid, q.len, base + q.cs, q.slot, q.pair, q.depth, t.nbase,
+                                          t.tbase, q.b, P, O, S.xchg[warp]);
+            else
+                warp_build_subtree(slo, shi, sid, q.len, base + q.cs, q.slot, q.pair, q.depth, t.nbase, t.tbase, q.b,
+                                   P, O, S.xchg[warp]);
+        }
     }
 }
 
@@ -2242,35 +2284,36 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
 // ---------------------------------------------------------------- persistent batched build
 //
 // A batch of meshes (every BLAS and the TLAS) built by one persistent launch
-// that takes node tasks from device-side queues, in place of the level
+// that takes node tasks from a device-side queue, in place of the level
 // passes and the subtree launches. One CTA of kMediumThreads threads per
-// resident slot loops: pop a task, build it, push its children.
-//   main queue   nodes above 32 objects. Above medium_max the CTA bins the
-//                node (3 x 32 bins in shared memory), warp 0 picks the split,
-//                the CTA partitions the records stably into the other buffer
-//                and pushes the children; at or below medium_max it builds
-//                the whole subtree in shared memory (medium_task), pushing its
-//                subtrees of <= 32 objects to the small queue.
-//   small queue  subtrees of <= 32 objects (the small list, ctr->n_small as
-//                its tail), taken four at a time, one per warp.
-// A push counts the task as pending, writes it, fences and then marks it
-// ready; a finished task is uncounted after its children were pushed, so
-// pending reaches 0 only when the whole batch is built, and every CTA then
-// leaves. Every wait (an empty queue while tasks are pending, a claimed slot
-// not yet marked ready) is bounded by a deadline on the global timer; when
-// one runs out the CTA records the time-out, raises abort and leaves, and so
-// do all others at their next poll: the launch ends with MGBVH_ERR_TIMEOUT.
+// resident slot loops: take a task, build it, push its children.
+//   above medium_max   the CTA bins the node (3 x 32 bins in shared memory),
+//                      warp 0 picks the split, the CTA partitions the records
+//                      stably into the other buffer and pushes the children;
+//   33..medium_max     the CTA builds the whole subtree in shared memory
+//                      (medium_task), its warps building each subtree of <= 32
+//                      objects as soon as they split it off;
+//   <= 32              (children of the nodes above medium_max) warp 0 builds it.
+// Tickets: a CTA takes the next ticket with one atomicAdd on the head (no
+// retries under contention) and waits for entry `ticket` to be marked ready,
+// or for the pending count to reach 0 (every task finished: the batch is
+// built, tickets past the last push are never filled, and the CTA leaves). A
+// push counts its task as pending, reserves the next entry, writes it, fences
+// and marks it ready; a finished task is uncounted after its children were
+// pushed. Every wait is bounded by a deadline on the global timer; when one
+// runs out the CTA records the time-out, raises abort and leaves, and so do
+// all others at their next poll: the launch ends with MGBVH_ERR_TIMEOUT.
 // Nodes that need the forced median are queued for the median passes, which
 // run after the launch as in the level-pass build.
 
 constexpr uint32_t kQueueMaxMesh = 1u << 22;  // largest mesh the persistent build takes (objects)
 #ifndef MGBVH_QUEUE_MIN_BLOCKS
-#define MGBVH_QUEUE_MIN_BLOCKS 4  // persistent CTAs per SM the register budget must allow (tuning knob)
+#define MGBVH_QUEUE_MIN_BLOCKS 3  // persistent CTAs per SM the register budget must allow (tuning knob)
 #endif
 
 struct QueueState {
-    uint32_t head, tail;  // main queue: next entry to pop, next entry to reserve
-    uint32_t shead;       // small queue: next entry to pop (its tail is ctr->n_small)
+    uint32_t head, tail;  // next ticket to hand out, next entry to reserve
+    uint32_t pad0;
     uint32_t pending;     // tasks pushed and not yet finished
     uint32_t abort;       // an error or a time-out: every CTA leaves
     uint32_t timeouts;    // waits that ran out
@@ -2278,13 +2321,10 @@ struct QueueState {
 };
 
 struct QueueArgs {
-    Task* q;           // main queue entries
+    Task* q;           // queue entries
     uint32_t* qready;  // 1 once entry i is written
     uint32_t* qcb;     // centroid bound keys of entry i (6; level-pass-size nodes)
     uint32_t qcap;
-    Task* small;       // small queue (the small list)
-    uint32_t* sready;
-    uint32_t scap;
     QueueState* st;
     Task* med;         // nodes waiting for the forced median (count in ctr->n_med)
     uint32_t med_cap;
@@ -2301,26 +2341,8 @@ __device__ __forceinline__ uint32_t vload(const uint32_t* p) { return *reinterpr
 
 __device__ __forceinline__ void queue_abort(const QueueArgs& Q) { atomicExch(&Q.st->abort, 1u); }
 
-// Waits until *flag is 1; false if the deadline passed or the build aborted.
-__device__ __forceinline__ bool wait_ready(const QueueArgs& Q, const uint32_t* flag) {
-    const unsigned long long t0 = global_ns();
-    uint32_t ns = 32;
-    while (vload(flag) == 0u) {
-        if (vload(&Q.st->abort)) return false;
-        if (global_ns() - t0 > Q.wait_ns) {
-            atomicAdd(&Q.st->timeouts, 1u);
-            queue_abort(Q);
-            return false;
-        }
-        __nanosleep(ns);
-        ns = min(ns * 2u, 1024u);
-    }
-    __threadfence();  // the entry (and the records it names) before the flag
-    return true;
-}
-
-// One thread: push a node task of more than 32 objects (cb: its centroid
-// bound keys when it is above medium_max).
+// One thread: push a node task (cb: its centroid bound keys when it is above
+// medium_max).
 __device__ void queue_push_main(const QueueArgs& Q, const Task& t, const uint32_t* cb, Counters* ctr) {
     atomicAdd(&Q.st->pending, 1u);
     const uint32_t i = atomicAdd(&Q.st->tail, 1u);
@@ -2336,56 +2358,28 @@ __device__ void queue_push_main(const QueueArgs& Q, const Task& t, const uint32_
     atomicExch(&Q.qready[i], 1u);
 }
 
-// One thread: push a subtree of <= 32 objects.
-__device__ void queue_push_small(const QueueArgs& Q, const Task& t, Counters* ctr) {
-    atomicAdd(&Q.st->pending, 1u);
-    const uint32_t i = atomicAdd(&ctr->n_small, 1u);
-    if (i >= Q.scap) {
-        set_error(ctr, MGBVH_ERR_CAPACITY, kSiteCapacity);
-        queue_abort(Q);
-        return;
-    }
-    Q.small[i] = t;
-    __threadfence();
-    atomicExch(&Q.sready[i], 1u);
-}
-
-// Thread 0: the next task (kind 1: main entry idx; kind 2: small entries idx
-// .. idx + count - 1) or none (kind 0: the batch is done, or aborted).
+// Thread 0: the next task (kind 1: entry idx) or none (kind 0: the batch is
+// done, or aborted).
 struct Popped {
     uint32_t kind, idx, count;
 };
 
-__device__ Popped queue_pop(const QueueArgs& Q, Counters* ctr) {
+__device__ Popped queue_pop(const QueueArgs& Q) {
     Popped p{0u, 0u, 0u};
+    if (vload(&Q.st->abort)) return p;
+    const uint32_t h = atomicAdd(&Q.st->head, 1u);
     const unsigned long long t0 = global_ns();
     uint32_t ns = 32;
     for (;;) {
+        if (h < Q.qcap && vload(Q.qready + h) != 0u) {
+            __threadfence();  // the entry (and the records it names) after its mark
+            p.kind = 1;
+            p.idx = h;
+            return p;
+        }
         if (vload(&Q.st->abort)) return p;
-        const uint32_t h = vload(&Q.st->head), tl = min(vload(&Q.st->tail), Q.qcap);
-        if (h < tl) {
-            if (atomicCAS(&Q.st->head, h, h + 1u) == h) {
-                if (!wait_ready(Q, Q.qready + h)) return p;
-                p.kind = 1;
-                p.idx = h;
-                return p;
-            }
-            continue;
-        }
-        const uint32_t sh = vload(&Q.st->shead), stl = min(vload(&ctr->n_small), Q.scap);
-        if (sh < stl) {
-            const uint32_t n = min(stl - sh, (uint32_t)kMediumWarps);
-            if (atomicCAS(&Q.st->shead, sh, sh + n) == sh) {
-                for (uint32_t k = 0; k < n; ++k)
-                    if (!wait_ready(Q, Q.sready + sh + k)) return p;
-                p.kind = 2;
-                p.idx = sh;
-                p.count = n;
-                return p;
-            }
-            continue;
-        }
-        if (vload(&Q.st->pending) == 0u) return p;  // every task finished: the batch is built
+        // nothing pending: no entry will come for this ticket
+        if (vload(&Q.st->pending) == 0u) return p;
         if (global_ns() - t0 > Q.wait_ns) {
             atomicAdd(&Q.st->timeouts, 1u);
             queue_abort(Q);
@@ -2407,7 +2401,7 @@ struct LargeSmem {
 
 // One CTA: a node above medium_max objects (records in buffer t.buf, its
 // centroid bound keys cbk), as lvl_bin + lvl_eval + lvl_part do for a level.
-__device__ void queue_large_task(const QueueArgs& Q, LargeSmem& L, const Task& t, const uint32_t* cbk, Rec* rec0,
+__device__ __noinline__ void queue_large_task(const QueueArgs& Q, LargeSmem& L, const Task& t, const uint32_t* cbk, Rec* rec0,
                                  Rec* rec1, const Params& P, const Out& O) {
     const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     const Rec* src = (t.buf ? rec1 : rec0) + t.start;
@@ -2636,62 +2630,70 @@ __device__ void queue_large_task(const QueueArgs& Q, LargeSmem& L, const Task& t
             ct.tile0 = ct.ntiles = 0;
             ct.nbase = t.nbase;
             ct.tbase = t.tbase;
-            if (len <= kSmallMax)
-                queue_push_small(Q, ct, O.ctr);
-            else
-                queue_push_main(Q, ct, len > P.medium_max ? L.keys + (c == 0 ? 6 : 0) : nullptr, O.ctr);
+            queue_push_main(Q, ct, len > P.medium_max ? L.keys + (c == 0 ? 6 : 0) : nullptr, O.ctr);
         }
     }
 }
 
+// The persistent build's subtree CTA and warp-subtree tasks, as separate
+// (not inlined) functions: each gets its own register allocation instead of
+// the union of every task kind's.
 template <uint32_t kCap, bool kLevels>
-__global__ void __launch_bounds__(kMediumThreads, MGBVH_QUEUE_MIN_BLOCKS) queue_build_kernel(QueueArgs Q, Rec* rec0, Rec* rec1, Params P,
-                                                                      Out O) {
+__device__ __noinline__ void queue_medium_task(MediumSmemQ<kCap>& S, const Task& t, Rec* rec0, Rec* rec1,
+                                               const Params& P, const Out& O) {
+    medium_task<false, MediumSmemQ<kCap>, true, kLevels>(S, t, rec0, rec1, nullptr, 0u, P, O,
+                                                         Learn{nullptr, 0, nullptr, 0, nullptr});
+}
+
+template <bool kLevels>
+__device__ __noinline__ void queue_small_task(const Task& t, const Rec* rec0, const Rec* rec1, const Params& P,
+                                              const Out& O, XRec* xchg) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const Rec* src = (t.buf ? rec1 : rec0) + t.start;
+    float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
+    uint32_t id = 0;
+    if (lane < t.len) {
+        const Rec r = ldcg_rec(src + lane);
+        lo[0] = r.lo.x;
+        lo[1] = r.lo.y;
+        lo[2] = r.lo.z;
+        id = __float_as_uint(r.lo.w);
+        hi[0] = r.hi.x;
+        hi[1] = r.hi.y;
+        hi[2] = r.hi.z;
+    }
+    const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
+    if constexpr (kLevels)
+        warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b, P, O,
+                                  xchg);
+    else
+        warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b, P, O, xchg);
+}
+
+template <uint32_t kCap, bool kLevels>
+__global__ void __launch_bounds__(kMediumThreads, MGBVH_QUEUE_MIN_BLOCKS)
+    queue_build_kernel(QueueArgs Q, Rec* rec0, Rec* rec1, Params P, Out O) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
+    MediumSmemQ<kCap>& S = *reinterpret_cast<MediumSmemQ<kCap>*>(smem_raw);
     LargeSmem& L = *reinterpret_cast<LargeSmem*>(smem_raw);  // the same space: one task at a time
     __shared__ Popped pop;
-    __shared__ XRec xchg[kMediumWarps][32];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t warp = threadIdx.x >> 5;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) pop = queue_pop(Q, O.ctr);
+        if (threadIdx.x == 0) pop = queue_pop(Q);
         __syncthreads();
         const Popped p = pop;
         if (p.kind == 0) break;
-        if (p.kind == 1) {
-            const Task t = ldcg_task(Q.q + p.idx);
-            if (t.len > P.medium_max)
-                queue_large_task(Q, L, t, Q.qcb + 6 * p.idx, rec0, rec1, P, O);
-            else
-                medium_task<false, MediumSmemT<kCap>, true>(S, t, rec0, rec1, Q.small, Q.scap, P, O,
-                                                            Learn{nullptr, 0, nullptr, 0, nullptr}, &Q);
-        } else if (warp < p.count) {
-            const Task t = ldcg_task(Q.small + p.idx + warp);
-            const Rec* src = (t.buf ? rec1 : rec0) + t.start;
-            float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};
-            uint32_t id = 0;
-            if (lane < t.len) {
-                const Rec r = ldcg_rec(src + lane);
-                lo[0] = r.lo.x;
-                lo[1] = r.lo.y;
-                lo[2] = r.lo.z;
-                id = __float_as_uint(r.lo.w);
-                hi[0] = r.hi.x;
-                hi[1] = r.hi.y;
-                hi[2] = r.hi.z;
-            }
-            const float b[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
-            if constexpr (kLevels)
-                warp_build_subtree_levels(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b,
-                                          P, O, xchg[warp]);
-            else
-                warp_build_subtree(lo, hi, id, t.len, t.start, t.slot, t.pair, t.depth, t.nbase, t.tbase, b, P,
-                                   O, xchg[warp]);
-        }
+        const Task t = ldcg_task(Q.q + p.idx);
+        if (t.len > P.medium_max)
+            queue_large_task(Q, L, t, Q.qcb + 6 * p.idx, rec0, rec1, P, O);
+        else if (t.len > kSmallMax)
+            queue_medium_task<kCap, kLevels>(S, t, rec0, rec1, P, O);
+        else if (warp == 0)  // a subtree of <= 32 objects split off a node above medium_max
+            queue_small_task<kLevels>(t, rec0, rec1, P, O, S.xchg[0]);
         __threadfence();
         __syncthreads();
-        if (threadIdx.x == 0) atomicSub(&Q.st->pending, p.kind == 1 ? 1u : p.count);
+        if (threadIdx.x == 0) atomicSub(&Q.st->pending, 1u);
     }
 }
 
@@ -2968,10 +2970,7 @@ __global__ void queue_roots_kernel(const DevMesh* __restrict__ meshes, uint32_t 
         t.tile0 = t.ntiles = 0;
         t.nbase = M.nbase;
         t.tbase = M.tbase;
-        if (M.cls == 1)
-            queue_push_small(Q, t, O.ctr);
-        else
-            queue_push_main(Q, t, M.n > medium_max ? mkeys + 12 * m + 6 : nullptr, O.ctr);
+        queue_push_main(Q, t, M.n > medium_max ? mkeys + 12 * m + 6 : nullptr, O.ctr);
     }
 }
 
@@ -3106,7 +3105,7 @@ struct mgbvh_ctx {
     // persistent batched build (mgbvh_set_batch_mode): main queue entries, their
     // ready flags and centroid keys, small-queue ready flags, queue state
     bool batch_queue = false;
-    DevBuf q, qready, qcb, sready, qstate;
+    DevBuf q, qready, qcb, qstate;
     void* h_qstate = nullptr;  // pinned QueueState of the last launch
     int queue_ctas[2] = {0, 0};  // resident CTAs of the 512- and 1024-record instances
     unsigned long long queue_wait_ns = 2000000000ull;
@@ -3841,19 +3840,14 @@ Params params_of(const mgbvh_ctx* ctx, const mgbvh_settings* st) {
     return P;
 }
 
-// Queue capacities of the persistent build for n objects over nm meshes:
-// every pushed task is a distinct node of at least 2 objects whose tasks form
-// a binary tree, so at most n - 1 + nm of them; the small queue holds
-// disjoint subtrees (the small list's bound).
+// The persistent build's queue (capacity ctx->qcap, set by run_batch) and
+// the median list.
 QueueArgs queue_args(mgbvh_ctx* ctx, const Caps& C) {
     QueueArgs Q;
     Q.q = P_<Task>(ctx->q);
     Q.qready = P_<uint32_t>(ctx->qready);
     Q.qcb = P_<uint32_t>(ctx->qcb);
     Q.qcap = ctx->qcap;
-    Q.small = P_<Task>(ctx->small);
-    Q.sready = P_<uint32_t>(ctx->sready);
-    Q.scap = C.small;
     Q.st = P_<QueueState>(ctx->qstate);
     Q.med = P_<Task>(ctx->med_list);
     Q.med_cap = C.tasks;
@@ -3908,7 +3902,6 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
         QueueArgs Q = queue_args(ctx, C);
         MG_CUDA(cudaMemsetAsync(ctx->qstate.p, 0, sizeof(QueueState), sm));
         MG_CUDA(cudaMemsetAsync(ctx->qready.p, 0, 4ull * Q.qcap, sm));
-        MG_CUDA(cudaMemsetAsync(ctx->sready.p, 0, 4ull * Q.scap, sm));
         // queue_hold: tasks counted as pending that never arrive (the test of
         // the bounded waits: the launch must end with a time-out)
         queue_roots_kernel<<<std::max(1u, std::min((nm + 7) / 8, 1024u)), 256, 0, sm>>>(
@@ -3917,7 +3910,7 @@ int enqueue_batch(mgbvh_ctx* ctx, const BatchPlan& B, const Caps& C, const mgbvh
         if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[0], sm));
         const bool small_cap = P.medium_max <= kMediumSmallCap;
         const bool lv = P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax;
-        const size_t smem = small_cap ? sizeof(MediumSmemSmall) : sizeof(MediumSmem);
+        const size_t smem = small_cap ? sizeof(MediumSmemQ<kMediumSmallCap>) : sizeof(MediumSmemQ<kMediumMax>);
         int grid = small_cap ? ctx->queue_ctas[0] : ctx->queue_ctas[1];
         if (ctx->queue_per_sm) grid = std::min(grid, ctx->sm_count * (int)ctx->queue_per_sm);
         if (small_cap && lv)
@@ -4011,12 +4004,14 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     uint32_t max_mesh = 0;
     for (const DevMesh& M : B.hm) max_mesh = std::max(max_mesh, M.n);
     const bool use_queue = ctx->batch_queue && !ctx->learn_w && !ctx->learn_samples && max_mesh <= kQueueMaxMesh;
-    const uint32_t qcap = 2u * (n / (kSmallMax + 1)) + nm + 8u;
+    // tasks: the roots, and two children per node above medium_max (> 32
+    // objects), whose nodes form binary trees with disjoint leaves of > 32
+    // objects: at most 2 * (2n / 33) of them
+    const uint32_t qcap = 4u * (n / (kSmallMax + 1)) + nm + 8u;
     if (use_queue) {
         ENS(ctx->q, sizeof(Task) * (size_t)qcap);
         ENS(ctx->qready, 4ull * qcap);
         ENS(ctx->qcb, 24ull * qcap);
-        ENS(ctx->sready, 4ull * C.small);
         ENS(ctx->qstate, sizeof(QueueState));
     }
     ctx->qcap = qcap;
@@ -4431,7 +4426,7 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->rbins, &ctx->tile_hist2, &ctx->med_list, &ctx->med_work, &ctx->med_off,
                      &ctx->med_seg, &ctx->med_keys[0], &ctx->med_keys[1], &ctx->med_vals[0],
                      &ctx->med_vals[1], &ctx->med_flag, &ctx->med_scan, &ctx->q, &ctx->qready,
-                     &ctx->qcb, &ctx->sready, &ctx->qstate};
+                     &ctx->qcb, &ctx->qstate};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_qstate) cudaFreeHost(ctx->h_qstate);
@@ -4618,7 +4613,7 @@ int mgbvh_set_batch_mode(mgbvh_ctx* ctx, int mode) {
         return fail(ctx, MGBVH_ERR_INVALID_ARG, "batch mode must be MGBVH_BATCH_LEVELS or MGBVH_BATCH_QUEUE");
     if (mode == MGBVH_BATCH_QUEUE && !ctx->queue_ctas[0]) {
         // shared-memory limits and resident CTAs of the persistent kernel's instances
-        const int s_small = (int)sizeof(MediumSmemSmall), s_big = (int)sizeof(MediumSmem);
+        const int s_small = (int)sizeof(MediumSmemQ<kMediumSmallCap>), s_big = (int)sizeof(MediumSmemQ<kMediumMax>);
         MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumSmallCap, true>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, s_small));
         MG_CUDA(cudaFuncSetAttribute(queue_build_kernel<kMediumSmallCap, false>,

@@ -742,16 +742,17 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             box_empty(bgt[a]);
         }
         const uint32_t maxn = __reduce_max_sync(kFull, work ? n : 0u);
-        // every lane's object in shared memory; the lanes of a segment read
-        // its objects in turn (one address per segment: broadcast loads)
-        xchg[lane].lo = make_float4(lo[0], lo[1], lo[2], 0.0f);
-        xchg[lane].hi = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        // every lane's object in shared memory, with its x and y centroids in
+        // the spare words; the lanes of a segment read its objects in turn
+        // (one address per segment: broadcast loads)
+        xchg[lane].lo = make_float4(lo[0], lo[1], lo[2], c[0]);
+        xchg[lane].hi = make_float4(hi[0], hi[1], hi[2], c[1]);
         __syncwarp();
         for (uint32_t r = 0; r < maxn; ++r) {
             if (!(work && r < n)) continue;  // lanes past their segment's objects merge nothing
             const float4 ja = xchg[s + r].lo, jb = xchg[s + r].hi;
             const float jl0 = ja.x, jl1 = ja.y, jl2 = ja.z, jh0 = jb.x, jh1 = jb.y, jh2 = jb.z;
-            const float jc[3] = {center_of(jl0, jh0), center_of(jl1, jh1), center_of(jl2, jh2)};
+            const float jc[3] = {ja.w, jb.w, center_of(jl2, jh2)};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 if (jc[a] < thr[a]) {  // bvh/src/lib.rs:308

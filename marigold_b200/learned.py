@@ -66,10 +66,19 @@ EVAL_MESHES = (("random65536_s9001", "random", 65536, 9001),
                ("icosphere8_s9002", "icosphere", 8, 9002))
 
 
+# the large mixed scene's generator (its seed, 5) at 1/4 size and at full size
+# (16,777,216 triangles): the learned form's evaluation on scenes unlike
+# single meshes; size is the divisor of the scene's parts
+EVAL_SCENES = (("mixed_quarter_s5", "mixed", 4, 5), ("mixed_full_s5", "mixed", 1, 5))
+
+
 def eval_mesh(kind: str, size: int, seed: int):
     from . import synth
     if kind == "random":
         return synth.random_triangles(size, seed=seed)
+    if kind == "mixed":
+        return synth.mixed_scene(seed=seed, n_blob=8388608 // size, grid=(2048, 1024 // size),
+                                 n_thin=4194304 // size)
     return synth.noisy_icosphere(size, seed=seed)
 
 

@@ -1,6 +1,6 @@
 """Writes full_sweep_sah.json: SAH cost (mgbvh_sah_cost) of the oracle's
 plain and full-sweep trees of the learned proposer's held-out evaluation
-meshes (marigold_b200.learned.EVAL_MESHES). The full sweep takes every
+meshes and scenes (marigold_b200.learned.EVAL_MESHES, EVAL_SCENES). The full sweep takes every
 centroid as a threshold on every axis at every node; it is the quality
 yardstick the learned form is measured against.
 
@@ -21,11 +21,11 @@ from oracle import oracle  # noqa: E402
 def main():
     oracle.build_library()
     out = {}
-    for name, kind, size, seed in learned.EVAL_MESHES:
+    for name, kind, size, seed in learned.EVAL_MESHES + learned.EVAL_SCENES:
         v, t = learned.eval_mesh(kind, size, seed)
         row = {"triangles": int(t.shape[0])}
         for key, kw in (("plain", {}), ("full_sweep", {"full_sweep": True})):
-            r = oracle.build(v, t, **kw)
+            r = oracle.build(v, t, vertex_stride_bytes=4 * v.shape[1], **kw)
             assert r["status"] == 0
             row[key] = sah_cost(r["nodes"].view(NODE_DTYPE).reshape(-1), r["lens"])
         out[name] = row
