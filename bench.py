@@ -41,8 +41,12 @@ METRIC = "BVH build Mtri/s"
 UNIT = "Mtri/s"
 SAMPLE_TRIS = 131072
 # dram__bytes_read.sum + dram__bytes_write.sum of one small_kernel launch on
-# this workload, from an ncu capture (cold cache): 47.33 MB + 48.36 MB
-SMALL_KERNEL_TRAFFIC = 95681024
+# this workload, from an ncu capture (cold cache): 47.06 MB + 48.91 MB
+SMALL_KERNEL_TRAFFIC = 95969280
+# smsp__inst_executed.sum of the same launch (warp instructions); the issue
+# ceiling is one warp instruction per SM sub-partition per cycle
+SMALL_KERNEL_INST = 490755129
+SM_SUBPARTITIONS = 4
 WORKLOAD = ("noisy icosphere L8 (1,310,720 tris, 655,362 verts), leaf 1, max_depth 32, "
             "reference split profile")
 
@@ -204,6 +208,25 @@ def algorithmic_bytes(n, n_verts, internal_len_sum, node_count):
     return (n * (12 + 3 * 32) + n * 24 + internal_len_sum * 56 + node_count * 32)
 
 
+def issue_roofline(inst, launch_ms, clk):
+    """The instruction-issue ceiling of a kernel: `inst` warp instructions
+    (smsp__inst_executed.sum from an ncu capture of the launch) at one per
+    sub-partition per cycle on every SM, at the median SM clock sampled
+    during the timed steps. frac is the ceiling's time over the measured one,
+    i.e. the fraction of issue slots the launch used."""
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    if not mhz or launch_ms <= 0:
+        return None
+    peak = sms * SM_SUBPARTITIONS * mhz * 1e6  # warp instructions per second
+    achieved = inst / (launch_ms * 1e-3)
+    return {"bound": "issue", "inst_per_launch": int(inst), "achieved": round(achieved / 1e9, 1),
+            "peak": round(peak / 1e9, 1), "unit": "Ginst/s", "frac": round(achieved / peak, 4),
+            "sm_mhz": mhz, "sms": sms,
+            "inst_source": "smsp__inst_executed.sum, one ncu capture of the launch"}
+
+
 def learned_leg(ctx, build_dev, c_args, c_count, d_nodes, d_lens, n, plain_sah, flush, stream, steps):
     """The learned form on the headline mesh (committed proposer, refine gate
     on): device-timed build Mtri/s as the plain build is timed, and its tree's
@@ -213,6 +236,7 @@ def learned_leg(ctx, build_dev, c_args, c_count, d_nodes, d_lens, n, plain_sah, 
     from marigold_b200.bvh import NODE_DTYPE, sah_cost
     weights = torch.from_numpy(learned.load_weights().view(np.int16)).cuda()
     ctx.set_split_proposer(weights, True)
+    ctx.set_proposer_gate(*learned.RECOMMENDED_GATE)
     try:
         for _ in range(3):
             flush.fill_(1)
@@ -232,11 +256,14 @@ def learned_leg(ctx, build_dev, c_args, c_count, d_nodes, d_lens, n, plain_sah, 
                        d_lens[:count].cpu().numpy().view(np.uint32))
     finally:
         ctx.set_split_proposer(None)
+        ctx.set_proposer_gate(0.0, 0)
     bms = float(np.mean(ms))
+    thr, min_n = learned.RECOMMENDED_GATE
     return {"value": round(n / (bms * 1e-3) / 1e6, 3), "unit": UNIT, "ms_per_step": round(bms, 4),
             "sah": round(sah, 4), "plain_sah": round(plain_sah, 4),
             "sah_delta_vs_plain_pct": round(100.0 * (sah / plain_sah - 1.0), 4),
-            "proposer": "marigold_b200/proposer_weights.bin, refine gate on"}
+            "proposer": f"marigold_b200/proposer_weights.bin, refine gate on (logit > {thr}), "
+                        f"network on nodes of >= {min_n} objects"}
 
 
 def trace_leg(steps, flush, scale=4):
@@ -448,6 +475,7 @@ def run_ours(args):
                      "traffic": SMALL_KERNEL_TRAFFIC,
                      "algorithmic_bytes_per_launch": int(small_alg),
                      "launch_ms": round(small_ms, 4), "subtrees": small_tasks,
+                     "issue": issue_roofline(SMALL_KERNEL_INST, small_ms, clocks.summary()),
                      "note": "issue-bound: the adaptive sweep's O(n^2) threshold evaluation"},
         "roofline_build": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm,
                            "unit": "GB/s", "frac": round(achieved / hbm, 4),
@@ -789,14 +817,16 @@ def _trace_rate(tr, d_nodes, count, dv, dt, d_perm, n, dr, m, stream, flush, rep
 
 def run_learned(args):
     """The learned split proposer against the plain builder on held-out seeds
-    of its two training generators (65,536 random small triangles; the
-    level-8 noisy icosphere). Per mesh and build form: device-timed build
+    of its training generators (65,536 random small triangles; the level-8
+    noisy icosphere) and on the large mixed scene at 1/4 and full size
+    (16,777,216 triangles). Per mesh and build form: device-timed build
     Mtri/s (L2 flushed before every build), total SAH cost, and closest-hit
     Mrays/s of 1,048,576 rays (origins uniform in the mesh box grown by 10%,
     uniform directions) on the built tree. The full-sweep SAH of each mesh
     comes from tests/golden/full_sweep_sah.json (written by the script beside
-    it). Forms: plain (the reference's tree), learned (trained network, refine
-    gate on), learned-ungated (every binned node of 33..1024 objects scores
+    it). Forms: plain (the reference's tree), learned (trained network with
+    the recommended gate: refine logit > 0, network on nodes of >= 1,025
+    objects), learned-ungated (every binned node of 33 or more objects scores
     the network's proposals)."""
     import torch
     from marigold_b200 import BvhSettings, _lib, build_device, learned, synth
@@ -812,7 +842,7 @@ def run_learned(args):
     stream = torch.cuda.current_stream()
     rows = []
     clocks = ClockSampler(0).__enter__()  # sampled through every timed build and trace below
-    for name, kind, size, seed in learned.EVAL_MESHES:
+    for name, kind, size, seed in learned.EVAL_MESHES + learned.EVAL_SCENES:
         v, t = learned.eval_mesh(kind, size, seed)
         n = t.shape[0]
         dv = torch.from_numpy(v).cuda()
@@ -829,6 +859,7 @@ def run_learned(args):
         for form, w, gate in (("plain", None, False), ("learned", weights, True),
                               ("learned_ungated", weights, False)):
             ctx.set_split_proposer(w, gate)
+            ctx.set_proposer_gate(*(learned.RECOMMENDED_GATE if gate else (0.0, 0)))
             ms = []
             for k in range(max(args.warmup, 3) + args.steps):
                 flush.fill_(k & 0xFF)
@@ -868,7 +899,9 @@ def run_learned(args):
         "network": {"samples": rec.get("samples"), "steps": rec.get("steps"),
                     "heldout_accuracy": rec.get("heldout_accuracy")},
         "config": {"medium_max": 1024, "leaf": 1, "max_depth": 32, "profile": "reference",
-                   "rays": 1048576, "l2": "flushed before every build and trace"},
+                   "rays": 1048576, "l2": "flushed before every build and trace",
+                   "gate": {"refine_logit_above": learned.RECOMMENDED_GATE[0],
+                            "min_objects": learned.RECOMMENDED_GATE[1]}},
     }
     print(json.dumps(out), flush=True)
 

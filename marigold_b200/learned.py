@@ -71,6 +71,13 @@ EVAL_MESHES = (("random65536_s9001", "random", 65536, 9001),
 # single meshes; size is the divisor of the scene's parts
 EVAL_SCENES = (("mixed_quarter_s5", "mixed", 4, 5), ("mixed_full_s5", "mixed", 1, 5))
 
+# The gate the library's users should set with mgbvh_set_proposer_gate for
+# the committed network: proposals are scored where the refine logit is above
+# 0, and the network runs only on nodes of 1,025 objects or more (above every
+# subtree CTA's size, so the subtree kernels run their plain form). The
+# library's own default (0, 0) runs the network at every binned node.
+RECOMMENDED_GATE = (0.0, 1025)
+
 
 def eval_mesh(kind: str, size: int, seed: int):
     from . import synth
