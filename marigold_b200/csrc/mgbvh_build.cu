@@ -38,7 +38,6 @@
 
 #include "mgbvh_device.cuh"
 #include "mgbvh_learn.cuh"
-#include "mgbvh_tma.cuh"
 
 namespace mgbvh {
 
@@ -57,9 +56,6 @@ constexpr int kTileThreads = 256;
 constexpr int kMediumWarps = MGBVH_MEDIUM_WARPS;
 constexpr int kMediumThreads = kMediumWarps * 32;
 constexpr uint32_t kBinWords = 3 * 32 * 7;  // [axis][bin]{count, lo key xyz, hi key xyz}
-// a node's global bins: kBinWords, then the count of its tiles binned so
-// far (the tile that completes it evaluates the node), padded to 16 bytes
-constexpr uint32_t kNodeBinWords = kBinWords + 4;
 
 // Level counter slots rotate over three: level L reads ctr->lvl[L % 3],
 // its evaluations append the next level's nodes to slot (L + 1) % 3, and
@@ -261,12 +257,6 @@ __device__ __forceinline__ void init_task_bins(uint32_t* b, uint32_t lane, uint3
     }
 }
 
-// A node's global bins (kNodeBinWords words): empty bins, no tile binned.
-__device__ __forceinline__ void init_node_bins(uint32_t* b, uint32_t lane, uint32_t nthreads) {
-    init_task_bins(b, lane, nthreads);
-    if (lane == 0) b[kBinWords] = 0;
-}
-
 // Root node: classify and enqueue (or finish, when the root is a leaf).
 // cls: 0 leaf, 1 small, 2 medium, 3 large.
 __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, float b0, float b1,
@@ -335,7 +325,7 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
         O.ctr->lvl[0][0] = 1;
         O.ctr->lvl[0][1] = ntiles;
     }
-    if (blockIdx.x == 0) init_node_bins(bins, threadIdx.x, blockDim.x);
+    if (blockIdx.x == 0) init_task_bins(bins, threadIdx.x, blockDim.x);
     if (gtid < 6) cbkeys[gtid] = O.ctr->root_keys[6 + gtid];
     for (uint32_t i = gtid; i < ntiles; i += gsz) {
         tile_task[i] = 0;
@@ -350,14 +340,12 @@ constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 #ifndef MGBVH_BIN_MIN_BLOCKS
 #define MGBVH_BIN_MIN_BLOCKS 4  // CTAs per SM the register budget must allow (tuning knob; 1 / 3 / 4 with batches of 8 / 4 / 4: 682 / 691 / 692 Mtri/s)
 #endif
+#ifndef MGBVH_PART_CODES
+#define MGBVH_PART_CODES 1  // 1: the bin pass stores each record's bins (16 bits) and the partition reads them
+#endif
+constexpr bool kPartCodes = MGBVH_PART_CODES != 0;
 #ifndef MGBVH_REFINE_AGG
 #define MGBVH_REFINE_AGG 1  // 1: the refine pass merges its edge intervals across the warp (0: per-lane atomics)
-#endif
-#ifndef MGBVH_TMA_LEVELS
-#define MGBVH_TMA_LEVELS 0  // 1: the level passes stage each tile in shared memory with bulk copies (measured 0.81 vs 0.75 ms of level passes at 3 CTAs/SM, 0.87 at 2)
-#endif
-#ifndef MGBVH_TMA_MIN_BLOCKS
-#define MGBVH_TMA_MIN_BLOCKS 3  // CTAs per SM of the staged level passes (64 KB of records each)
 #endif
 #ifndef MGBVH_BIN_BATCH
 #define MGBVH_BIN_BATCH 4  // records a thread loads before binning them (tuning knob; divides 8)
@@ -369,45 +357,6 @@ static_assert(kRecsPerThread % kBinBatch == 0, "the bin batch divides the record
 #endif
 constexpr int kPartUnroll = MGBVH_PART_UNROLL;
 
-// Bulk copy of a tile's records (cnt of them, contiguous) into shared
-// memory, in chunks, completing on `bar`; issued by one thread.
-constexpr uint32_t kTileBytes = kTile * 32u;  // a tile of records in shared memory
-constexpr uint32_t kBulkChunk = 16384;        // bytes per cp.async.bulk
-constexpr uint32_t kBulkPolls = 1u << 22;  // mbarrier polls before a wait gives up
-__device__ __forceinline__ void tile_bulk_load(Rec* srec, const Rec* src, uint32_t cnt, uint64_t* bar) {
-    const uint32_t bytes = cnt * static_cast<uint32_t>(sizeof(Rec));
-    mbar_arrive_expect_tx(bar, bytes);
-    for (uint32_t off = 0; off < bytes; off += kBulkChunk)
-        bulk_load(reinterpret_cast<char*>(srec) + off, reinterpret_cast<const char*>(src) + off,
-                  min(kBulkChunk, bytes - off), bar);
-}
-
-// Every thread waits for the tile's copy (phase `phase`, then flipped).
-// false for the whole CTA if any thread's bounded wait ran out: the error is
-// recorded, the copy gets one more bounded wait to land, and the caller
-// returns.
-__device__ __forceinline__ bool tile_bulk_wait(uint64_t* bar, uint32_t& phase, Counters* ctr) {
-    const bool ok = mbar_wait_bounded(bar, phase, kBulkPolls);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) {
-            set_error(ctr, MGBVH_ERR_TIMEOUT, kSiteBulkCopy);
-            mbar_wait_bounded(bar, phase, kBulkPolls);
-        }
-        return false;
-    }
-    phase ^= 1u;
-    return true;
-}
-
-// A load that bypasses L1 where the data was written by other CTAs of the
-// same launch (L1 is not coherent within a launch).
-template <bool kCoherent>
-__device__ __forceinline__ uint32_t ld_maybe_cg(const uint32_t* p) {
-    if constexpr (kCoherent)
-        return __ldcg(p);
-    else
-        return *p;
-}
 
 struct EvalArgs {
     const Task* tasks;
@@ -443,7 +392,6 @@ struct EvalArgs {
 // a leaf, a next-level task, a medium or a small subtree. Each lane scans a
 // contiguous run of the node's tiles (independent loads), runs joined by a
 // warp scan.
-template <bool kCoherent = false>
 __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane,
                            const Task& t, Decision& d, const uint32_t* hist, uint32_t row) {
     const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
@@ -453,7 +401,7 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     const uint32_t i0 = min(lane * per, t.ntiles), i1 = min(i0 + per, t.ntiles);
     uint32_t sum = 0;
 #pragma unroll 8
-    for (uint32_t i = i0; i < i1; ++i) sum += ld_maybe_cg<kCoherent>(h + i);
+    for (uint32_t i = i0; i < i1; ++i) sum += h[i];
     uint32_t inc = sum;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -463,7 +411,7 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     const uint32_t total = __shfl_sync(kFull, inc, 31);
     uint32_t run = inc - sum;
     for (uint32_t i = i0; i < i1; ++i) {
-        const uint32_t v = ld_maybe_cg<kCoherent>(h + i);
+        const uint32_t v = h[i];
         lt[i] = run;
         run += v;
     }
@@ -539,7 +487,7 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
             ct.tile0 = t0;
             ct.ntiles = nt;
             if (lane == 0) A.next_tasks[ti] = ct;
-            init_node_bins(A.next_bins + (size_t)ti * kNodeBinWords, lane, 32);
+            init_task_bins(A.next_bins + (size_t)ti * kBinWords, lane, 32);
             if (lane < 6) A.next_cbkeys[6 * ti + lane] = lane < 3 ? kKeyPosInf : kKeyNegInf;
             for (uint32_t i = lane; i < nt; i += 32) {
                 A.next_tile_task[t0 + i] = ti;
@@ -565,10 +513,9 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     if (lane == 0) A.dec[w] = d;
 }
 
-template <bool kCoherent = false>
 __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
     const Task t = A.tasks[w];
-    const uint32_t* tb = A.bins + (size_t)w * kNodeBinWords;
+    const uint32_t* tb = A.bins + (size_t)w * kBinWords;
     if (A.refine && lane == 0) A.refine[w].on = 0;  // before any return: nothing pending
     float cmn[3], ext[3];
 #pragma unroll
@@ -598,8 +545,8 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const uint32_t* bw = tb + (a * 32 + lane) * 7;
-            cnt[a] = ld_maybe_cg<kCoherent>(bw);
-            for (int i = 0; i < 6; ++i) box[a][i] = funkey(ld_maybe_cg<kCoherent>(bw + 1 + i));
+            cnt[a] = bw[0];
+            for (int i = 0; i < 6; ++i) box[a][i] = funkey(bw[1 + i]);
             axis_ok[a] = !(ext[a] == 0.0f);
         }
         Cand best;
@@ -654,7 +601,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         d.ltb[i] = win.lt[i];
         d.gtb[i] = win.gt[i];
     }
-    if (!kCoherent && A.lw && B == 32u && t.len >= A.lmin_n) {  // the fused evaluation runs without the learned form
+    if (A.lw && B == 32u && t.len >= A.lmin_n) {
         // the learned form: run the network; with proposals to score, the
         // decision waits for the refine pass (lvl_eval2_kernel)
         const float cb[6] = {cmn[0], cmn[1], cmn[2], funkey(A.cbkeys[6 * w + 3]),
@@ -683,7 +630,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
             return;
         }
     }
-    emit_split<kCoherent>(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u + d.split_bin);
+    emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u + d.split_bin);
 }
 
 __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
@@ -694,59 +641,32 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
         eval_task(A, P, O, w, lane);
 }
 
-// The node evaluation of the fused bin pass: bins and tile histograms were
-// written by other CTAs of the same launch, so they are read from L2.
-__device__ __noinline__ void eval_task_fused(const EvalArgs& A, const Params& P, const Out& O, uint32_t w,
-                                             uint32_t lane) {
-    eval_task<true>(A, P, O, w, lane);
-}
-
 // Per-tile bin histograms (count + AABB per axis and bin) of the large nodes
 // with shared-memory atomics, merged into the node's global bins. Grid-stride over
 // the level's tiles; the tile count is read on the device. Each thread loads
 // its records of the tile first (kTile / kTileThreads of them), then bins
 // them. Also clears the level counter slot two levels ahead (the previous
 // level's kernels, which read it, have finished; the next writer is the
-// next level's evaluation).
-// kFuse: the CTA that merges a node's last tile evaluates the node as
-// lvl_eval_kernel would (the "last block" pattern: every CTA fences its
-// merges, then counts its tile in the node's bins), so no separate
-// evaluation launch is needed.
-// kTma: the tile's records are first brought into shared memory by bulk
-// copies (kTile * 32 bytes of dynamic shared memory) and binned from there.
-template <bool kFuse, bool kTma>
-__global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MGBVH_BIN_MIN_BLOCKS) lvl_bin_kernel(
-    const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* bins,
+// next level's evaluation). Each record's bin on every axis (5 bits each)
+// goes to `codes` at its position, for the partition pass.
+__global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_kernel(
+    const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys, uint32_t* __restrict__ bins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
-    uint32_t* tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
-    const Rec* __restrict__ rec1, Counters* ctr, uint32_t lv, Params P, EvalArgs A, Out O) {
-    extern __shared__ __align__(128) unsigned char bin_dsm[];
+    uint32_t* __restrict__ tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
+    const Rec* __restrict__ rec1, uint16_t* __restrict__ codes, Counters* __restrict__ ctr, uint32_t lv,
+    Params P) {
     __shared__ uint32_t sb[kBinWords];
-    __shared__ uint32_t s_last;
-    __shared__ __align__(8) uint64_t s_bar;
-    Rec* const srec = reinterpret_cast<Rec*>(bin_dsm);
-    uint32_t phase = 0;
-    if constexpr (kTma) {
-        if (threadIdx.x == 0) mbar_init(&s_bar, 1);
-    }
     if (blockIdx.x == 0 && threadIdx.x < 2) ctr->lvl[lvl_free(lv)][threadIdx.x] = 0;
     const uint32_t ntiles = ctr->lvl[lv][1];
     const uint32_t B = P.bins ? P.bins : 32u;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        __syncthreads();  // (kTma: also publishes the barrier's initialization)
+        __syncthreads();
+        init_task_bins(sb, threadIdx.x, blockDim.x);
         const uint32_t ti = tile_task[tile];
         const Task& t = tasks[ti];
         const uint32_t begin = tile_begin[tile];
         const uint32_t cnt = min(kTile, t.len - begin);
-        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;  // kTma: the shared-memory copy, once loaded
-        if constexpr (kTma) {
-            if (threadIdx.x == 0) tile_bulk_load(srec, src, cnt, &s_bar);
-        }
-        init_task_bins(sb, threadIdx.x, blockDim.x);
-        if constexpr (kTma) {
-            if (!tile_bulk_wait(&s_bar, phase, ctr)) return;  // block-uniform; also orders the bins' initialization
-            src = srec;
-        }
+        const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
         float cmn[3], ext[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -765,15 +685,18 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
                     rh[k] = src[i].hi;
                 }
             }
-            if (!kTma && k0 == 0) __syncthreads();  // the tile's bins are initialized
+            if (k0 == 0) __syncthreads();  // the tile's bins are initialized
 #pragma unroll
             for (uint32_t k = 0; k < kBinBatch; ++k) {
-                if (threadIdx.x + (k0 + k) * kTileThreads >= cnt) break;
+                const uint32_t i = threadIdx.x + (k0 + k) * kTileThreads;
+                if (i >= cnt) break;
                 const float l[3] = {rl[k].x, rl[k].y, rl[k].z}, h[3] = {rh[k].x, rh[k].y, rh[k].z};
+                uint32_t code = 0;
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
                     if (ext[a] == 0.0f) continue;  // block-uniform
                     const uint32_t b = bin_of(center_of(l[a], h[a]), cmn[a], ext[a], B);
+                    code |= b << (5 * a);
                     uint32_t* w = sb + (a * 32 + b) * 7;
                     atomicAdd(w, 1u);
                     atomicMin(w + 1, fkey(l[0]));
@@ -783,6 +706,7 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
                     atomicMax(w + 5, fkey(h[1]));
                     atomicMax(w + 6, fkey(h[2]));
                 }
+                if (kPartCodes) codes[t.start + begin + i] = static_cast<uint16_t>(code);
             }
         }
         __syncthreads();
@@ -798,7 +722,7 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
             }
             tile_hist[(size_t)threadIdx.x * cap_tiles + tile] = inc - c;
         }
-        uint32_t* gb = bins + (size_t)ti * kNodeBinWords;
+        uint32_t* gb = bins + (size_t)ti * kBinWords;
         for (uint32_t k = threadIdx.x; k < kBinWords; k += blockDim.x) {
             const uint32_t bin = k / 7u, f = k % 7u;
             const uint32_t v = sb[k];
@@ -809,16 +733,6 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
                 atomicMin(gb + k, v);
             else
                 atomicMax(gb + k, v);
-        }
-        if constexpr (kFuse) {
-            __threadfence();  // this tile's merges and histogram rows before its count
-            __syncthreads();
-            if (threadIdx.x == 0) s_last = atomicAdd(gb + kBinWords, 1u) + 1u == t.ntiles ? 1u : 0u;
-            __syncthreads();
-            if (s_last && threadIdx.x < 32) {
-                __threadfence();
-                eval_task_fused(A, P, O, ti, threadIdx.x);
-            }
         }
     }
 }
@@ -1148,7 +1062,7 @@ __global__ void __launch_bounds__(256) lvl_sample_kernel(const Task* __restrict_
             for (int a = 0; a < 6; ++a) cb[a] = funkey(cbkeys[6 * w + a]);
             uint32_t cnt[3];
             for (int a = 0; a < 3; ++a)
-                cnt[a] = cb[3 + a] - cb[a] == 0.0f ? 0u : bins[(size_t)w * kNodeBinWords + (a * 32 + lane) * 7];
+                cnt[a] = cb[3 + a] - cb[a] == 0.0f ? 0u : bins[(size_t)w * kBinWords + (a * 32 + lane) * 7];
             float f[24];
             node_features(nb, cb, n, t.depth, cnt, f);
             if (lane == 0) {
@@ -1173,27 +1087,14 @@ constexpr uint32_t kPartPerLane = kTile / kTileThreads;  // 8
 #define MGBVH_PART_MIN_BLOCKS 5  // CTAs per SM the register budget must allow (tuning knob)
 #endif
 
-// kTma: the tile's records are first brought into shared memory by bulk
-// copies (kTile * 32 bytes of dynamic shared memory), and both passes read
-// them there: one global read of each record instead of two, and a tile in
-// flight per CTA without registers held for it.
-template <bool kTma>
-__global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MGBVH_PART_MIN_BLOCKS) lvl_part_kernel(
+__global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_kernel(
     const Task* __restrict__ tasks, const Decision* __restrict__ dec,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
-    const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, uint32_t* next_cbkeys, uint32_t lv,
-    Out O) {
-    extern __shared__ __align__(128) unsigned char part_dsm[];
+    const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, const uint16_t* __restrict__ codes,
+    uint32_t* next_cbkeys, uint32_t lv, Out O) {
     __shared__ uint32_t wcnt[kTileThreads / 32];
     __shared__ uint32_t sk[12];
     __shared__ int sbad;
-    __shared__ __align__(8) uint64_t s_bar;
-    Rec* const srec = reinterpret_cast<Rec*>(part_dsm);
-    uint32_t phase = 0;
-    if constexpr (kTma) {
-        if (threadIdx.x == 0) mbar_init(&s_bar, 1);
-        __syncthreads();
-    }
     const uint32_t ntiles = O.ctr->lvl[lv][1];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t below = (1u << lane) - 1u;
@@ -1204,15 +1105,12 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
         const uint32_t begin = tile_begin[tile];
         const uint32_t tstart = t.start, tlen = t.len;
         const uint32_t cnt = min(kTile, tlen - begin);
-        const Rec* src = (t.buf ? rec1 : rec0) + tstart + begin;  // kTma: the shared-memory copy, once loaded
+        const Rec* src = (t.buf ? rec1 : rec0) + tstart + begin;
         Rec* dst = t.buf ? rec0 : rec1;
         if (d.kind == 1) {
             for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x)
                 O.perm[tstart + begin + i] = __float_as_uint(src[i].lo.w);
             continue;
-        }
-        if constexpr (kTma) {
-            if (threadIdx.x == 0) tile_bulk_load(srec, src, cnt, &s_bar);
         }
         const uint32_t axis = d.axis, split_bin = d.split_bin, nbins = d.bins, n_lt = d.n_lt;
         const float cmin = d.cmin, ext = d.ext, thr = d.thr;
@@ -1220,33 +1118,47 @@ __global__ void __launch_bounds__(kTileThreads, kTma ? MGBVH_TMA_MIN_BLOCKS : MG
         if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
         if (threadIdx.x == 0) sbad = 0;
         const uint32_t w0 = warp * (32u * kPartPerLane);
-        if constexpr (kTma) {
-            if (!tile_bulk_wait(&s_bar, phase, O.ctr)) return;  // block-uniform
-            src = srec;
-        }
-        // pass 1: sides (the split axis's bounds of all this lane's records
-        // are loaded first)
+        // pass 1: sides (from the bin pass's codes for a binned split; else the
+        // split axis's bounds of all this lane's records are loaded first)
         uint32_t bal[kPartPerLane];
         uint32_t lt_w = 0;
-        float pl[kPartPerLane], ph[kPartPerLane];
+        if (kPartCodes && !use_thr) {
+            // binned split: the bin pass left each record's bin on the split axis
+            const uint16_t* cs = codes + tstart + begin;
+            const uint32_t sh = 5u * axis;
+            uint32_t cj[kPartPerLane];
 #pragma unroll
-        for (uint32_t j = 0; j < kPartPerLane; ++j) {
-            const uint32_t i = w0 + j * 32u + lane;
-            if (i < cnt) {
-                pl[j] = reinterpret_cast<const float*>(&src[i].lo)[axis];
-                ph[j] = reinterpret_cast<const float*>(&src[i].hi)[axis];
+            for (uint32_t j = 0; j < kPartPerLane; ++j) {
+                const uint32_t i = w0 + j * 32u + lane;
+                cj[j] = i < cnt ? cs[i] : 0xFFFFu;
             }
-        }
 #pragma unroll
-        for (uint32_t j = 0; j < kPartPerLane; ++j) {
-            const uint32_t i = w0 + j * 32u + lane;
-            bool pred = false;
-            if (i < cnt) {
-                const float c = center_of(pl[j], ph[j]);
-                pred = use_thr ? c < thr : bin_of(c, cmin, ext, nbins) < split_bin;
+            for (uint32_t j = 0; j < kPartPerLane; ++j) {
+                const bool pred = w0 + j * 32u + lane < cnt && ((cj[j] >> sh) & 31u) < split_bin;
+                bal[j] = __ballot_sync(kFull, pred);
+                lt_w += __popc(bal[j]);
             }
-            bal[j] = __ballot_sync(kFull, pred);
-            lt_w += __popc(bal[j]);
+        } else {
+            float pl[kPartPerLane], ph[kPartPerLane];
+#pragma unroll
+            for (uint32_t j = 0; j < kPartPerLane; ++j) {
+                const uint32_t i = w0 + j * 32u + lane;
+                if (i < cnt) {
+                    pl[j] = reinterpret_cast<const float*>(&src[i].lo)[axis];
+                    ph[j] = reinterpret_cast<const float*>(&src[i].hi)[axis];
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kPartPerLane; ++j) {
+                const uint32_t i = w0 + j * 32u + lane;
+                bool pred = false;
+                if (i < cnt) {
+                    const float c = center_of(pl[j], ph[j]);
+                    pred = use_thr ? c < thr : bin_of(c, cmin, ext, nbins) < split_bin;
+                }
+                bal[j] = __ballot_sync(kFull, pred);
+                lt_w += __popc(bal[j]);
+            }
         }
         if (lane == 0) wcnt[warp] = lt_w;
         __syncthreads();
@@ -1602,7 +1514,7 @@ __global__ void __launch_bounds__(128) med_finish_kernel(const Task* __restrict_
                 ct.tile0 = t0;
                 ct.ntiles = nt;
                 if (lane == 0) M.tasks[ti] = ct;
-                init_node_bins(M.bins + (size_t)ti * kNodeBinWords, lane, 32);
+                init_task_bins(M.bins + (size_t)ti * kBinWords, lane, 32);
                 if (lane < 6) M.cbkeys[6 * ti + lane] = ck[(c == 0 ? 6 : 0) + lane];
                 for (uint32_t i = lane; i < nt; i += 32) {
                     M.tile_task[t0 + i] = ti;
@@ -3100,7 +3012,7 @@ __global__ void init_roots_kernel(const DevMesh* __restrict__ meshes, uint32_t n
             if (lane == 0) medium[M.list_index] = t;
         } else {
             if (lane == 0) large[M.list_index] = t;
-            init_node_bins(bins + (size_t)M.list_index * kNodeBinWords, lane, 32);
+            init_task_bins(bins + (size_t)M.list_index * kBinWords, lane, 32);
             if (lane < 6) cbkeys[6 * M.list_index + lane] = mkeys[12 * m + 6 + lane];
             for (uint32_t i = lane; i < M.ntiles; i += 32) {
                 tile_task[M.tile0 + i] = M.list_index;
@@ -3273,6 +3185,7 @@ struct mgbvh_ctx {
     std::string err;
     DevBuf rec[2], tasks[2], bins[2], cbkeys[2], tile_task[2], tile_begin[2];
     DevBuf tile_hist, tile_lt, dec, medium, small, nodes, lens, used, newidx, widened, perm, ctr, cub_tmp;
+    DevBuf bincode;  // per object of a level pass: its bin on each axis (5 bits each)
     DevBuf in_a, in_b, out_nodes, out_lens;
     DevBuf mesh_buf, toff_buf, noff_buf, mkeys;
     // forced medians of level-pass nodes: the waiting list, its working copy,
@@ -3407,7 +3320,6 @@ const char* site_text(uint32_t site) {
         case kSiteMedian: return "forced median: a half's count differs from len / 2 (bvh/src/lib.rs:621-634)";
         case kSiteCapacity: return "internal task list overflow";
         case kSiteMeshIndex: return "an instance names a mesh past mesh_count";
-        case kSiteBulkCopy: return "a bulk copy of a tile into shared memory did not land within its bounded wait";
         default: return "device error";
     }
 }
@@ -3430,8 +3342,6 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     // counts on the device, so levels are launched in batches and the host
     // reads the next level's count only at the end of a batch.
     const int tile_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * 8u);
-    // staged passes: as many CTAs as fit at once (each keeps a tile in flight)
-    const int tma_grid = (int)std::min<uint32_t>(C.tiles, (uint32_t)ctx->sm_count * MGBVH_TMA_MIN_BLOCKS);
     const int eval_grid = (int)std::min<uint32_t>((C.tasks + 3) / 4, (uint32_t)ctx->sm_count * 4u);
     uint32_t level = 0;
     bool more = has_large;
@@ -3444,12 +3354,6 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
     LN.samples = ctx->learn_samples;
     LN.cap = ctx->learn_cap;
     LN.count = ctx->learn_count;
-    // the node evaluation runs inside the bin pass unless the learned form
-    // (network, refine passes, samples) needs the separate kernels
-#ifndef MGBVH_FUSE_EVAL
-#define MGBVH_FUSE_EVAL 0  // 1: evaluation inside the bin pass (measured slower: 1.19 vs 0.76 ms of level passes)
-#endif
-    const bool fuse_eval = MGBVH_FUSE_EVAL && !LN.w && !LN.samples;
     bool first_batch = true;
     while (more) {
         const uint32_t batch = fixed_levels ? fixed_levels
@@ -3459,7 +3363,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
         for (uint32_t bl = 0; bl < batch; ++bl, ++level) {
             // buffers alternate between two sets; level counters rotate over three slots
             const uint32_t bf = level & 1u, nx = bf ^ 1u, lv = level % 3u;
-            launches += fuse_eval ? 2 : 3;
+            launches += 3;
             EvalArgs A;
             A.tasks = P_<Task>(ctx->tasks[bf]);
             A.lv = lv;
@@ -3487,13 +3391,11 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             A.rbins = LN.w ? P_<uint32_t>(ctx->rbins) : nullptr;
             A.tile_hist2 = LN.w ? P_<uint32_t>(ctx->tile_hist2) : nullptr;
             A.med = P_<Task>(ctx->med_list);
-            auto bin = fuse_eval ? (MGBVH_TMA_LEVELS ? lvl_bin_kernel<true, true> : lvl_bin_kernel<true, false>)
-                                 : (MGBVH_TMA_LEVELS ? lvl_bin_kernel<false, true> : lvl_bin_kernel<false, false>);
-            bin<<<MGBVH_TMA_LEVELS ? tma_grid : tile_grid, kTileThreads, MGBVH_TMA_LEVELS ? kTileBytes : 0, sm>>>(
+            lvl_bin_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
                 P_<Task>(ctx->tasks[bf]), P_<uint32_t>(ctx->cbkeys[bf]), P_<uint32_t>(ctx->bins[bf]),
                 P_<uint32_t>(ctx->tile_task[bf]), P_<uint32_t>(ctx->tile_begin[bf]),
-                P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, d_ctr, lv, P, A, O);
-            if (!fuse_eval) lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+                P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, P_<uint16_t>(ctx->bincode), d_ctr, lv, P);
+            lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
             if (LN.samples) {
                 lvl_sample_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(
                     A.tasks, A.dec, A.bins, A.cbkeys, rec0, rec1, d_ctr, lv, P, LN);
@@ -3507,11 +3409,10 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 lvl_eval2_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
                 launches += 2;
             }
-            auto part = MGBVH_TMA_LEVELS ? lvl_part_kernel<true> : lvl_part_kernel<false>;
-            part<<<MGBVH_TMA_LEVELS ? tma_grid : tile_grid, kTileThreads, MGBVH_TMA_LEVELS ? kTileBytes : 0, sm>>>(
+            lvl_part_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
                 P_<Task>(ctx->tasks[bf]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[bf]),
                 P_<uint32_t>(ctx->tile_begin[bf]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
-                P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
+                P_<uint16_t>(ctx->bincode), P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
         }
         MG_CUDA(cudaGetLastError());
         if (fixed_levels || optimistic) break;
@@ -3727,13 +3628,14 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
     for (int i = 0; i < 2; ++i) {
         ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
-        ENS(ctx->bins[i], 4ull * kNodeBinWords * C.tasks);
+        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
         ENS(ctx->cbkeys[i], 24ull * C.tasks);
         ENS(ctx->tile_task[i], 4ull * C.tiles);
         ENS(ctx->tile_begin[i], 4ull * C.tiles);
     }
     ENS(ctx->tile_hist, 4ull * 96 * C.tiles);  // [axis][bin][tile]
     ENS(ctx->tile_lt, 4ull * C.tiles);
+    ENS(ctx->bincode, 2ull * n);
     ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
     ENS(ctx->med_list, sizeof(Task) * (size_t)C.tasks);
     ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
@@ -4166,13 +4068,14 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
     ENS(ctx->rec[1], sizeof(Rec) * (size_t)n);
     for (int i = 0; i < 2; ++i) {
         ENS(ctx->tasks[i], sizeof(Task) * (size_t)C.tasks);
-        ENS(ctx->bins[i], 4ull * kNodeBinWords * C.tasks);
+        ENS(ctx->bins[i], 4ull * kBinWords * C.tasks);
         ENS(ctx->cbkeys[i], 24ull * C.tasks);
         ENS(ctx->tile_task[i], 4ull * C.tiles);
         ENS(ctx->tile_begin[i], 4ull * C.tiles);
     }
     ENS(ctx->tile_hist, 4ull * 96 * C.tiles);
     ENS(ctx->tile_lt, 4ull * C.tiles);
+    ENS(ctx->bincode, 2ull * n);
     ENS(ctx->dec, sizeof(Decision) * (size_t)C.tasks);
     ENS(ctx->med_list, sizeof(Task) * (size_t)C.tasks);
     ENS(ctx->medium, sizeof(Task) * (size_t)C.medium);
@@ -4594,13 +4497,7 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
                              (int)sizeof(MediumSmemSmall)) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<true, kMediumSmallCap>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmemSmall)) != cudaSuccess ||
-        cudaFuncSetAttribute(lvl_part_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTileBytes) != cudaSuccess ||
-        cudaFuncSetAttribute(lvl_bin_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTileBytes) != cudaSuccess ||
-        cudaFuncSetAttribute(lvl_bin_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTileBytes) != cudaSuccess) {
+                             (int)sizeof(MediumSmemSmall)) != cudaSuccess) {
         mgbvh_destroy(ctx);
         return MGBVH_ERR_CUDA;
     }
@@ -4624,7 +4521,7 @@ void mgbvh_destroy(mgbvh_ctx* ctx) {
                      &ctx->rbins, &ctx->tile_hist2, &ctx->med_list, &ctx->med_work, &ctx->med_off,
                      &ctx->med_seg, &ctx->med_keys[0], &ctx->med_keys[1], &ctx->med_vals[0],
                      &ctx->med_vals[1], &ctx->med_flag, &ctx->med_scan, &ctx->q, &ctx->qready,
-                     &ctx->qcb, &ctx->qstate};
+                     &ctx->qcb, &ctx->qstate, &ctx->bincode};
     for (DevBuf* b : all)
         if (b->p) cudaFree(b->p);
     if (ctx->h_qstate) cudaFreeHost(ctx->h_qstate);

@@ -80,7 +80,6 @@ enum ErrorSite : uint32_t {
     kSiteMedian = 4,       // forced median of a level-pass node: counts of its halves differ
     kSiteCapacity = 5,
     kSiteMeshIndex = 6,  // an instance names a mesh past the mesh count
-    kSiteBulkCopy = 7,   // a bulk copy into shared memory did not land within its bounded wait
 };
 
 __device__ __forceinline__ void set_error(Counters* c, int status, uint32_t site) {
@@ -614,48 +613,31 @@ __device__ void warp_build_subtree(float lo[3], float hi[3], uint32_t id, uint32
     }
 }
 
-// Segmented reductions over contiguous lane ranges [s, end); `mask` holds
-// exactly the lanes of the calling lane's range, and every lane of the warp
-// calls with its own range's mask (ranges are disjoint and cover the warp).
-#ifndef MGBVH_SEG_REDUX
-#define MGBVH_SEG_REDUX 0  // 1: redux.sync per range mask (measured 2.4x slower in the subtree kernels: different masks in one warp serialize); 0: shuffle-down tree bounded by the range end
-#endif
-__device__ __forceinline__ uint32_t seg_min(uint32_t v, uint32_t lane, uint32_t s, uint32_t end,
-                                            uint32_t mask) {
-#if MGBVH_SEG_REDUX
-    return __reduce_min_sync(mask, v);
-#else
+// Segmented reductions over contiguous lane ranges [s, end): shuffle-down
+// tree bounded by the segment end, then a broadcast from the segment's first
+// lane. Every lane takes part with full masks (per-segment masks in one
+// warp serialize: one pass per distinct mask).
+__device__ __forceinline__ uint32_t seg_min(uint32_t v, uint32_t lane, uint32_t s, uint32_t end) {
 #pragma unroll
     for (uint32_t d = 1; d < 32; d <<= 1) {
         const uint32_t u = __shfl_down_sync(kFull, v, d);
         if (lane + d < end) v = min(v, u);
     }
     return __shfl_sync(kFull, v, s);
-#endif
 }
 
-__device__ __forceinline__ uint32_t seg_max(uint32_t v, uint32_t lane, uint32_t s, uint32_t end,
-                                            uint32_t mask) {
-#if MGBVH_SEG_REDUX
-    return __reduce_max_sync(mask, v);
-#else
+__device__ __forceinline__ uint32_t seg_max(uint32_t v, uint32_t lane, uint32_t s, uint32_t end) {
 #pragma unroll
     for (uint32_t d = 1; d < 32; d <<= 1) {
         const uint32_t u = __shfl_down_sync(kFull, v, d);
         if (lane + d < end) v = max(v, u);
     }
     return __shfl_sync(kFull, v, s);
-#endif
 }
 
-// Lexicographic (hi, lo) minimum over the range.
+// Lexicographic (hi, lo) minimum over the segment.
 __device__ __forceinline__ void seg_min2(uint32_t& hi, uint32_t& lo, uint32_t lane, uint32_t s,
-                                         uint32_t end, uint32_t mask) {
-#if MGBVH_SEG_REDUX
-    const uint32_t h = __reduce_min_sync(mask, hi);
-    lo = __reduce_min_sync(mask, hi == h ? lo : 0xFFFFFFFFu);
-    hi = h;
-#else
+                                         uint32_t end) {
 #pragma unroll
     for (uint32_t d = 1; d < 32; d <<= 1) {
         const uint32_t uh = __shfl_down_sync(kFull, hi, d);
@@ -667,7 +649,6 @@ __device__ __forceinline__ void seg_min2(uint32_t& hi, uint32_t& lo, uint32_t la
     }
     hi = __shfl_sync(kFull, hi, s);
     lo = __shfl_sync(kFull, lo, s);
-#endif
 }
 
 // Lanes [s, s+n) as a mask.
@@ -740,8 +721,8 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         float cmn[3], ext[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            cmn[a] = funkey(seg_min(work ? fkey(c[a]) : kKeyPosInf, lane, ss, se, m));
-            const float cmx = funkey(seg_max(work ? fkey(c[a]) : kKeyNegInf, lane, ss, se, m));
+            cmn[a] = funkey(seg_min(work ? fkey(c[a]) : kKeyPosInf, lane, ss, se));
+            const float cmx = funkey(seg_max(work ? fkey(c[a]) : kKeyNegInf, lane, ss, se));
             ext[a] = __fsub_rn(cmx, cmn[a]);
         }
         const float sa_p = surface_area6(nb);
@@ -820,7 +801,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
         // first minimum per segment: (cost, axis, threshold index)
         uint32_t mh = static_cast<uint32_t>(best.key >> 32);
         uint32_t ml = static_cast<uint32_t>(best.key);
-        seg_min2(mh, ml, lane, ss, se, m);
+        seg_min2(mh, ml, lane, ss, se);
         const bool found = work && ml != kNoKey;
         bool median = false;
         uint32_t axis = 0, n_lt = 0;
@@ -860,10 +841,10 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
                 float ml6[6], mg6[6];
 #pragma unroll
                 for (int i = 0; i < 3; ++i) {
-                    ml6[i] = funkey(seg_min(in_lt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se, m));
-                    mg6[i] = funkey(seg_min(in_gt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se, m));
-                    ml6[3 + i] = funkey(seg_max(in_lt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se, m));
-                    mg6[3 + i] = funkey(seg_max(in_gt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se, m));
+                    ml6[i] = funkey(seg_min(in_lt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se));
+                    mg6[i] = funkey(seg_min(in_gt ? fkey(lo[i]) : kKeyPosInf, lane, ss, se));
+                    ml6[3 + i] = funkey(seg_max(in_lt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se));
+                    mg6[3 + i] = funkey(seg_max(in_gt ? fkey(hi[i]) : kKeyNegInf, lane, ss, se));
                 }
                 if (median) {
                     const uint32_t ck =
