@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -197,6 +198,7 @@ __global__ void __launch_bounds__(256) prep_indexed_kernel(const float* __restri
                                                            const uint32_t* __restrict__ tris,
                                                            uint32_t n, Rec* __restrict__ out,
                                                            Counters* ctr) {
+    pdl_enter();
     __shared__ uint32_t sk[12];
     if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
     __syncthreads();
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(256) prep_indexed_kernel(const float* __restri
 // Object records from AABBs (min xyz, max xyz): the AsBoundingVolume path.
 __global__ void __launch_bounds__(256) prep_aabbs_kernel(const float* __restrict__ aabbs, uint32_t n,
                                                          Rec* __restrict__ out, Counters* ctr) {
+    pdl_enter();
     __shared__ uint32_t sk[12];
     if (threadIdx.x < 12) sk[threadIdx.x] = ((threadIdx.x % 6) < 3) ? kKeyPosInf : kKeyNegInf;
     __syncthreads();
@@ -264,6 +267,7 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
                                  uint32_t* cbkeys, uint32_t* tile_task, uint32_t* tile_begin,
                                  Task* medium, Task* small, Out O, uint32_t ntiles,
                                  uint32_t max_depth) {
+    pdl_enter();
     float b[6];
     if (has_bounds) {
         b[0] = b0; b[1] = b1; b[2] = b2; b[3] = b3; b[4] = b4; b[5] = b5;
@@ -634,6 +638,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
 }
 
 __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
+    pdl_enter();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
@@ -655,6 +660,7 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_ke
     uint32_t* __restrict__ tile_hist, uint32_t cap_tiles, const Rec* __restrict__ rec0,
     const Rec* __restrict__ rec1, uint16_t* __restrict__ codes, Counters* __restrict__ ctr, uint32_t lv,
     Params P) {
+    pdl_enter();
     __shared__ uint32_t sb[kBinWords];
     if (blockIdx.x == 0 && threadIdx.x < 2) ctr->lvl[lvl_free(lv)][threadIdx.x] = 0;
     const uint32_t ntiles = ctr->lvl[lv][1];
@@ -748,6 +754,7 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
     uint32_t* __restrict__ tile_hist2, uint32_t cap_tiles, const Rec* __restrict__ rec0,
     const Rec* __restrict__ rec1, const Counters* __restrict__ ctr, uint32_t lv) {
+    pdl_enter();
     __shared__ uint32_t sb[kRBinWords];
     __shared__ float sthr[32];
     const uint32_t ntiles = ctr->lvl[lv][1];
@@ -937,6 +944,7 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
 }
 
 __global__ void __launch_bounds__(128) lvl_eval2_kernel(EvalArgs A, Params P, Out O) {
+    pdl_enter();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
@@ -959,6 +967,7 @@ __global__ void __launch_bounds__(256) lvl_sample_kernel(const Task* __restrict_
                                                          const Rec* __restrict__ rec1,
                                                          const Counters* __restrict__ ctr, uint32_t lv,
                                                          Params P, Learn LN) {
+    pdl_enter();
     __shared__ float3 slo[kSampleChunk], shi[kSampleChunk];
     __shared__ uint32_t rk[8], ra[8], rt[8];
     __shared__ float rthr[8];
@@ -1092,6 +1101,7 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_PART_MIN_BLOCKS) lvl_part_
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
     const uint32_t* __restrict__ tile_lt, Rec* rec0, Rec* rec1, const uint16_t* __restrict__ codes,
     uint32_t* next_cbkeys, uint32_t lv, Out O) {
+    pdl_enter();
     __shared__ uint32_t wcnt[kTileThreads / 32];
     __shared__ uint32_t sk[12];
     __shared__ int sbad;
@@ -2224,6 +2234,7 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? MGBVH_MEDIUM_LEARN_CT
                                                                 Rec* rec0, Rec* rec1, Task* small,
                                                                 uint32_t cap_small, Params P, Out O,
                                                                 Learn LN, const uint32_t* range) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
     // range (nullable): tasks [range[0], range[1]) instead of all of them
@@ -2254,6 +2265,7 @@ __device__ __forceinline__ void write_task_root(const Out& O, const Task& t) {
 // on.
 __global__ void __launch_bounds__(256) medium_count_kernel(const Task* __restrict__ tasks, Out O,
                                                            uint32_t slots) {
+    pdl_enter();
     const uint32_t n = O.ctr->n_medium;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const Task t = tasks[i];
@@ -2267,6 +2279,7 @@ __global__ void __launch_bounds__(256) medium_count_kernel(const Task* __restric
 // writes its own slots.
 __global__ void __launch_bounds__(256) medium_sort_kernel(const Task* __restrict__ in, Task* __restrict__ out,
                                                           Counters* __restrict__ ctr, uint32_t slots) {
+    pdl_enter();
     uint32_t off[kStreamChunks + 1];
     off[0] = 0;
 #pragma unroll
@@ -2302,6 +2315,7 @@ __global__ void __launch_bounds__(256) medium_sort_kernel(const Task* __restrict
 // (srange[c] is the previous chunk's end).
 __global__ void __launch_bounds__(256) small_select_kernel(const Task* __restrict__ in, Task* __restrict__ out,
                                                            uint32_t cap, Out O, uint32_t c, uint32_t slots) {
+    pdl_enter();
     __shared__ uint32_t last;
     Counters* ctr = O.ctr;
     const uint32_t n = ctr->n_small;
@@ -2339,6 +2353,7 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
                                                    const Rec* __restrict__ rec0,
                                                    const Rec* __restrict__ rec1, Params P, Out O,
                                                    const uint32_t* range) {
+    pdl_enter();
     __shared__ XRec xchg[8][32];
     const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
     const uint32_t w0 = range ? range[0] : 0u;
@@ -3324,6 +3339,30 @@ const char* site_text(uint32_t site) {
     }
 }
 
+#ifndef MGBVH_PDL
+#define MGBVH_PDL 1  // 1: pipeline kernels launched with programmatic stream serialization
+#endif
+
+// Launches a pipeline kernel on stream `st`. With MGBVH_PDL the launch
+// allows programmatic stream serialization: the kernel's CTAs may be
+// scheduled while the previous kernel in the stream finishes, and wait in
+// pdl_enter() (griddepcontrol.wait) until it has completed, so the launch
+// latency between dependent kernels overlaps the previous kernel's tail.
+template <typename... KArgs, typename... Args>
+void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = MGBVH_PDL ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);  // errors surface at cudaGetLastError
+}
+
 // Level passes (nodes above medium_max), then the medium and small subtree
 // kernels, on the context's stream. Root tasks are already queued.
 // fixed_levels > 0: launch exactly that many level passes and never read
@@ -3391,25 +3430,25 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             A.rbins = LN.w ? P_<uint32_t>(ctx->rbins) : nullptr;
             A.tile_hist2 = LN.w ? P_<uint32_t>(ctx->tile_hist2) : nullptr;
             A.med = P_<Task>(ctx->med_list);
-            lvl_bin_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+            launch_k(lvl_bin_kernel, tile_grid, kTileThreads, 0, sm,
                 P_<Task>(ctx->tasks[bf]), P_<uint32_t>(ctx->cbkeys[bf]), P_<uint32_t>(ctx->bins[bf]),
                 P_<uint32_t>(ctx->tile_task[bf]), P_<uint32_t>(ctx->tile_begin[bf]),
                 P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, P_<uint16_t>(ctx->bincode), d_ctr, lv, P);
-            lvl_eval_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+            launch_k(lvl_eval_kernel, eval_grid, 128, 0, sm, A, P, O);
             if (LN.samples) {
-                lvl_sample_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(
+                launch_k(lvl_sample_kernel, ctx->sm_count * 2, 256, 0, sm,
                     A.tasks, A.dec, A.bins, A.cbkeys, rec0, rec1, d_ctr, lv, P, LN);
                 launches++;
             }
             if (LN.w) {
-                lvl_refine_bin_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+                launch_k(lvl_refine_bin_kernel, tile_grid, kTileThreads, 0, sm,
                     A.tasks, A.cbkeys, A.refine, A.rbins, P_<uint32_t>(ctx->tile_task[bf]),
                     P_<uint32_t>(ctx->tile_begin[bf]), P_<uint32_t>(ctx->tile_hist2), C.tiles, rec0, rec1,
                     d_ctr, lv);
-                lvl_eval2_kernel<<<eval_grid, 128, 0, sm>>>(A, P, O);
+                launch_k(lvl_eval2_kernel, eval_grid, 128, 0, sm, A, P, O);
                 launches += 2;
             }
-            lvl_part_kernel<<<tile_grid, kTileThreads, 0, sm>>>(
+            launch_k(lvl_part_kernel, tile_grid, kTileThreads, 0, sm,
                 P_<Task>(ctx->tasks[bf]), P_<Decision>(ctx->dec), P_<uint32_t>(ctx->tile_task[bf]),
                 P_<uint32_t>(ctx->tile_begin[bf]), P_<uint32_t>(ctx->tile_lt), rec0, rec1,
                 P_<uint16_t>(ctx->bincode), P_<uint32_t>(ctx->cbkeys[nx]), lv, O);
@@ -3439,16 +3478,16 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * (uint32_t)MGBVH_MEDIUM_SMALL_CTAS);
         auto medium = [&](const Task* tasks, const uint32_t* range) {
             if (lrn && small_cap)
-                medium_kernel<true, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
+                launch_k(medium_kernel<true, kMediumSmallCap>, mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else if (lrn)
-                medium_kernel<true, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                launch_k(medium_kernel<true, kMediumMax>, mgrid, kMediumThreads, sizeof(MediumSmem), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else if (small_cap)
-                medium_kernel<false, kMediumSmallCap><<<mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm>>>(
+                launch_k(medium_kernel<false, kMediumSmallCap>, mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else
-                medium_kernel<false, kMediumMax><<<mgrid, kMediumThreads, sizeof(MediumSmem), sm>>>(
+                launch_k(medium_kernel<false, kMediumMax>, mgrid, kMediumThreads, sizeof(MediumSmem), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
         };
         // small subtrees: count read on the device; grid sized for full occupancy
@@ -3467,15 +3506,15 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             // the copy stream while the next chunks run.
             const uint32_t S = ctx->stream_slots;
             if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
-            medium_count_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->medium), O, S);
-            medium_sort_kernel<<<ctx->sm_count * 2, 256, 0, sm>>>(P_<Task>(ctx->medium), P_<Task>(ctx->medium2),
+            launch_k(medium_count_kernel, ctx->sm_count * 2, 256, 0, sm, P_<Task>(ctx->medium), O, S);
+            launch_k(medium_sort_kernel, ctx->sm_count * 2, 256, 0, sm, P_<Task>(ctx->medium), P_<Task>(ctx->medium2),
                                                                    d_ctr, S);
             launches += 2;
             for (uint32_t c = 0; c < kStreamChunks; ++c) {
                 medium(P_<Task>(ctx->medium2), d_ctr->mrange + c);
-                small_select_kernel<<<ctx->sm_count, 256, 0, sm>>>(P_<Task>(ctx->small), P_<Task>(ctx->small2),
+                launch_k(small_select_kernel, ctx->sm_count, 256, 0, sm, P_<Task>(ctx->small), P_<Task>(ctx->small2),
                                                                    C.small, O, c, S);
-                small<<<small_grid, ctx->small_threads, 0, sm>>>(P_<Task>(ctx->small2), rec0, rec1, P, O,
+                launch_k(small, small_grid, ctx->small_threads, 0, sm, P_<Task>(ctx->small2), rec0, rec1, P, O,
                                                          d_ctr->srange + c);
                 launches += 3;
                 MG_CUDA(cudaEventRecord(ctx->evs[c], sm));
@@ -3493,7 +3532,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             medium(P_<Task>(ctx->medium), nullptr);
             launches++;
             if (!fixed_levels) MG_CUDA(cudaEventRecord(ctx->evp[2], sm));
-            small<<<small_grid, ctx->small_threads, 0, sm>>>(P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
+            launch_k(small, small_grid, ctx->small_threads, 0, sm, P_<Task>(ctx->small), rec0, rec1, P, O, nullptr);
             launches++;
         }
         MG_CUDA(cudaGetLastError());
@@ -3680,10 +3719,10 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     MG_CUDA(cudaEventRecord(ctx->ev0, sm));
     const int prep_blocks = (int)std::min<uint32_t>((n + 255) / 256, 148u * 8u);
     if (in.kind == kIndexed)
-        prep_indexed_kernel<<<prep_blocks, 256, 0, sm>>>(in.verts, in.stride_bytes / 4, in.nverts,
+        launch_k(prep_indexed_kernel, prep_blocks, 256, 0, sm, in.verts, in.stride_bytes / 4, in.nverts,
                                                           in.tris, n, rec0, d_ctr);
     else
-        prep_aabbs_kernel<<<prep_blocks, 256, 0, sm>>>(in.aabbs, n, rec0, d_ctr);
+        launch_k(prep_aabbs_kernel, prep_blocks, 256, 0, sm, in.aabbs, n, rec0, d_ctr);
 
     const bool root_leaf = n <= 1 || st->max_depth == 0 ||
                            (n <= st->max_leaf_objects && n < 2u * st->min_leaf_objects);
@@ -3701,7 +3740,7 @@ int run_build(mgbvh_ctx* ctx, const Input& in, const mgbvh_settings* st, mgbvh_n
     const float* bb = st->bounds;
     {
         const int blocks = (int)std::min<uint32_t>((std::max(n, ntiles0) + 255) / 256 + 1, 1024u);
-        init_root_kernel<<<blocks, 256, 0, sm>>>(
+        launch_k(init_root_kernel, blocks, 256, 0, sm,
             n, cls, st->has_bounds, bb[0], bb[1], bb[2], bb[3], bb[4], bb[5], P_<Task>(ctx->tasks[0]),
             P_<uint32_t>(ctx->bins[0]), P_<uint32_t>(ctx->cbkeys[0]), P_<uint32_t>(ctx->tile_task[0]),
             P_<uint32_t>(ctx->tile_begin[0]), P_<Task>(ctx->medium), P_<Task>(ctx->small), O, ntiles0,

@@ -651,6 +651,18 @@ __device__ __forceinline__ void seg_min2(uint32_t& hi, uint32_t& lo, uint32_t la
     lo = __shfl_sync(kFull, lo, s);
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while its predecessor in the stream is
+// still finishing. griddepcontrol.wait blocks until the predecessor grid has
+// completed and its memory operations are visible (a no-op for an ordinary
+// launch); the kernel then lets its own dependent grid be scheduled. Called
+// first in every kernel of the build pipeline, before any read of a
+// predecessor's output.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Lanes [s, s+n) as a mask.
 __device__ __forceinline__ uint32_t seg_mask(uint32_t s, uint32_t n) {
     return n >= 32u ? kFull : (((1u << n) - 1u) << s);
