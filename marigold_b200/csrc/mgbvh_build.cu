@@ -2228,6 +2228,12 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
 #define MGBVH_MEDIUM_LEARN_CTAS 4  // learned-form subtree CTAs per SM the register budget must allow (tuning knob)
 #endif
 
+// The subtree CTA's dynamic shared memory.
+template <bool kLearn, uint32_t kCap>
+constexpr size_t medium_smem_bytes() {
+    return sizeof(MediumSmemT<kCap>);
+}
+
 template <bool kLearn, uint32_t kCap>
 __global__ void __launch_bounds__(kMediumThreads, kLearn ? MGBVH_MEDIUM_LEARN_CTAS : MGBVH_MEDIUM_SMALL_CTAS)
     medium_kernel(const Task* __restrict__ tasks,
@@ -3478,16 +3484,16 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             std::min<uint32_t>(C.medium, (uint32_t)ctx->sm_count * (uint32_t)MGBVH_MEDIUM_SMALL_CTAS);
         auto medium = [&](const Task* tasks, const uint32_t* range) {
             if (lrn && small_cap)
-                launch_k(medium_kernel<true, kMediumSmallCap>, mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm,
+                launch_k(medium_kernel<true, kMediumSmallCap>, mgrid_s, kMediumThreads, medium_smem_bytes<true, kMediumSmallCap>(), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else if (lrn)
-                launch_k(medium_kernel<true, kMediumMax>, mgrid, kMediumThreads, sizeof(MediumSmem), sm,
+                launch_k(medium_kernel<true, kMediumMax>, mgrid, kMediumThreads, medium_smem_bytes<true, kMediumMax>(), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else if (small_cap)
-                launch_k(medium_kernel<false, kMediumSmallCap>, mgrid_s, kMediumThreads, sizeof(MediumSmemSmall), sm,
+                launch_k(medium_kernel<false, kMediumSmallCap>, mgrid_s, kMediumThreads, medium_smem_bytes<false, kMediumSmallCap>(), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
             else
-                launch_k(medium_kernel<false, kMediumMax>, mgrid, kMediumThreads, sizeof(MediumSmem), sm,
+                launch_k(medium_kernel<false, kMediumMax>, mgrid, kMediumThreads, medium_smem_bytes<false, kMediumMax>(), sm,
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
         };
         // small subtrees: count read on the device; grid sized for full occupancy
@@ -4528,15 +4534,15 @@ int mgbvh_create(int device, mgbvh_ctx** out_ctx) {
         cudaMallocHost(&ctx->h_ctr, sizeof(Counters)) != cudaSuccess ||
         cudaMallocHost(&ctx->h_init, sizeof(Counters)) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmem)) != cudaSuccess ||
+                             (int)medium_smem_bytes<false, kMediumMax>()) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<true, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmem)) != cudaSuccess ||
+                             (int)medium_smem_bytes<true, kMediumMax>()) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<false, kMediumSmallCap>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmemSmall)) != cudaSuccess ||
+                             (int)medium_smem_bytes<false, kMediumSmallCap>()) != cudaSuccess ||
         cudaFuncSetAttribute(medium_kernel<true, kMediumSmallCap>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmemSmall)) != cudaSuccess) {
+                             (int)medium_smem_bytes<true, kMediumSmallCap>()) != cudaSuccess) {
         mgbvh_destroy(ctx);
         return MGBVH_ERR_CUDA;
     }
@@ -4884,7 +4890,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
     int sms = 0;
     if (cudaGetSymbolAddress(&addr, g_noalloc_scratch) != cudaSuccess || !addr) return MGBVH_ERR_CUDA;
     if (cudaFuncSetAttribute(medium_kernel<false, kMediumMax>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(MediumSmem)) != cudaSuccess)
+                             (int)medium_smem_bytes<false, kMediumMax>()) != cudaSuccess)
         return MGBVH_ERR_CUDA;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0)
         return MGBVH_ERR_CUDA;
@@ -4918,7 +4924,7 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
                                                       nullptr, nullptr, S->medium, S->small, O, 0u,
                                                       st->max_depth);
     if (cls == 2)
-        medium_kernel<false, kMediumMax><<<1, kMediumThreads, sizeof(MediumSmem), sm>>>(
+        medium_kernel<false, kMediumMax><<<1, kMediumThreads, medium_smem_bytes<false, kMediumMax>(), sm>>>(
             S->medium, S->rec, S->rec, S->small, kNoAllocMax / 2 + 8, P, O, Learn{nullptr, 0, nullptr, 0, nullptr},
             nullptr);
     if (cls != 0) {
