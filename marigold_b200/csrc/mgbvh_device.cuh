@@ -699,113 +699,6 @@ __device__ __forceinline__ void warp_exchange(uint32_t dst, uint32_t lane, float
     __syncwarp();
 }
 
-#ifndef MGBVH_PAIR_STEP
-#define MGBVH_PAIR_STEP 0  // 1: two-object segments are split in closed form when their parent splits
-#endif
-
-// One object's box grown from the empty box, as the sweep merges it.
-__device__ __forceinline__ void box_of(const float* l, const float* h, float* b) {
-    box_empty(b);
-    b[0] = fminf(b[0], l[0]);
-    b[1] = fminf(b[1], l[1]);
-    b[2] = fminf(b[2], l[2]);
-    b[3] = fmaxf(b[3], h[0]);
-    b[4] = fmaxf(b[4], h[1]);
-    b[5] = fmaxf(b[5], h[2]);
-}
-
-// A segment of two objects (lanes s, s + 1; the leaf rule does not stop it)
-// split at once instead of by one more pass of the level loop, with the
-// same result as that pass when leaves hold one object (max_leaf < 2, so no
-// cost-based leaf): lane k's candidates on each axis are its own centroid
-// as threshold, valid where the other object's centroid is strictly below
-// it (lt = that object, gt = lane k's own); their cost does not depend on
-// the axis, so lane k's first valid axis is its candidate; the smaller
-// (cost, axis, lane) key of the two lanes wins (bvh/src/lib.rs:392-442 with
-// steps = one centroid per object, :505-520). The parent node and both
-// one-object leaves are written, and the permutation entries. A pair with no
-// valid candidate (coincident or NaN centroids: the forced median) stays in
-// the level loop.
-__device__ __forceinline__ void pair_step(bool& live, uint32_t s, uint32_t n, uint32_t slot, uint32_t pair,
-                                          uint32_t depth, const float* nb, const float* lo, const float* hi,
-                                          uint32_t id, uint32_t lane, uint32_t base, uint32_t nbase, uint32_t tbase,
-                                          const Params& P, const Out& O, bool& any_split, uint32_t& hmax) {
-    const bool is_pair = live && n == 2u && P.max_leaf < 2u;
-    if (!__any_sync(kFull, is_pair)) return;
-    const uint32_t k = lane - s;  // 0 or 1 on a pair's lanes
-    const uint32_t partner = is_pair ? s + 1u - k : lane;
-    float ol[3], oh[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        ol[i] = __shfl_sync(kFull, lo[i], partner);
-        oh[i] = __shfl_sync(kFull, hi[i], partner);
-    }
-    const uint32_t oid = __shfl_sync(kFull, id, partner);
-    if (!is_pair) return;
-    // object 0 (lane s) and object 1 (lane s + 1)
-    float l0[3], h0[3], l1[3], h1[3], c0[3], c1[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        l0[i] = k == 0u ? lo[i] : ol[i];
-        h0[i] = k == 0u ? hi[i] : oh[i];
-        l1[i] = k == 0u ? ol[i] : lo[i];
-        h1[i] = k == 0u ? oh[i] : hi[i];
-        c0[i] = center_of(l0[i], h0[i]);
-        c1[i] = center_of(l1[i], h1[i]);
-    }
-    float b0[6], b1[6];
-    box_of(l0, h0, b0);
-    box_of(l1, h1, b1);
-    const float sa_p = surface_area6(nb);
-    // lane 0's candidate: lt = object 1, gt = object 0; lane 1's: the reverse
-    uint64_t key = ~0ull;
-#pragma unroll
-    for (uint32_t kk = 0; kk < 2u; ++kk) {
-        uint32_t ax = 3u;
-#pragma unroll
-        for (int a = 2; a >= 0; --a) {
-            const bool v = kk == 0u ? c1[a] < c0[a] : c0[a] < c1[a];
-            if (v) ax = static_cast<uint32_t>(a);
-        }
-        if (ax == 3u) continue;
-        const float cost = kk == 0u ? split_cost(surface_area6(b1), surface_area6(b0), sa_p, 1u, 1u)
-                                    : split_cost(surface_area6(b0), surface_area6(b1), sa_p, 1u, 1u);
-        const uint64_t kq = cand_key(cost, ax, kk);
-        if (kq < key) key = kq;
-    }
-    if (key == ~0ull) return;  // the forced median: left to the level loop
-    const uint32_t kw = static_cast<uint32_t>(key) & 0xFFu;  // lane whose object goes to gt
-    // lt: object 1 - kw at position s; gt: object kw at position s + 1
-    float blt[6], bgt[6], clt[3], cgt[3];
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        blt[i] = kw == 0u ? b1[i] : b0[i];
-        bgt[i] = kw == 0u ? b0[i] : b1[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        clt[i] = kw == 0u ? c1[i] : c0[i];
-        cgt[i] = kw == 0u ? c0[i] : c1[i];
-    }
-    if (k == 0u) {
-        if (!box_contains(blt, clt[0], clt[1], clt[2]) || !box_contains(bgt, cgt[0], cgt[1], cgt[2]))
-            set_error(O.ctr, MGBVH_ERR_ASSERT, kSiteContain);  // bvh/src/lib.rs:637-646
-        lane_store_node(O, nbase + slot, nb, base + s - tbase, 2u, pair);
-        lane_store_node(O, nbase + pair + 1u, blt, base + s - tbase, 1u, 0u);
-        lane_store_node(O, nbase + pair, bgt, base + s + 1u - tbase, 1u, 0u);
-        any_split = true;
-        hmax = max(hmax, depth);
-    }
-    // position s + k takes the lt object's id (k = 0) or the gt object's (k = 1)
-    const uint32_t own_obj = k, want = k == 0u ? 1u - kw : kw;
-    O.perm[base + s + k] = want == own_obj ? id : oid;
-    live = false;
-}
-
-#ifndef MGBVH_EARLY_LEAF
-#define MGBVH_EARLY_LEAF 1  // 1: leaf children are written when their parent splits
-#endif
-
 // Level-synchronous form of warp_build_subtree: every node of one depth of
 // the subtree is evaluated at the same time, each on its own lane range
 // (segment), with segmented warp reductions. Valid when every node of the
@@ -1032,7 +925,7 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             depth++;
             // a child that the leaf rule stops (:556) is written now rather
             // than by one more pass of the loop (the same node and entries)
-            if (MGBVH_EARLY_LEAF && (n <= 1u || depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf))) {
+            if (n <= 1u || depth == P.max_depth || (n <= P.max_leaf && n < 2u * P.min_leaf)) {
                 if (lane == s) {
                     lane_store_node(O, nbase + slot, nb, base + s - tbase, n, 0u);
                     if (n > 1u) {
@@ -1045,8 +938,6 @@ __device__ void warp_build_subtree_levels(float lo[3], float hi[3], uint32_t id,
             }
         }
         if (leaf) live = false;
-        if (MGBVH_PAIR_STEP) pair_step(live, s, n, slot, pair, depth, nb, lo, hi, id, lane, base, nbase, tbase, P, O,
-                                       any_split, hmax);
     }
     // counters: one atomic per warp
     const uint32_t hm = __reduce_max_sync(kFull, any_split ? hmax : 0u);
