@@ -517,6 +517,9 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     if (lane == 0) A.dec[w] = d;
 }
 
+// kLearn: with the learned form's network (a separate instantiation keeps
+// the plain evaluation's code small: a cold kernel fetches every instruction).
+template <bool kLearn>
 __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint32_t w, uint32_t lane) {
     const Task t = A.tasks[w];
     const uint32_t* tb = A.bins + (size_t)w * kBinWords;
@@ -605,7 +608,7 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
         d.ltb[i] = win.lt[i];
         d.gtb[i] = win.gt[i];
     }
-    if (A.lw && B == 32u && t.len >= A.lmin_n) {
+    if (kLearn && A.lw && B == 32u && t.len >= A.lmin_n) {
         // the learned form: run the network; with proposals to score, the
         // decision waits for the refine pass (lvl_eval2_kernel)
         const float cb[6] = {cmn[0], cmn[1], cmn[2], funkey(A.cbkeys[6 * w + 3]),
@@ -637,13 +640,14 @@ __device__ void eval_task(const EvalArgs& A, const Params& P, const Out& O, uint
     emit_split(A, P, O, w, lane, t, d, A.tile_hist, d.axis * 32u + d.split_bin);
 }
 
+template <bool kLearn>
 __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out O) {
     pdl_enter();
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_tasks; w += nwarps)
-        eval_task(A, P, O, w, lane);
+        eval_task<kLearn>(A, P, O, w, lane);
 }
 
 // Per-tile bin histograms (count + AABB per axis and bin) of the large nodes
@@ -3440,7 +3444,7 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 P_<Task>(ctx->tasks[bf]), P_<uint32_t>(ctx->cbkeys[bf]), P_<uint32_t>(ctx->bins[bf]),
                 P_<uint32_t>(ctx->tile_task[bf]), P_<uint32_t>(ctx->tile_begin[bf]),
                 P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, P_<uint16_t>(ctx->bincode), d_ctr, lv, P);
-            launch_k(lvl_eval_kernel, eval_grid, 128, 0, sm, A, P, O);
+            launch_k(LN.w ? lvl_eval_kernel<true> : lvl_eval_kernel<false>, eval_grid, 128, 0, sm, A, P, O);
             if (LN.samples) {
                 launch_k(lvl_sample_kernel, ctx->sm_count * 2, 256, 0, sm,
                     A.tasks, A.dec, A.bins, A.cbkeys, rec0, rec1, d_ctr, lv, P, LN);
