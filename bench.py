@@ -517,7 +517,7 @@ def run_mixed(args):
     """The large mixed scene: 16,777,216 triangles (8,388,608 in 64 Gaussian
     blobs, a 2048 x 1024-quad ground grid, 4,194,304 thin 1:200 triangles),
     built twice, plain (the reference profile) and learned (the committed
-    split proposer, refine gate on), then 8,388,608 closest-hit rays with
+    split proposer with the recommended gate), then 8,388,608 closest-hit rays with
     origins uniform in the scene box grown by 10% and uniform directions on
     each tree. Each traversal is checked hit for hit against GPU brute force
     on a 65,536-ray subset (the brute-force kernel is itself checked against
@@ -566,6 +566,7 @@ def run_mixed(args):
     clocks = ClockSampler(0).__enter__()  # sampled through every timed build and trace below
     for form in ("plain", "learned"):
         ctx.set_split_proposer(weights if form == "learned" else None, True)
+        ctx.set_proposer_gate(*(learned.RECOMMENDED_GATE if form == "learned" else (0.0, 0)))
         build_ms, count, st = [], 0, {}
         for k in range(max(args.warmup, 1) + args.steps):
             flush.fill_(k & 0xFF)

@@ -204,6 +204,7 @@ __global__ void __launch_bounds__(256) prep_indexed_kernel(const float* __restri
     __syncthreads();
     uint32_t k[12];
     init_key12(k);
+    const bool vec4 = (stride_floats & 3u) == 0u && (reinterpret_cast<uintptr_t>(verts) & 15u) == 0u;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t t0 = tris[3 * (size_t)i], t1 = tris[3 * (size_t)i + 1], t2 = tris[3 * (size_t)i + 2];
         if (t0 >= nverts || t1 >= nverts || t2 >= nverts) {
@@ -213,11 +214,28 @@ __global__ void __launch_bounds__(256) prep_indexed_kernel(const float* __restri
         const float* p0 = verts + (size_t)t0 * stride_floats;
         const float* p1 = verts + (size_t)t1 * stride_floats;
         const float* p2 = verts + (size_t)t2 * stride_floats;
+        float v0[3], v1[3], v2[3];
+        if (vec4) {
+            // 16-byte vertex rows: one load per vertex (the position and
+            // the next word of the row, which is not used)
+            const float4 a = __ldg(reinterpret_cast<const float4*>(p0));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(p1));
+            const float4 c = __ldg(reinterpret_cast<const float4*>(p2));
+            v0[0] = a.x, v0[1] = a.y, v0[2] = a.z;
+            v1[0] = b.x, v1[1] = b.y, v1[2] = b.z;
+            v2[0] = c.x, v2[1] = c.y, v2[2] = c.z;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                v0[q] = __ldg(p0 + q);
+                v1[q] = __ldg(p1 + q);
+                v2[q] = __ldg(p2 + q);
+            }
+        }
         float lo[3], hi[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float x0 = __fadd_rn(__ldg(p0 + a), 0.0f), x1 = __fadd_rn(__ldg(p1 + a), 0.0f),
-                        x2 = __fadd_rn(__ldg(p2 + a), 0.0f);
+            const float x0 = __fadd_rn(v0[a], 0.0f), x1 = __fadd_rn(v1[a], 0.0f), x2 = __fadd_rn(v2[a], 0.0f);
             lo[a] = fminf(fminf(x0, x1), x2);
             hi[a] = fmaxf(fmaxf(x0, x1), x2);
         }
