@@ -535,6 +535,12 @@ __device__ void emit_split(const EvalArgs& A, const Params& P, const Out& O, uin
     if (lane == 0) A.dec[w] = d;
 }
 
+// transposed network parameters as 16-byte vectors (the learned evaluation
+// stages them in shared memory)
+constexpr uint32_t kEvalWeightVec = mgbvh_mlp::kTParams * 2u / 16u;
+static_assert(mgbvh_mlp::kTParams * 2u % 16u == 0u, "the transposed parameters are whole 16-byte vectors");
+constexpr size_t kEvalWeightBytes = mgbvh_mlp::kTParams * 2u;
+
 // kLearn: with the learned form's network (a separate instantiation keeps
 // the plain evaluation's code small: a cold kernel fetches every instruction).
 template <bool kLearn>
@@ -664,6 +670,20 @@ __global__ void __launch_bounds__(128) lvl_eval_kernel(EvalArgs A, Params P, Out
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n_tasks = O.ctr->lvl[A.lv][0];
     const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+    if constexpr (kLearn) {
+        // the network's parameters staged in shared memory by the whole CTA
+        // (19.8 KB, coalesced), so each forward pass reads them at shared-memory
+        // latency instead of one dependent L2 round trip per group of inputs
+        extern __shared__ __align__(16) unsigned char eval_dsm[];
+        if (blockIdx.x * (blockDim.x >> 5) >= n_tasks) return;  // block-uniform: no node here
+        if (A.lw) {
+            const uint4* gw = reinterpret_cast<const uint4*>(A.lw);
+            uint4* sw = reinterpret_cast<uint4*>(eval_dsm);
+            for (uint32_t i = threadIdx.x; i < kEvalWeightVec; i += blockDim.x) sw[i] = gw[i];
+            __syncthreads();
+            A.lw = reinterpret_cast<const __nv_bfloat16*>(eval_dsm);
+        }
+    }
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_tasks; w += nwarps)
         eval_task<kLearn>(A, P, O, w, lane);
 }
@@ -765,17 +785,41 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_ke
     }
 }
 
+// The coarse-bin window of a proposal (bucket q of 16 on an axis whose
+// centroid range is [cmin, cmin + ext]): objects whose 32-bin index on that
+// axis is below lo lie below every one of the proposal's thresholds
+// (interval 0), above hi above every one (interval 16), and only the rest
+// need their centroid compared. The 16 thresholds span
+// [cmin + ext * (16q + 1) / 256, cmin + ext * (q + 1) / 16], and the coarse
+// bins outside [2q - 1, 2q + 2] are at least ext / 32 away from them, far
+// more than the rounding of the bin index (a few ulps of ext) and of the
+// thresholds (an ulp of the coordinates), as long as the coordinates are
+// within 2^14 extents of the origin; else (or without bin codes) the window
+// is every bin and every object is compared, as before.
+__device__ __forceinline__ bool refine_window(float cmin, float ext, uint32_t q, uint32_t& lo, uint32_t& hi) {
+    const float cmax = __fadd_rn(cmin, ext);
+    const bool ok = kPartCodes && ext > 0.0f && ext < 3.0e38f && fabsf(cmin) <= __fmul_rn(ext, 16384.0f) &&
+                    fabsf(cmax) <= __fmul_rn(ext, 16384.0f);
+    lo = ok && q > 0u ? 2u * q - 1u : 0u;
+    hi = ok ? min(2u * q + 2u, 31u) : 31u;
+    return ok;
+}
+
 // Interval bins of the pending nodes: for each proposal, the node's objects
 // by the interval of their centroid among the proposal's 16 thresholds
 // (count + AABB keys), with shared-memory atomics, merged into the node's
-// global interval bins; per-tile running counts go to tile_hist2. Grid-stride over
-// the level's tiles.
+// global interval bins; per-tile running counts go to tile_hist2. Only the
+// objects inside the proposal's coarse-bin window (refine_window) are read
+// and compared: the bin pass's codes place the others, whose counts come
+// from the tile's bin prefix counts here and whose boxes come from the
+// node's coarse bins in lvl_eval2. Grid-stride over the level's tiles.
 __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys,
     const LvlRefine* __restrict__ refine, uint32_t* __restrict__ rbins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
-    uint32_t* __restrict__ tile_hist2, uint32_t cap_tiles, const Rec* __restrict__ rec0,
-    const Rec* __restrict__ rec1, const Counters* __restrict__ ctr, uint32_t lv) {
+    uint32_t* __restrict__ tile_hist2, const uint32_t* __restrict__ tile_hist, uint32_t cap_tiles,
+    const Rec* __restrict__ rec0, const Rec* __restrict__ rec1, const uint16_t* __restrict__ codes,
+    const Counters* __restrict__ ctr, uint32_t lv) {
     pdl_enter();
     __shared__ uint32_t sb[kRBinWords];
     __shared__ float sthr[32];
@@ -789,7 +833,7 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
             const uint32_t f7 = i % 7u;
             sb[i] = f7 == 0 ? 0u : (f7 <= 3 ? kKeyPosInf : kKeyNegInf);
         }
-        uint32_t ax[2];
+        uint32_t ax[2], wlo[2], whi[2];
         bool act[2];
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
@@ -797,6 +841,7 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
             const float cmin = funkey(cbkeys[6 * ti + ax[p]]);
             const float ext = __fsub_rn(funkey(cbkeys[6 * ti + 3 + ax[p]]), cmin);
             act[p] = ext > 0.0f;
+            refine_window(cmin, ext, R.prop[p] & 15u, wlo[p], whi[p]);
             if (threadIdx.x >= 16u * p && threadIdx.x < 16u * (p + 1))
                 sthr[threadIdx.x] = proposal_threshold(cmin, ext, R.prop[p] & 15u, threadIdx.x & 15u);
         }
@@ -805,30 +850,27 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
         const uint32_t begin = tile_begin[tile];
         const uint32_t cnt = min(kTile, t.len - begin);
         const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
-        // warp-uniform trip count: the first and last intervals (objects on
-        // either side of the proposal's bucket, most of them, and spatially
-        // coherent) are merged across the warp and updated by one lane each;
-        // objects inside the bucket update their interval lane by lane
-        const uint32_t lane = threadIdx.x & 31u;
-        for (uint32_t i0 = 0; i0 < cnt; i0 += blockDim.x) {
-            const uint32_t i = i0 + threadIdx.x;
-            const bool valid = i < cnt;
-            float l[3] = {0.0f, 0.0f, 0.0f}, h[3] = {0.0f, 0.0f, 0.0f};
-            if (valid) {
-                const float4 lo = src[i].lo, hi = src[i].hi;
-                l[0] = lo.x;
-                l[1] = lo.y;
-                l[2] = lo.z;
-                h[0] = hi.x;
-                h[1] = hi.y;
-                h[2] = hi.z;
+        const uint16_t* cs = codes + t.start + begin;
+        const bool all0 = wlo[0] == 0u && whi[0] == 31u, all1 = wlo[1] == 0u && whi[1] == 31u;
+        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
+            bool in[2];
+            if (all0 && all1) {
+                in[0] = in[1] = true;
+            } else {
+                const uint32_t code = cs[i];
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    const uint32_t b = (code >> (5u * ax[p])) & 31u;
+                    in[p] = b >= wlo[p] && b <= whi[p];
+                }
             }
-            const uint32_t kl[3] = {fkey(l[0]), fkey(l[1]), fkey(l[2])};
-            const uint32_t kh[3] = {fkey(h[0]), fkey(h[1]), fkey(h[2])};
+            if (!((act[0] && in[0]) || (act[1] && in[1]))) continue;
+            const float4 lo = src[i].lo, hi = src[i].hi;
+            const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
 #pragma unroll
             for (int p = 0; p < 2; ++p) {
-                if (!act[p]) continue;  // block-uniform
-                const float c = center_of(l[ax[p]], h[ax[p]]);
+                if (!act[p] || !in[p]) continue;
+                const float c = center_of(sel3(l, ax[p]), sel3(h, ax[p]));
                 // interval = number of thresholds thr with !(c < thr)
                 uint32_t lo_i = 0, hi_i = 16;
 #pragma unroll
@@ -841,49 +883,21 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
                             hi_i = mid;
                     }
                 }
-#if MGBVH_REFINE_AGG
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const uint32_t iv = e ? 16u : 0u;
-                    const bool in = valid && lo_i == iv;
-                    const uint32_t g = __ballot_sync(kFull, in);
-                    if (g == 0u) continue;  // warp-uniform
-                    uint32_t m[6];
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        m[q] = __reduce_min_sync(kFull, in ? kl[q] : kKeyPosInf);
-                        m[3 + q] = __reduce_max_sync(kFull, in ? kh[q] : kKeyNegInf);
-                    }
-                    if (lane == static_cast<uint32_t>(e)) {
-                        uint32_t* wd = sb + (p * 17 + iv) * 7;
-                        atomicAdd(wd, static_cast<uint32_t>(__popc(g)));
-                        atomicMin(wd + 1, m[0]);
-                        atomicMin(wd + 2, m[1]);
-                        atomicMin(wd + 3, m[2]);
-                        atomicMax(wd + 4, m[3]);
-                        atomicMax(wd + 5, m[4]);
-                        atomicMax(wd + 6, m[5]);
-                    }
-                }
-                if (valid && lo_i != 0u && lo_i != 16u) {
-#else
-                if (valid) {
-#endif
-                    uint32_t* wd = sb + (p * 17 + lo_i) * 7;
-                    atomicAdd(wd, 1u);
-                    atomicMin(wd + 1, kl[0]);
-                    atomicMin(wd + 2, kl[1]);
-                    atomicMin(wd + 3, kl[2]);
-                    atomicMax(wd + 4, kh[0]);
-                    atomicMax(wd + 5, kh[1]);
-                    atomicMax(wd + 6, kh[2]);
-                }
+                uint32_t* wd = sb + (p * 17 + lo_i) * 7;
+                atomicAdd(wd, 1u);
+                atomicMin(wd + 1, fkey(l[0]));
+                atomicMin(wd + 2, fkey(l[1]));
+                atomicMin(wd + 3, fkey(l[2]));
+                atomicMax(wd + 4, fkey(h[0]));
+                atomicMax(wd + 5, fkey(h[1]));
+                atomicMax(wd + 6, fkey(h[2]));
             }
         }
         __syncthreads();
         if (threadIdx.x < 64) {
             // per proposal (one warp each): the tile's count of objects in
-            // intervals 0..j, an inclusive scan over the 17 intervals
+            // intervals 0..j, an inclusive scan over the 17 intervals, plus
+            // the tile's objects below the window (interval 0 by their bin)
             const uint32_t lane = threadIdx.x & 31u, p = threadIdx.x >> 5;
             const uint32_t c = lane < 17 ? sb[(p * 17 + lane) * 7] : 0u;
             uint32_t inc = c;
@@ -892,7 +906,9 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
                 const uint32_t u = __shfl_up_sync(kFull, inc, off);
                 if (lane >= static_cast<uint32_t>(off)) inc += u;
             }
-            if (lane < 17) tile_hist2[(size_t)(p * 17 + lane) * cap_tiles + tile] = inc;
+            const uint32_t below = wlo[p] ? tile_hist[(size_t)(ax[p] * 32u + wlo[p]) * cap_tiles + tile] : 0u;
+            if (lane < 16) tile_hist2[(size_t)(p * 17 + lane) * cap_tiles + tile] = inc + below;
+            if (lane == 16) tile_hist2[(size_t)(p * 17 + 16) * cap_tiles + tile] = cnt;
         }
         uint32_t* gb = rbins + (size_t)ti * kRBinWords;
         for (uint32_t k = threadIdx.x; k < kRBinWords; k += blockDim.x) {
@@ -926,6 +942,47 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
     box_empty(lt);
     box_empty(gt);
     uint32_t nl = 0, ng = 0;
+    // the objects outside the proposal's coarse-bin window: the node's coarse
+    // bins below it (interval 0) and above it (interval 16), merged across
+    // the proposal's 16 lanes (lane k takes bins k and k + 16)
+    uint32_t win_lo = 0, win_hi = 31;
+    refine_window(cmin, ext, R.prop[p] & 15u, win_lo, win_hi);
+    uint32_t e0 = 0, e16 = 0;
+    uint32_t k0[6] = {kKeyPosInf, kKeyPosInf, kKeyPosInf, kKeyNegInf, kKeyNegInf, kKeyNegInf};
+    uint32_t k16[6] = {kKeyPosInf, kKeyPosInf, kKeyPosInf, kKeyNegInf, kKeyNegInf, kKeyNegInf};
+    const uint32_t* cbn = A.bins + (size_t)w * kBinWords + a * 32u * 7u;
+#pragma unroll
+    for (uint32_t h = 0; h < 2; ++h) {
+        const uint32_t bin = k + 16u * h;
+        const bool lo_side = bin < win_lo, hi_side = bin > win_hi;
+        if (!(lo_side || hi_side)) continue;
+        const uint32_t* bw = cbn + bin * 7u;
+        const uint32_t c = bw[0];
+        if (c == 0) continue;
+        if (lo_side)
+            e0 += c;
+        else
+            e16 += c;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const uint32_t v = bw[1 + i];
+            if (lo_side)
+                k0[i] = i < 3 ? min(k0[i], v) : max(k0[i], v);
+            else
+                k16[i] = i < 3 ? min(k16[i], v) : max(k16[i], v);
+        }
+    }
+#pragma unroll
+    for (int off = 8; off > 0; off >>= 1) {  // within the proposal's 16 lanes
+        e0 += __shfl_xor_sync(kFull, e0, off);
+        e16 += __shfl_xor_sync(kFull, e16, off);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            const uint32_t u0 = __shfl_xor_sync(kFull, k0[i], off), u16 = __shfl_xor_sync(kFull, k16[i], off);
+            k0[i] = i < 3 ? min(k0[i], u0) : max(k0[i], u0);
+            k16[i] = i < 3 ? min(k16[i], u16) : max(k16[i], u16);
+        }
+    }
     uint32_t cj[17];
 #pragma unroll
     for (uint32_t j = 0; j < 17; ++j) cj[j] = rb[j * 7];  // all counts in flight at once
@@ -940,6 +997,16 @@ __device__ void eval2_task(const EvalArgs& A, const Params& P, const Out& O, uin
             ng += c;
         box_grow2(lt, gt, j <= k, funkey(b[1]), funkey(b[2]), funkey(b[3]), funkey(b[4]), funkey(b[5]),
                   funkey(b[6]));
+    }
+    if (e0) {  // interval 0 is on the lt side of every threshold
+        nl += e0;
+        box_grow2(lt, gt, true, funkey(k0[0]), funkey(k0[1]), funkey(k0[2]), funkey(k0[3]), funkey(k0[4]),
+                  funkey(k0[5]));
+    }
+    if (e16) {  // interval 16 is on the gt side of every threshold
+        ng += e16;
+        box_grow2(lt, gt, false, funkey(k16[0]), funkey(k16[1]), funkey(k16[2]), funkey(k16[3]),
+                  funkey(k16[4]), funkey(k16[5]));
     }
     const float nb[6] = {t.lo[0], t.lo[1], t.lo[2], t.hi[0], t.hi[1], t.hi[2]};
     uint64_t key = ~0ull;
@@ -3462,7 +3529,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                 P_<Task>(ctx->tasks[bf]), P_<uint32_t>(ctx->cbkeys[bf]), P_<uint32_t>(ctx->bins[bf]),
                 P_<uint32_t>(ctx->tile_task[bf]), P_<uint32_t>(ctx->tile_begin[bf]),
                 P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, P_<uint16_t>(ctx->bincode), d_ctr, lv, P);
-            launch_k(LN.w ? lvl_eval_kernel<true> : lvl_eval_kernel<false>, eval_grid, 128, 0, sm, A, P, O);
+            launch_k(LN.w ? lvl_eval_kernel<true> : lvl_eval_kernel<false>, eval_grid, 128, LN.w ? kEvalWeightBytes : 0,
+                     sm, A, P, O);
             if (LN.samples) {
                 launch_k(lvl_sample_kernel, ctx->sm_count * 2, 256, 0, sm,
                     A.tasks, A.dec, A.bins, A.cbkeys, rec0, rec1, d_ctr, lv, P, LN);
@@ -3471,8 +3539,8 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
             if (LN.w) {
                 launch_k(lvl_refine_bin_kernel, tile_grid, kTileThreads, 0, sm,
                     A.tasks, A.cbkeys, A.refine, A.rbins, P_<uint32_t>(ctx->tile_task[bf]),
-                    P_<uint32_t>(ctx->tile_begin[bf]), P_<uint32_t>(ctx->tile_hist2), C.tiles, rec0, rec1,
-                    d_ctr, lv);
+                    P_<uint32_t>(ctx->tile_begin[bf]), P_<uint32_t>(ctx->tile_hist2),
+                    P_<uint32_t>(ctx->tile_hist), C.tiles, rec0, rec1, P_<uint16_t>(ctx->bincode), d_ctr, lv);
                 launch_k(lvl_eval2_kernel, eval_grid, 128, 0, sm, A, P, O);
                 launches += 2;
             }
