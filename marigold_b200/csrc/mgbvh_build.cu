@@ -796,9 +796,21 @@ __global__ void __launch_bounds__(kTileThreads, MGBVH_BIN_MIN_BLOCKS) lvl_bin_ke
 // thresholds (an ulp of the coordinates), as long as the coordinates are
 // within 2^14 extents of the origin; else (or without bin codes) the window
 // is every bin and every object is compared, as before.
+#ifndef MGBVH_REFINE_WINDOW
+#define MGBVH_REFINE_WINDOW 1  // 0: the refine pass compares every object (no coarse-bin window)
+#endif
+#ifndef MGBVH_REFINE_BATCH
+#define MGBVH_REFINE_BATCH 4  // objects a thread of the refine pass handles at a time (tuning knob; divides 8)
+#endif
+#ifndef MGBVH_REFINE_MIN_BLOCKS
+#define MGBVH_REFINE_MIN_BLOCKS 4  // refine-pass CTAs per SM the register budget must allow (tuning knob)
+#endif
+constexpr uint32_t kRefineBatch = MGBVH_REFINE_BATCH;
+
 __device__ __forceinline__ bool refine_window(float cmin, float ext, uint32_t q, uint32_t& lo, uint32_t& hi) {
     const float cmax = __fadd_rn(cmin, ext);
-    const bool ok = kPartCodes && ext > 0.0f && ext < 3.0e38f && fabsf(cmin) <= __fmul_rn(ext, 16384.0f) &&
+    const bool ok = MGBVH_REFINE_WINDOW && kPartCodes && ext > 0.0f && ext < 3.0e38f &&
+                    fabsf(cmin) <= __fmul_rn(ext, 16384.0f) &&
                     fabsf(cmax) <= __fmul_rn(ext, 16384.0f);
     lo = ok && q > 0u ? 2u * q - 1u : 0u;
     hi = ok ? min(2u * q + 2u, 31u) : 31u;
@@ -813,7 +825,7 @@ __device__ __forceinline__ bool refine_window(float cmin, float ext, uint32_t q,
 // and compared: the bin pass's codes place the others, whose counts come
 // from the tile's bin prefix counts here and whose boxes come from the
 // node's coarse bins in lvl_eval2. Grid-stride over the level's tiles.
-__global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
+__global__ void __launch_bounds__(kTileThreads, MGBVH_REFINE_MIN_BLOCKS) lvl_refine_bin_kernel(
     const Task* __restrict__ tasks, const uint32_t* __restrict__ cbkeys,
     const LvlRefine* __restrict__ refine, uint32_t* __restrict__ rbins,
     const uint32_t* __restrict__ tile_task, const uint32_t* __restrict__ tile_begin,
@@ -852,45 +864,60 @@ __global__ void __launch_bounds__(kTileThreads) lvl_refine_bin_kernel(
         const Rec* src = (t.buf ? rec1 : rec0) + t.start + begin;
         const uint16_t* cs = codes + t.start + begin;
         const bool all0 = wlo[0] == 0u && whi[0] == 31u, all1 = wlo[1] == 0u && whi[1] == 31u;
-        for (uint32_t i = threadIdx.x; i < cnt; i += blockDim.x) {
-            bool in[2];
-            if (all0 && all1) {
-                in[0] = in[1] = true;
-            } else {
-                const uint32_t code = cs[i];
+        // batches of kRefineBatch objects per thread: their codes loaded
+        // together, then the records of those inside a window, then compared
+#pragma unroll
+        for (uint32_t j0 = 0; j0 < kRecsPerThread; j0 += kRefineBatch) {
+            uint32_t code[kRefineBatch];
+#pragma unroll
+            for (uint32_t q = 0; q < kRefineBatch; ++q) {
+                const uint32_t i = threadIdx.x + (j0 + q) * kTileThreads;
+                code[q] = (i < cnt && !(all0 && all1)) ? cs[i] : 0u;
+            }
+            bool in[kRefineBatch][2];
+            float4 rl[kRefineBatch], rh[kRefineBatch];
+#pragma unroll
+            for (uint32_t q = 0; q < kRefineBatch; ++q) {
+                const uint32_t i = threadIdx.x + (j0 + q) * kTileThreads;
 #pragma unroll
                 for (int p = 0; p < 2; ++p) {
-                    const uint32_t b = (code >> (5u * ax[p])) & 31u;
-                    in[p] = b >= wlo[p] && b <= whi[p];
+                    const uint32_t b = (code[q] >> (5u * ax[p])) & 31u;
+                    in[q][p] = i < cnt && act[p] && b >= wlo[p] && b <= whi[p];
+                }
+                if (in[q][0] || in[q][1]) {
+                    rl[q] = src[i].lo;
+                    rh[q] = src[i].hi;
                 }
             }
-            if (!((act[0] && in[0]) || (act[1] && in[1]))) continue;
-            const float4 lo = src[i].lo, hi = src[i].hi;
-            const float l[3] = {lo.x, lo.y, lo.z}, h[3] = {hi.x, hi.y, hi.z};
 #pragma unroll
-            for (int p = 0; p < 2; ++p) {
-                if (!act[p] || !in[p]) continue;
-                const float c = center_of(sel3(l, ax[p]), sel3(h, ax[p]));
-                // interval = number of thresholds thr with !(c < thr)
-                uint32_t lo_i = 0, hi_i = 16;
+            for (uint32_t q = 0; q < kRefineBatch; ++q) {
+                if (!(in[q][0] || in[q][1])) continue;
+                const float l[3] = {rl[q].x, rl[q].y, rl[q].z}, h[3] = {rh[q].x, rh[q].y, rh[q].z};
 #pragma unroll
-                for (int s = 0; s < 5; ++s) {
-                    if (lo_i < hi_i) {
-                        const uint32_t mid = (lo_i + hi_i) >> 1;
-                        if (!(c < sthr[16 * p + mid]))
-                            lo_i = mid + 1;
-                        else
-                            hi_i = mid;
+                for (int p = 0; p < 2; ++p) {
+                    if (!in[q][p]) continue;
+                    const float c = center_of(sel3(l, ax[p]), sel3(h, ax[p]));
+                    // interval = number of thresholds thr with !(c < thr)
+                    uint32_t lo_i = 0, hi_i = 16;
+#pragma unroll
+                    for (int st = 0; st < 5; ++st) {
+                        if (lo_i < hi_i) {
+                            const uint32_t mid = (lo_i + hi_i) >> 1;
+                            if (!(c < sthr[16 * p + mid]))
+                                lo_i = mid + 1;
+                            else
+                                hi_i = mid;
+                        }
                     }
+                    uint32_t* wd = sb + (p * 17 + lo_i) * 7;
+                    atomicAdd(wd, 1u);
+                    atomicMin(wd + 1, fkey(l[0]));
+                    atomicMin(wd + 2, fkey(l[1]));
+                    atomicMin(wd + 3, fkey(l[2]));
+                    atomicMax(wd + 4, fkey(h[0]));
+                    atomicMax(wd + 5, fkey(h[1]));
+                    atomicMax(wd + 6, fkey(h[2]));
                 }
-                uint32_t* wd = sb + (p * 17 + lo_i) * 7;
-                atomicAdd(wd, 1u);
-                atomicMin(wd + 1, fkey(l[0]));
-                atomicMin(wd + 2, fkey(l[1]));
-                atomicMin(wd + 3, fkey(l[2]));
-                atomicMax(wd + 4, fkey(h[0]));
-                atomicMax(wd + 5, fkey(h[1]));
-                atomicMax(wd + 6, fkey(h[2]));
             }
         }
         __syncthreads();
