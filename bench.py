@@ -826,7 +826,7 @@ def run_learned(args):
     uniform directions) on the built tree. The full-sweep SAH of each mesh
     comes from tests/golden/full_sweep_sah.json (written by the script beside
     it). Forms: plain (the reference's tree), learned (trained network with
-    the recommended gate: refine logit > 0, network on nodes of >= 1,025
+    the recommended gate: refine logit > 0, network on nodes of >= 2,048
     objects), learned-ungated (every binned node of 33 or more objects scores
     the network's proposals)."""
     import torch
