@@ -4,9 +4,9 @@ Everything runs on the GPU through libmgbvh.so:
   * samples: builds of synthetic meshes (random small triangles, noisy
     icospheres and small mixed scenes, fresh seeds) in sample mode, where the
     builder writes, for every binned node of 33..8192 objects, its 24
-    features and the exact
-    full-sweep SAH optimum (axis, 1/16 position bucket) plus whether that
-    optimum beats the plain binned split (mgbvh_set_sample_output);
+    features and the exact full-sweep SAH optimum (axis, 1/16 position
+    bucket) plus whether that optimum beats the plain binned split
+    (mgbvh_set_sample_output);
   * training: the project's own forward/backward kernels (BF16 weights,
     FP32 accumulation) and Adam on FP32 master weights;
   * use: mgbvh_set_split_proposer, after which builds score the network's
