@@ -1414,6 +1414,8 @@ __global__ void med_reset_kernel(Counters* ctr) {
         ctr->n_medium = 0;
         ctr->n_small = 0;
         ctr->n_med = 0;
+        ctr->medium_take = 0;
+        ctr->small_take = 0;
     }
 }
 
@@ -2344,6 +2346,13 @@ __device__ __forceinline__ void medium_task(MS& S, const Task t, Rec* rec0, Rec*
 #define MGBVH_MEDIUM_LEARN_CTAS 4  // learned-form subtree CTAs per SM the register budget must allow (tuning knob)
 #endif
 
+#ifndef MGBVH_SMALL_TAKE
+#define MGBVH_SMALL_TAKE 1  // 1: small-subtree warps take tasks from a counter (0: grid-stride order)
+#endif
+#ifndef MGBVH_MEDIUM_TAKE
+#define MGBVH_MEDIUM_TAKE 1  // 1: subtree CTAs take tasks from a counter (0: grid-stride order)
+#endif
+
 // The subtree CTA's dynamic shared memory.
 template <bool kLearn, uint32_t kCap>
 constexpr size_t medium_smem_bytes() {
@@ -2359,9 +2368,23 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? MGBVH_MEDIUM_LEARN_CT
     pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
-    // range (nullable): tasks [range[0], range[1]) instead of all of them
+    // range (nullable): tasks [range[0], range[1]) instead of all of them,
+    // in grid-stride order; without one, CTAs take the tasks in turn from a
+    // counter (subtree sizes vary, so a fixed assignment leaves a tail)
     const uint32_t t0 = range ? range[0] : 0u;
     const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
+    if (MGBVH_MEDIUM_TAKE && !range) {
+        __shared__ uint32_t s_ti;
+        for (;;) {
+            __syncthreads();  // the previous task's readers of s_ti and of S are done
+            if (threadIdx.x == 0) s_ti = atomicAdd(&O.ctr->medium_take, 1u);
+            __syncthreads();
+            const uint32_t ti = s_ti;
+            if (ti >= n_tasks) break;
+            medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
+        }
+        return;
+    }
     for (uint32_t ti = t0 + blockIdx.x; ti < n_tasks; ti += gridDim.x) {
         __syncthreads();
         medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
@@ -2481,7 +2504,17 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
     const uint32_t w0 = range ? range[0] : 0u;
     const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
     const uint32_t wpb = blockDim.x >> 5;  // warps per CTA (64..256 threads)
-    for (uint32_t w = w0 + blockIdx.x * wpb + wib; w < n_tasks; w += gridDim.x * wpb) {
+    // without a range, warps take tasks in turn from a counter (subtree
+    // sizes vary, so a fixed assignment leaves a tail); with one, grid-stride
+    const bool take = MGBVH_SMALL_TAKE && !range;
+    uint32_t w = w0 + blockIdx.x * wpb + wib;
+    for (;; w += gridDim.x * wpb) {
+        if (take) {
+            uint32_t tw = 0;
+            if (lane == 0) tw = atomicAdd(&O.ctr->small_take, 1u);
+            w = __shfl_sync(kFull, tw, 0);
+        }
+        if (w >= n_tasks) break;
         const Task t = tasks[w];
         const Rec* src = (t.buf ? rec1 : rec0) + t.start;
         float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {0.f, 0.f, 0.f};

@@ -60,6 +60,8 @@ struct Counters {
     uint32_t root_keys[12];  // object bounds lo/hi keys, centroid lo/hi keys
     uint32_t learned;        // nodes where a proposal of the split network replaced the binned split
     uint32_t n_med;          // level-pass nodes waiting for a forced median split (the median passes)
+    uint32_t medium_take;    // next subtree CTA task to take (subtree CTAs take tasks in turn)
+    uint32_t small_take;     // next small-subtree task to take (warps take tasks in turn)
     // streamed output (slot chunks): subtrees of 33..medium_max objects per
     // chunk, their placement cursors and sorted ranges; subtrees of <= 32
     // objects selected so far, the sorted range of each chunk's, and the CTAs
