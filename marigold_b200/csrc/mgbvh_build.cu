@@ -359,6 +359,7 @@ __global__ void init_root_kernel(uint32_t n, uint32_t cls, uint32_t has_bounds, 
 
 constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 
+
 #ifndef MGBVH_BIN_MIN_BLOCKS
 #define MGBVH_BIN_MIN_BLOCKS 4  // CTAs per SM the register budget must allow (tuning knob; 1 / 3 / 4 with batches of 8 / 4 / 4: 682 / 691 / 692 Mtri/s)
 #endif
