@@ -367,9 +367,6 @@ constexpr uint32_t kRecsPerThread = kTile / kTileThreads;  // 8
 #define MGBVH_PART_CODES 1  // 1: the bin pass stores each record's bins (16 bits) and the partition reads them
 #endif
 constexpr bool kPartCodes = MGBVH_PART_CODES != 0;
-#ifndef MGBVH_REFINE_AGG
-#define MGBVH_REFINE_AGG 1  // 1: the refine pass merges its edge intervals across the warp (0: per-lane atomics)
-#endif
 #ifndef MGBVH_BIN_BATCH
 #define MGBVH_BIN_BATCH 4  // records a thread loads before binning them (tuning knob; divides 8)
 #endif
