@@ -41,11 +41,11 @@ METRIC = "BVH build Mtri/s"
 UNIT = "Mtri/s"
 SAMPLE_TRIS = 131072
 # dram__bytes_read.sum + dram__bytes_write.sum of one small_kernel launch on
-# this workload, from an ncu capture (cold cache): 47.01 MB + 49.92 MB
-SMALL_KERNEL_TRAFFIC = 96931840
+# this workload, from an ncu capture (cold cache): 46.45 MB + 52.79 MB
+SMALL_KERNEL_TRAFFIC = 99239936
 # smsp__inst_executed.sum of the same launch (warp instructions); the issue
 # ceiling is one warp instruction per SM sub-partition per cycle
-SMALL_KERNEL_INST = 417821559
+SMALL_KERNEL_INST = 406144260
 SM_SUBPARTITIONS = 4
 WORKLOAD = ("noisy icosphere L8 (1,310,720 tris, 655,362 verts), leaf 1, max_depth 32, "
             "reference split profile")
