@@ -2366,26 +2366,28 @@ __global__ void __launch_bounds__(kMediumThreads, kLearn ? MGBVH_MEDIUM_LEARN_CT
     pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MediumSmemT<kCap>& S = *reinterpret_cast<MediumSmemT<kCap>*>(smem_raw);
-    // range (nullable): tasks [range[0], range[1]) instead of all of them,
-    // in grid-stride order; without one, CTAs take the tasks in turn from a
-    // counter (subtree sizes vary, so a fixed assignment leaves a tail)
+    // range (nullable): tasks [range[0], range[1]) instead of all of them
+    // (range is ctr->mrange + c for slot chunk c). CTAs take the tasks in
+    // turn from a counter (subtree sizes vary, so a fixed assignment leaves
+    // a tail): medium_take, or mtake[c] for a chunk.
     const uint32_t t0 = range ? range[0] : 0u;
     const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_medium);
-    if (MGBVH_MEDIUM_TAKE && !range) {
+    if (MGBVH_MEDIUM_TAKE) {
         __shared__ uint32_t s_ti;
+        uint32_t* take = range ? O.ctr->mtake + (range - O.ctr->mrange) : &O.ctr->medium_take;
         for (;;) {
             __syncthreads();  // the previous task's readers of s_ti and of S are done
-            if (threadIdx.x == 0) s_ti = atomicAdd(&O.ctr->medium_take, 1u);
+            if (threadIdx.x == 0) s_ti = t0 + atomicAdd(take, 1u);
             __syncthreads();
             const uint32_t ti = s_ti;
             if (ti >= n_tasks) break;
             medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
         }
-        return;
-    }
-    for (uint32_t ti = t0 + blockIdx.x; ti < n_tasks; ti += gridDim.x) {
-        __syncthreads();
-        medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
+    } else {
+        for (uint32_t ti = t0 + blockIdx.x; ti < n_tasks; ti += gridDim.x) {
+            __syncthreads();
+            medium_task<kLearn>(S, tasks[ti], rec0, rec1, small, cap_small, P, O, LN);
+        }
     }
 }
 
@@ -2502,14 +2504,15 @@ __global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(cons
     const uint32_t w0 = range ? range[0] : 0u;
     const uint32_t n_tasks = range ? range[1] : *reinterpret_cast<volatile uint32_t*>(&O.ctr->n_small);
     const uint32_t wpb = blockDim.x >> 5;  // warps per CTA (64..256 threads)
-    // without a range, warps take tasks in turn from a counter (subtree
-    // sizes vary, so a fixed assignment leaves a tail); with one, grid-stride
-    const bool take = MGBVH_SMALL_TAKE && !range;
+    // warps take tasks in turn from a counter (subtree sizes vary, so a
+    // fixed assignment leaves a tail): small_take, or stake[c] for slot
+    // chunk c (range is ctr->srange + c)
+    uint32_t* take = range ? O.ctr->stake + (range - O.ctr->srange) : &O.ctr->small_take;
     uint32_t w = w0 + blockIdx.x * wpb + wib;
     for (;; w += gridDim.x * wpb) {
-        if (take) {
+        if (MGBVH_SMALL_TAKE) {
             uint32_t tw = 0;
-            if (lane == 0) tw = atomicAdd(&O.ctr->small_take, 1u);
+            if (lane == 0) tw = w0 + atomicAdd(take, 1u);
             w = __shfl_sync(kFull, tw, 0);
         }
         if (w >= n_tasks) break;

@@ -62,6 +62,8 @@ struct Counters {
     uint32_t n_med;          // level-pass nodes waiting for a forced median split (the median passes)
     uint32_t medium_take;    // next subtree CTA task to take (subtree CTAs take tasks in turn)
     uint32_t small_take;     // next small-subtree task to take (warps take tasks in turn)
+    uint32_t mtake[8];       // streamed output: the same, per slot chunk (subtree CTA tasks)
+    uint32_t stake[8];       // streamed output: the same, per slot chunk (small-subtree tasks)
     // streamed output (slot chunks): subtrees of 33..medium_max objects per
     // chunk, their placement cursors and sorted ranges; subtrees of <= 32
     // objects selected so far, the sorted range of each chunk's, and the CTAs
