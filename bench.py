@@ -41,11 +41,13 @@ METRIC = "BVH build Mtri/s"
 UNIT = "Mtri/s"
 SAMPLE_TRIS = 131072
 # dram__bytes_read.sum + dram__bytes_write.sum of one small_kernel launch on
-# this workload, from an ncu capture (cold cache): 46.45 MB + 52.79 MB
-SMALL_KERNEL_TRAFFIC = 99239936
-# smsp__inst_executed.sum of the same launch (warp instructions); the issue
-# ceiling is one warp instruction per SM sub-partition per cycle
-SMALL_KERNEL_INST = 406144260
+# this workload (24 warps per SM), from an ncu capture (cold cache):
+# 52.85 MB + 58.80 MB
+SMALL_KERNEL_TRAFFIC = 111650048
+# smsp__inst_executed.sum of the same launch (warp instructions, spill loads
+# and stores included); the issue ceiling is one warp instruction per SM
+# sub-partition per cycle
+SMALL_KERNEL_INST = 464942099
 SM_SUBPARTITIONS = 4
 WORKLOAD = ("noisy icosphere L8 (1,310,720 tris, 655,362 verts), leaf 1, max_depth 32, "
             "reference split profile")

@@ -273,6 +273,12 @@ MGBVH_API int mgbvh_set_queue_limits(mgbvh_ctx* ctx, uint32_t wait_microseconds,
    MGBVH_BATCH_QUEUE launch (0: as many as fit). The autotuner
    (marigold_b200/autotune.py) picks them per workload. */
 MGBVH_API int mgbvh_set_launch_shape(mgbvh_ctx* ctx, uint32_t small_threads, uint32_t queue_ctas_per_sm);
+/* Occupancy of the kernel that builds subtrees of <= 32 objects, speed only
+   (the trees do not change): the resident warps per SM its register budget
+   allows, 24 (80 registers a thread; 0 selects it) or 16 (126 registers,
+   fewer spills); any other value gives MGBVH_ERR_UNSUPPORTED. The autotuner
+   picks it per workload. */
+MGBVH_API int mgbvh_set_small_occupancy(mgbvh_ctx* ctx, uint32_t warps_per_sm);
 
 /* World AABBs of instances for the TLAS, computed on the GPU as marigold's
    scene upload computes them on the host (marigold/src/app/data/scene/

@@ -38,6 +38,7 @@ EXPORTED = (
     "mgbvh_tracer_build_wide", "mgbvh_tracer_wide_nodes", "mgbvh_trace_closest_wide_dev",
     "mgbvh_tracer_set_scene_dev", "mgbvh_trace_scene_dev", "mgbvh_trace_scene_bruteforce_dev",
     "mgbvh_set_batch_mode", "mgbvh_set_queue_limits", "mgbvh_set_launch_shape", "mgbvh_set_proposer_gate",
+    "mgbvh_set_small_occupancy",
 )
 BATCH_LEVELS = 0
 BATCH_QUEUE = 1
@@ -211,6 +212,8 @@ def load():
         L.mgbvh_set_queue_limits.restype = ctypes.c_int
         L.mgbvh_set_launch_shape.argtypes = [P, u32, u32]
         L.mgbvh_set_launch_shape.restype = ctypes.c_int
+        L.mgbvh_set_small_occupancy.argtypes = [P, u32]
+        L.mgbvh_set_small_occupancy.restype = ctypes.c_int
         L.mgbvh_set_proposer_gate.argtypes = [P, ctypes.c_float, u32]
         L.mgbvh_set_proposer_gate.restype = ctypes.c_int
         L.mgbvh_sah_cost.argtypes = [P, P, u32]
@@ -257,6 +260,10 @@ class Context:
 
     def set_launch_shape(self, small_threads: int = 0, queue_ctas_per_sm: int = 0):
         self.check(self.L.mgbvh_set_launch_shape(self.ptr, small_threads, queue_ctas_per_sm))
+
+    def set_small_occupancy(self, warps_per_sm: int = 0):
+        """Resident warps per SM of the small-subtree kernel: 24 (0) or 16."""
+        self.check(self.L.mgbvh_set_small_occupancy(self.ptr, warps_per_sm))
 
     def set_proposer_gate(self, refine_threshold: float = 0.0, min_objects: int = 0):
         """The learned form's cost knobs (see include/mgbvh.h)."""

@@ -5,6 +5,8 @@ Knobs tuned per workload:
     per-subtree kernels (33..1024): the level-to-subtree switch-over.
   * small_threads — the block size of the kernel that builds subtrees of
     <= 32 objects, one warp each (64, 128 or 256 threads per CTA).
+  * small_warps — that kernel's resident warps per SM (24 with an 80-register
+    budget, or 16 with 126 registers and fewer spills).
   * batch_mode and queue_ctas_per_sm (batched workloads) — level passes and
     subtree launches, or one persistent launch over device-side task queues
     with a given number of resident CTAs per SM.
@@ -14,11 +16,13 @@ Knobs tuned per workload:
     when its total SAH cost is within 1% of the reference profile's.
 Every knob but bins changes speed only, never the tree (each phase and
 mode computes the same split decisions): the fastest value is taken, the
-knobs one after another (switch-over, block size, batch mode, persistent
-CTAs per SM, bins), each at the best values found before it.
+knobs one after another (switch-over, block size, small-subtree occupancy,
+batch mode, persistent CTAs per SM, bins), each at the best values found
+before it.
 
 Each candidate is timed as the median of several builds (CUDA events on the
-build stream, inputs resident on the device, L2 flushed before each build).
+build stream, inputs resident on the device, L2 flushed before each build);
+batched workloads as replays of a captured CUDA graph, the form they run in.
 Run on a GPU:  python -m marigold_b200.autotune [--workloads ...]
 """
 from __future__ import annotations
@@ -36,9 +40,11 @@ TABLE = os.path.join(HERE, "tuning.json")
 
 MEDIUM_MAX = (64, 128, 256, 512, 1024)
 SMALL_THREADS = (64, 128, 256)
+SMALL_WARPS = (16, 24)
 QUEUE_CTAS = (1, 2, 3)
 BINS = (0, 8, 16, 24)
-DEFAULTS = {"medium_max": 1024, "small_threads": 256, "batch_mode": "levels", "queue_ctas_per_sm": 0, "bins": 0}
+DEFAULTS = {"medium_max": 1024, "small_threads": 256, "small_warps": 24, "batch_mode": "levels",
+            "queue_ctas_per_sm": 0, "bins": 0}
 
 
 def load_table() -> dict:
@@ -61,6 +67,7 @@ def apply(ctx, workload: str) -> dict:
     c = {k: choice(workload, k) for k in DEFAULTS}
     ctx.set_tuning(int(c["medium_max"]))
     ctx.set_launch_shape(int(c["small_threads"]), int(c["queue_ctas_per_sm"]))
+    ctx.set_small_occupancy(int(c["small_warps"]))
     ctx.set_batch_mode(c["batch_mode"] == "queue")
     return c
 
@@ -90,6 +97,7 @@ def _measure(ctx, meshes, knobs, reps=5):
     from . import BvhSettings, build_batch_device
     ctx.set_tuning(knobs["medium_max"])
     ctx.set_launch_shape(knobs["small_threads"], knobs["queue_ctas_per_sm"])
+    ctx.set_small_occupancy(knobs["small_warps"])
     ctx.set_batch_mode(knobs["batch_mode"] == "queue")
     descs = []
     for m in meshes:
@@ -139,6 +147,8 @@ def tune(names):
                 m["dev_v"] = torch.from_numpy(m["v"]).cuda()
                 m["dev_t"] = torch.from_numpy(m["t"].view(np.int32)).cuda()
                 m["n"] = m["t"].shape[0]
+        # batched workloads are timed as they run: replays of a captured graph
+        ctx.set_graph_capture(batched)
         rows = []
         best = dict(DEFAULTS)
 
@@ -157,6 +167,7 @@ def tune(names):
 
         pick("medium_max", MEDIUM_MAX)
         pick("small_threads", SMALL_THREADS)
+        pick("small_warps", SMALL_WARPS)
         if batched:
             pick("batch_mode", ("levels", "queue"))
             if best["batch_mode"] == "queue":
@@ -174,8 +185,8 @@ def tune(names):
             "choice": dict(best),
             "reference_profile_sah": ref_sah,
             "candidates": rows,
-            "rule": ("knobs that leave the tree unchanged (medium_max, small_threads, batch_mode, "
-                     "queue_ctas_per_sm): the fastest, one knob after another; bins other than the "
+            "rule": ("knobs that leave the tree unchanged (medium_max, small_threads, small_warps, "
+                     "batch_mode, queue_ctas_per_sm): the fastest, one knob after another; bins other than the "
                      "reference profile only where allowed and within 1% of its SAH")
                     + ("" if bins_free else "; bins fixed to the reference profile"),
             "measured": time.strftime("%Y-%m-%d"),

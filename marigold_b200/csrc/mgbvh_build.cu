@@ -2489,12 +2489,16 @@ __global__ void __launch_bounds__(256) small_select_kernel(const Task* __restric
 // One warp per subtree of <= 32 objects. kLevels: the level-synchronous
 // builder (every node adaptive with one threshold per object); otherwise the
 // depth-first builder that also covers binned nodes and fixed step counts.
-template <bool kLevels>
-#ifndef MGBVH_SMALL_MIN_BLOCKS
-#define MGBVH_SMALL_MIN_BLOCKS 1  // CTAs per SM the register budget must allow (tuning knob)
-#endif
+// kMinBlocks: CTAs of 256 threads per SM the register budget allows (the
+// context's small-subtree occupancy): 3 (80 registers, 24 warps per SM) or 2
+// (126 registers, 16 warps). The kernel is issue-bound on fixed-latency
+// dependencies; on the noisy icosphere the extra warps hide more of them than
+// the spills of the tighter budget add (warp-subtree phase 0.568 -> 0.543 ms;
+// 4 CTAs at 64 registers: 0.594 ms), while the batched scene builds 3% faster
+// at 16 warps. The autotuner picks it per workload.
+template <bool kLevels, int kMinBlocks>
 // range (nullable): build tasks [range[0], range[1]) instead of all of them.
-__global__ void __launch_bounds__(256, MGBVH_SMALL_MIN_BLOCKS) small_kernel(const Task* __restrict__ tasks,
+__global__ void __launch_bounds__(256, kMinBlocks) small_kernel(const Task* __restrict__ tasks,
                                                    const Rec* __restrict__ rec0,
                                                    const Rec* __restrict__ rec1, Params P, Out O,
                                                    const uint32_t* range) {
@@ -3375,6 +3379,8 @@ struct mgbvh_ctx {
     // the warp-subtree kernel, persistent CTAs per SM (0: as many as fit)
     uint32_t small_threads = 256;
     uint32_t queue_per_sm = 0;
+    // resident warps per SM of the warp-subtree kernel (mgbvh_set_small_occupancy)
+    uint32_t small_warps = 24;
     void* pin = nullptr;  // pinned staging of a batch plan
     size_t pin_bytes = 0;
     bool graph_mode = false;
@@ -3648,8 +3654,9 @@ int run_pipeline(mgbvh_ctx* ctx, const Caps& C, const Params& P, const Out& O, R
                     tasks, rec0, rec1, P_<Task>(ctx->small), C.small, P, O, LN, range);
         };
         // small subtrees: count read on the device; grid sized for full occupancy
-        auto small = (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax) ? small_kernel<true>
-                                                                              : small_kernel<false>;
+        const bool lv_small = P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax;
+        auto small = ctx->small_warps == 16u ? (lv_small ? small_kernel<true, 2> : small_kernel<false, 2>)
+                                             : (lv_small ? small_kernel<true, 3> : small_kernel<false, 3>);
         // as many warps as 8 CTAs of 256 threads per SM, whatever the CTA size
         const int small_grid = ctx->sm_count * (2048 / (int)ctx->small_threads);
         if (ctx->stream_slots && ctx->h_nodes_out) {
@@ -4359,6 +4366,7 @@ int run_batch(mgbvh_ctx* ctx, const mgbvh_mesh_desc* meshes, uint32_t nm, const 
         put(&ctx->queue_hold, 4);
         put(&ctx->queue_wait_ns, sizeof(ctx->queue_wait_ns));
         put(&ctx->small_threads, 4);
+        put(&ctx->small_warps, 4);
         put(&ctx->queue_per_sm, 4);
     }
     uint32_t launches = 0, levels = 0;
@@ -4942,6 +4950,15 @@ int mgbvh_set_launch_shape(mgbvh_ctx* ctx, uint32_t small_threads, uint32_t queu
     return MGBVH_OK;
 }
 
+int mgbvh_set_small_occupancy(mgbvh_ctx* ctx, uint32_t warps_per_sm) {
+    if (!ctx) return MGBVH_ERR_INVALID_ARG;
+    if (warps_per_sm == 0) warps_per_sm = 24;
+    if (warps_per_sm != 16 && warps_per_sm != 24)
+        return fail(ctx, MGBVH_ERR_UNSUPPORTED, "small-subtree occupancy must be 16 or 24 warps per SM");
+    ctx->small_warps = warps_per_sm;
+    return MGBVH_OK;
+}
+
 int mgbvh_set_queue_limits(mgbvh_ctx* ctx, uint32_t wait_microseconds, uint32_t held_tasks) {
     if (!ctx) return MGBVH_ERR_INVALID_ARG;
     ctx->queue_wait_ns = wait_microseconds ? 1000ull * wait_microseconds : 2000000000ull;
@@ -5081,9 +5098,9 @@ int mgbvh_build_aabbs_noalloc(const float* d_aabbs, uint32_t count, const mgbvh_
     if (cls != 0) {
         const int grid = std::max(1, std::min(sms, (int)((n / 2 + 8 + 7) / 8)));
         if (P.adaptive_steps == 0 && P.adaptive_max_n == kSmallMax)
-            small_kernel<true><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
+            small_kernel<true, 3><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
         else
-            small_kernel<false><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
+            small_kernel<false, 3><<<grid, 256, 0, sm>>>(S->small, S->rec, S->rec, P, O, nullptr);
     }
     noalloc_finish_kernel<<<1, 1024, 0, sm>>>(S, slots, d_out_nodes, d_out_lens, node_capacity);
     if (cudaGetLastError() != cudaSuccess) return MGBVH_ERR_CUDA;

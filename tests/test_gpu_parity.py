@@ -73,6 +73,27 @@ def test_knobs_and_leaf_bounds(oracle, gpu_ctx, kw):
     both(oracle, gpu_ctx, vertices=v, triangles=t, **kw)
 
 
+@pytest.mark.parametrize("small_threads,small_warps", [(256, 16), (256, 24), (128, 16), (64, 24)])
+@pytest.mark.parametrize("kw", [dict(), dict(bins=16)])
+def test_launch_shapes_leave_the_tree_unchanged(oracle, small_threads, small_warps, kw):
+    # the small-subtree kernel's block size and occupancy (both register
+    # budgets, level-synchronous and depth-first builders) change speed only
+    v, t = synth.random_triangles(20000, 11)
+    ctx = _lib.Context(0)
+    try:
+        ctx.set_launch_shape(small_threads, 0)
+        ctx.set_small_occupancy(small_warps)
+        both(oracle, ctx, vertices=v, triangles=t, **kw)
+    finally:
+        ctx.close()
+
+
+def test_small_occupancy_rejects_other_values(gpu_ctx):
+    for bad in (8, 20, 32):
+        assert gpu_ctx.L.mgbvh_set_small_occupancy(gpu_ctx.ptr, bad) == _lib.ERR_UNSUPPORTED
+    assert gpu_ctx.L.mgbvh_set_small_occupancy(gpu_ctx.ptr, 0) == 0
+
+
 def test_aabb_path_tlas_like(oracle, gpu_ctx):
     # the TLAS path: AsBoundingVolume objects, root bounds = union (bounds: None)
     rng = np.random.default_rng(3)
