@@ -158,6 +158,25 @@ def _measure(meshes, knobs, batched, reps=5):
         ctx.close()
 
 
+def pick_knob(trial, best, key, values):
+    """Times each value of one knob with trial(**{key: value}) (which returns
+    a row with "ms") and sets best[key] to the fastest. When the two fastest
+    are within CLOSE of each other, they are timed in turn CONFIRM more times
+    each and the lower mean wins (its first row is returned)."""
+    cands = [trial(**{key: v}) for v in values]
+    order = sorted(cands, key=lambda r: r["ms"])
+    top = order[0]
+    if len(order) > 1 and order[1]["ms"] <= CLOSE * top["ms"]:
+        a, b = top[key], order[1][key]
+        ta, tb = [top["ms"]], [order[1]["ms"]]
+        for _ in range(CONFIRM):
+            ta.append(trial(**{key: a})["ms"])
+            tb.append(trial(**{key: b})["ms"])
+        top = order[0] if np.mean(ta) <= np.mean(tb) else order[1]
+    best[key] = top[key]
+    return top
+
+
 def tune(names):
     import torch
     table = load_table()
@@ -182,20 +201,7 @@ def tune(names):
             return rows[-1]
 
         def pick(key, values):
-            cands = [trial(**{key: v}) for v in values]
-            order = sorted(cands, key=lambda r: r["ms"])
-            top = order[0]
-            if len(order) > 1 and order[1]["ms"] <= CLOSE * top["ms"]:
-                # the two fastest are within run-to-run spread: time them in
-                # turn CONFIRM more times each and keep the lower mean
-                a, b = top[key], order[1][key]
-                ta, tb = [top["ms"]], [order[1]["ms"]]
-                for _ in range(CONFIRM):
-                    ta.append(trial(**{key: a})["ms"])
-                    tb.append(trial(**{key: b})["ms"])
-                top = order[0] if np.mean(ta) <= np.mean(tb) else order[1]
-            best[key] = top[key]
-            return top
+            return pick_knob(trial, best, key, values)
 
         pick("medium_max", MEDIUM_MAX)
         pick("small_threads", SMALL_THREADS)
