@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(128) trace_persistent_kernel(const float4* __r
         }
         if (!__any_sync(kFull, has)) {
             if (exhausted) break;
-            continue;  // all lanes idle: the next round refills them
+            continue;  // all lanes idle: the loop's next pass refills them
         }
         if (has && sp > 0) {
             const uint32_t ni = stack[--sp];
@@ -720,7 +720,7 @@ __global__ void __launch_bounds__(128) trace_wide_persistent_kernel(
         }
         if (!__any_sync(kFull, has)) {
             if (exhausted) break;
-            continue;  // all lanes idle: the next round refills them
+            continue;  // all lanes idle: the loop's next pass refills them
         }
         if (has && sp > 0) {
             --sp;
