@@ -210,14 +210,16 @@ def algorithmic_bytes(n, n_verts, internal_len_sum, node_count):
     return (n * (12 + 3 * 32) + n * 24 + internal_len_sum * 56 + node_count * 32)
 
 
-def issue_roofline(inst, launch_ms, clk):
+def issue_roofline(inst, launch_ms, clk, sms=None):
     """The instruction-issue ceiling of a kernel: `inst` warp instructions
     (smsp__inst_executed.sum from an ncu capture of the launch) at one per
-    sub-partition per cycle on every SM, at the median SM clock sampled
-    during the timed steps. frac is the ceiling's time over the measured one,
-    i.e. the fraction of issue slots the launch used."""
-    import torch
-    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    sub-partition per cycle on every SM (`sms`, else the current device's
+    count), at the median SM clock sampled during the timed steps. frac is
+    the ceiling's time over the measured one, i.e. the fraction of issue
+    slots the launch used."""
+    if sms is None:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz")
     if not mhz or launch_ms <= 0:
         return None

@@ -62,3 +62,18 @@ def test_reference_arm_prints_on_rank_zero_only():
                        timeout=120)
     assert r.returncode == 0
     assert r.stdout.strip() == ""
+
+
+def test_issue_roofline_arithmetic():
+    # the small kernel's capture on 148 SMs at 1965 MHz: 464.9M warp
+    # instructions take 0.400 ms at one per sub-partition per cycle
+    sys.path.insert(0, ROOT)
+    import bench
+    r = bench.issue_roofline(464942099, 0.544, {"sm_mhz": 1965}, sms=148)
+    assert r["peak"] == round(148 * 4 * 1965e6 / 1e9, 1)
+    assert abs(r["frac"] - 464942099 / 0.544e-3 / (148 * 4 * 1965e6)) < 1e-4
+    assert 0.73 < r["frac"] < 0.74
+    # the sampled clock missing: the maximum clock; no clock or no time: None
+    assert bench.issue_roofline(1000, 1.0, {"sm_max_mhz": 1000}, sms=1)["sm_mhz"] == 1000
+    assert bench.issue_roofline(1000, 1.0, {}, sms=1) is None
+    assert bench.issue_roofline(1000, 0.0, {"sm_mhz": 1965}, sms=1) is None
